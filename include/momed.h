@@ -1,0 +1,143 @@
+/*
+ * momed.h -- C ABI of libmomed_b200.so, the B200 (sm_100a) backend for
+ * MomentumED.jl's matrix-free Hamiltonian map and Lanczos eigensolve.
+ *
+ * The reference binds this path through its GPU plugin hooks
+ * (MomentumED/src/method/gpu_interface.jl:13-21); each entry point below names
+ * the hook or function it replaces.  Conventions:
+ *   - every call returns an int status (MOMED_OK == 0); the message of the last
+ *     failure on a handle is momed_last_error(h).  Nothing traps or throws.
+ *   - orbitals are bits: bit i-1 of a uint64 is orbital i (EDCore MBS64).
+ *   - complex arrays are interleaved (re, im) of double (c128) or float (c64).
+ *   - basis indices are 0-based inside the ABI (the Julia shim adds 1).
+ *   - inputs are copied; the caller keeps ownership of its buffers.  Device
+ *     buffers inside a handle are owned by the handle.
+ *   - one handle per host thread; distinct handles are independent.
+ */
+#ifndef MOMED_H
+#define MOMED_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MOMED_API __attribute__((visibility("default")))
+#else
+#define MOMED_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOMED_OK        0
+#define MOMED_EINVAL    1   /* bad argument or size */
+#define MOMED_ENOMEM    2   /* device memory / HBM budget refused */
+#define MOMED_ECUDA     3   /* CUDA runtime error (message carries the CUDA text) */
+#define MOMED_ENOTCONV  4   /* eigensolver stopped at maxiter (results still written) */
+#define MOMED_ETIMEOUT  5   /* a bounded wait gave up */
+#define MOMED_ESTATE    6   /* call order (e.g. matvec before set_basis) */
+#define MOMED_ENODEV    7   /* no usable CUDA device */
+
+#define MOMED_C128      0   /* complex double vectors / FP64 arithmetic */
+#define MOMED_C64       1   /* complex float vectors, FP32 accumulate */
+
+#define MOMED_PREC_FP64   0 /* plain: c128 matvec, FP64 Lanczos */
+#define MOMED_PREC_MIXED  1 /* c64 matvec + FP64 recurrences, then FP64 Rayleigh-Ritz / refinement */
+
+typedef struct momed_handle momed_handle;
+
+/* EDPara subset the basis enumerator needs (init_parameter.jl:62-146). */
+typedef struct {
+    int32_t dim, Nk, Nc_mix, Nc_conserve;
+    const int64_t* k_list;   /* k_list[d + dim*i], column i of the Julia dim x Nk matrix */
+    const int64_t* Gk;       /* [dim]; 0 = no periodicity in that direction */
+} momed_para;
+
+typedef struct {
+    int32_t nev;          /* eigenpairs wanted (EDsolve N) */
+    int32_t krylovdim;    /* Krylov subspace size (KrylovKit krylovdim; default 30) */
+    int32_t maxiter;      /* restarts (KrylovKit maxiter; default 100) */
+    int32_t precision;    /* MOMED_PREC_FP64 or MOMED_PREC_MIXED */
+    double  tol;          /* residual-norm tolerance (KrylovKit tol; default 1e-12) */
+    uint64_t seed;        /* start vector seed when vec0 == NULL */
+    int32_t want_vectors; /* 0: eigenvalues only */
+    int32_t vecs_on_device;
+} momed_solve_opts;
+
+typedef struct {
+    int32_t converged;     /* leading eigenpairs with residual <= tol */
+    int32_t restarts;
+    int64_t matvecs;       /* all matvecs */
+    int64_t matvecs_fp64;  /* of which FP64 (mixed mode) */
+    double  seconds;       /* device time of the solve */
+} momed_info;
+
+/* Library */
+MOMED_API const char* momed_version(void);
+MOMED_API int  momed_create(int device, momed_handle** out);             /* activate_gpu_device (gpu_interface.jl:41-55) */
+MOMED_API int  momed_destroy(momed_handle* h);                           /* release_gpu_memory (MomentumEDCUDAExt.jl:43-47) */
+MOMED_API const char* momed_last_error(const momed_handle* h);
+MOMED_API int  momed_set_stream(momed_handle* h, void* cuda_stream);      /* optional; default: the handle's own stream */
+MOMED_API int  momed_set_hbm_budget(momed_handle* h, int64_t bytes);      /* admission limit for this handle (0 = free memory) */
+
+/* Kernel (a): basis enumeration per momentum sector.
+ * Replaces ED_momentum_subspaces (momentum_decomposition.jl:339-413) without selection_rule.
+ * mask (sorted 1-based orbitals) may be NULL (mlen < 0).  momentum_list (nmom * dim) restricts
+ * the sectors when nmom >= 0; nmom < 0 enumerates every momentum in the reference order.
+ * The result stays on the device; fetch it with momed_enumeration_copy. */
+MOMED_API int  momed_enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each, int32_t ncc,
+                           const int64_t* mask, int32_t mlen, const int64_t* momentum_list, int32_t nmom,
+                           int64_t* n_sectors, int64_t* n_total);
+/* sector_k [n_sectors*dim], sector_sizes [n_sectors], basis [n_total] (host, or device if basis_on_device). */
+MOMED_API int  momed_enumeration_copy(momed_handle* h, int64_t* sector_k, int64_t* sector_sizes, uint64_t* basis,
+                            int32_t basis_on_device);
+/* Use sector s of the last enumeration as the working basis (device to device). */
+MOMED_API int  momed_select_sector(momed_handle* h, int64_t s);
+
+/* Working basis: the sorted HilbertSubspace list (hilbert_subspace.jl:19-30), uploaded as in
+ * create_gpu_linearmap (MomentumEDCUDAExt.jl:94-113). */
+MOMED_API int  momed_set_basis(momed_handle* h, const uint64_t* basis, int64_t n, int32_t on_device);
+
+/* Operator: the Hermitian-completed, sorted scatter list of LinearMap (linear_map.jl:22-37),
+ * flattened as in create_gpu_linearmap: amp[2*nscat] (c128), in/out/parity masks.
+ * parity may be NULL (recomputed).  Amplitudes of c64 matvecs are rounded from these. */
+MOMED_API int  momed_set_scatter(momed_handle* h, const double* amp, const uint64_t* in, const uint64_t* out,
+                       const uint64_t* parity, int64_t nscat);
+/* Parametrised operator H(u) = A + u B on one term list (amp_b may be NULL = zeros): used by
+ * the batched solver where u is an interaction strength (two-body amplitudes scaled by u). */
+MOMED_API int  momed_set_scatter_pair(momed_handle* h, const double* amp_a, const double* amp_b, const uint64_t* in,
+                            const uint64_t* out, const uint64_t* parity, int64_t nscat);
+
+/* Parameter u of the operator H(u) = A + u B set by momed_set_scatter_pair (default 1). */
+MOMED_API int  momed_set_param(momed_handle* h, double u);
+
+/* y = H x: the callable (y, x) of CuLinearMap (MomentumEDCUDAExt.jl:119-122, kernel at
+ * gpu_interface.jl:128-163), computing H*x as the CPU LinearMap does (linear_map.jl:100-118).
+ * precision MOMED_C128 / MOMED_C64; x, y host or device (on_device). */
+MOMED_API int  momed_matvec(momed_handle* h, const void* x, void* y, int32_t precision, int32_t on_device);
+
+/* Lowest nev eigenpairs: krylov_map_solve (MomentumEDCUDAExt.jl:159-179) -> KrylovKit eigsolve(:SR).
+ * vals[nev] ascending; resid[nev] = ||H x - e x|| per pair (may be NULL);
+ * vecs [nev][N] c128 (host, or device if opts->vecs_on_device).  vec0 (c128, host) may be NULL.
+ * Returns MOMED_ENOTCONV when fewer than nev pairs met tol (results still written). */
+MOMED_API int  momed_eigsolve(momed_handle* h, const momed_solve_opts* opts, const double* vec0,
+                    double* vals, double* resid, void* vecs, momed_info* info);
+
+/* Batched solve of H(u) = A + u B (momed_set_scatter_pair) for nu values of u at once on the
+ * working basis: block matvec over all u, one Lanczos per u.  vals [nu][nev], resid [nu][nev];
+ * vecs [nu][nev][N] c128 host (may be NULL).  Mixed precision is opts->precision. */
+MOMED_API int  momed_batch_solve(momed_handle* h, const momed_solve_opts* opts, const double* u, int32_t nu,
+                       double* vals, double* resid, double* vecs, momed_info* info);
+
+/* Diagnostics for roofline accounting: exact (row, term) hit count of the working operator
+ * on the working basis, the index mode (0 = ranked tables, 1 = checked tables, 2 = search),
+ * and the bytes of the lookup tables. */
+MOMED_API int  momed_stats(momed_handle* h, int64_t* nnz, int32_t* index_mode, int64_t* table_bytes);
+
+/* Device time (ms) of the last matvec kernel launch on the handle's stream. */
+MOMED_API int  momed_last_kernel_ms(momed_handle* h, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOMED_H */

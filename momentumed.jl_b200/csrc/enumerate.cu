@@ -1,0 +1,427 @@
+// Kernel (a): per-momentum-sector basis enumeration.
+//
+// Reference: ED_momentum_subspaces (MomentumED/src/preparation/momentum_decomposition.jl:339-413)
+// recurses over the conserved components, last component outermost and in the
+// highest bits (accumulated_mbs * mbs_smaller, EDCore manybodystate_basis.jl:81-83),
+// each component walked in colex order (EDCore colex_mbslist.jl), and pushes
+// every state into the sector of its total momentum residue (init_parameter.jl:148-152).
+// Walking the mixed-radix rank r = sum_c rank_c * stride_c (component 0 fastest)
+// in increasing order yields the states in increasing uint64 order, so each
+// sector's list comes out sorted exactly as the reference builds it.
+//
+// GPU scheme: the rank space is cut into one contiguous chunk per thread.  A
+// thread unranks its chunk start (combinadic unranking per component) and then
+// steps with the next-combination rule.  Pass 1 counts per (sector, block);
+// the host scans those counts; pass 2 recounts, scans per sector inside the
+// block and writes every state at its final position.
+#include <algorithm>
+#include <climits>
+#include <numeric>
+
+#include "momed_internal.cuh"
+
+namespace momed {
+
+namespace {
+
+constexpr int kMaxComp = 8;
+constexpr int kSecWin = 32;      // sectors handled per pass window
+constexpr int kThreads = 256;
+
+struct Comp {
+    int32_t t;            // particles (|N|)
+    int32_t len;          // available positions
+    int32_t shift;        // first bit of the component
+    int32_t masked;       // positions come from pos[] (mask) instead of 0..len-1
+    int64_t count;        // C(len, t)
+    int64_t stride;       // rank stride
+    int8_t pos[64];       // bit offsets (within the component) of available positions
+};
+
+struct EnumParams {
+    int32_t ncomp, dim;
+    Comp comp[kMaxComp];
+    int64_t total;        // product of counts
+    int64_t chunk;        // ranks per thread
+    int32_t kv[64][3];    // signed momentum of each global orbital (dim <= 3)
+    int32_t Gk[3];
+    int32_t box_lo[3];
+    int32_t box_ext[3];
+    const int32_t* sec_of; // [prod box_ext] sector id or -1
+    const uint64_t* binom;  // [65 * 65] C(n, k) as uint64
+};
+
+__device__ __forceinline__ uint64_t dbinom(const uint64_t* b, int n, int k) {
+    return (k < 0 || n < 0 || k > n) ? 0ull : b[n * 65 + k];
+}
+
+// pattern (over len positions, t set bits) of the rank-th combination in colex order
+__device__ uint64_t unrank_pattern(const uint64_t* binom, int len, int t, int64_t rank) {
+    uint64_t pat = 0;
+    int64_t x = rank;
+    for (int i = t; i >= 1; --i) {
+        int c = i - 1;
+        while (c + 1 < len && (int64_t)dbinom(binom, c + 1, i) <= x) ++c;
+        pat |= 1ull << c;
+        x -= (int64_t)dbinom(binom, c, i);
+    }
+    return pat;
+}
+
+// next larger integer with the same popcount
+__device__ __forceinline__ uint64_t next_comb(uint64_t x) {
+    uint64_t c = x & (~x + 1ull);
+    uint64_t r = x + c;
+    return r | (((x ^ r) >> 2) >> (__ffsll((long long)c) - 1));
+}
+
+__device__ __forceinline__ uint64_t deposit(const Comp& c, uint64_t pat) {
+    if (!c.masked) return pat << c.shift;
+    uint64_t out = 0;
+    while (pat) {
+        int p = __ffsll((long long)pat) - 1;
+        out |= 1ull << (c.shift + c.pos[p]);
+        pat &= pat - 1ull;
+    }
+    return out;
+}
+
+__device__ __forceinline__ int sector_of(const EnumParams& P, uint64_t s) {
+    int k[3] = {0, 0, 0};
+    while (s) {
+        int o = __ffsll((long long)s) - 1;
+        for (int d = 0; d < P.dim; ++d) k[d] += P.kv[o][d];
+        s &= s - 1ull;
+    }
+    int64_t idx = 0, stride = 1;
+    for (int d = 0; d < P.dim; ++d) {
+        int v = k[d];
+        if (P.Gk[d] != 0) { v %= P.Gk[d]; if (v < 0) v += P.Gk[d]; }
+        v -= P.box_lo[d];
+        if (v < 0 || v >= P.box_ext[d]) return -1;
+        idx += (int64_t)v * stride;
+        stride *= P.box_ext[d];
+    }
+    return __ldg(P.sec_of + idx);
+}
+
+// Walk ranks [r0, r1) calling f(state) in order.
+template <typename F>
+__device__ void walk(const EnumParams& P, int64_t r0, int64_t r1, F&& f) {
+    if (r0 >= r1) return;
+    uint64_t pat[kMaxComp];
+    int64_t rk[kMaxComp];
+    uint64_t part[kMaxComp];
+    int64_t rem = r0;
+    for (int c = P.ncomp - 1; c >= 0; --c) {
+        rk[c] = rem / P.comp[c].stride;
+        rem -= rk[c] * P.comp[c].stride;
+    }
+    uint64_t state = 0;
+    for (int c = 0; c < P.ncomp; ++c) {
+        pat[c] = unrank_pattern(P.binom, P.comp[c].len, P.comp[c].t, rk[c]);
+        part[c] = deposit(P.comp[c], pat[c]);
+        state |= part[c];
+    }
+    for (int64_t r = r0; r < r1; ++r) {
+        f(state);
+        // advance component 0 with carry
+        for (int c = 0; c < P.ncomp; ++c) {
+            state &= ~part[c];
+            if (rk[c] + 1 < P.comp[c].count) {
+                ++rk[c];
+                pat[c] = next_comb(pat[c]);
+                part[c] = deposit(P.comp[c], pat[c]);
+                state |= part[c];
+                break;
+            }
+            rk[c] = 0;
+            pat[c] = P.comp[c].t ? ((1ull << P.comp[c].t) - 1ull) : 0ull;
+            part[c] = deposit(P.comp[c], pat[c]);
+            state |= part[c];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_enum_count(EnumParams P, int win0, int nwin, int32_t* block_counts /* [nwin][nblocks] */) {
+    __shared__ int32_t sc[kSecWin];
+    if (threadIdx.x < kSecWin) sc[threadIdx.x] = 0;
+    __syncthreads();
+    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t r0 = tid * P.chunk, r1 = min(P.total, r0 + P.chunk);
+    int32_t cnt[kSecWin];
+#pragma unroll
+    for (int i = 0; i < kSecWin; ++i) cnt[i] = 0;
+    walk(P, r0, r1, [&](uint64_t s) {
+        int sec = sector_of(P, s) - win0;
+        if (sec >= 0 && sec < nwin) {
+#pragma unroll
+            for (int i = 0; i < kSecWin; ++i) cnt[i] += (i == sec);
+        }
+    });
+    for (int i = 0; i < nwin; ++i)
+        if (cnt[i]) atomicAdd(&sc[i], cnt[i]);
+    __syncthreads();
+    if (threadIdx.x < nwin) block_counts[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = sc[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_enum_write(EnumParams P, int win0, int nwin, const int64_t* block_offsets /* [nwin][nblocks] */, uint64_t* out) {
+    __shared__ int32_t warp_tot[kThreads / 32];
+    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t r0 = tid * P.chunk, r1 = min(P.total, r0 + P.chunk);
+    int32_t cnt[kSecWin];
+#pragma unroll
+    for (int i = 0; i < kSecWin; ++i) cnt[i] = 0;
+    walk(P, r0, r1, [&](uint64_t s) {
+        int sec = sector_of(P, s) - win0;
+        if (sec >= 0 && sec < nwin) {
+#pragma unroll
+            for (int i = 0; i < kSecWin; ++i) cnt[i] += (i == sec);
+        }
+    });
+    // per-sector exclusive scan over the block's threads (thread order = rank order)
+    int64_t pos[kSecWin];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int i = 0; i < kSecWin; ++i) {
+        int v = (i < nwin) ? cnt[i] : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) warp_tot[wid] = incl;
+        __syncthreads();
+        int before = 0;
+        for (int w = 0; w < wid; ++w) before += warp_tot[w];
+        __syncthreads();
+        pos[i] = (i < nwin) ? block_offsets[(int64_t)i * gridDim.x + blockIdx.x] + before + (incl - v) : 0;
+    }
+    walk(P, r0, r1, [&](uint64_t s) {
+        int sec = sector_of(P, s) - win0;
+        if (sec >= 0 && sec < nwin) {
+            int64_t p = 0;
+#pragma unroll
+            for (int i = 0; i < kSecWin; ++i) {
+                if (i == sec) { p = pos[i]; pos[i] = p + 1; }
+            }
+            out[p] = s;
+        }
+    });
+}
+
+int64_t hbinom(int n, int k) {
+    if (k < 0 || n < 0 || k > n) return 0;
+    if (k > n - k) k = n - k;
+    __int128 r = 1;
+    for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+    return r > (__int128)INT64_MAX ? INT64_MAX : (int64_t)r;
+}
+
+int64_t jmod(int64_t a, int64_t g) { int64_t r = a % g; return r < 0 ? r + g : r; }
+
+}  // namespace
+
+void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each, int ncc, const int64_t* mask,
+                     int mlen, const int64_t* momentum_list, int nmom) {
+    MOMED_REQUIRE(p && p->k_list && p->Gk, MOMED_EINVAL, "para, k_list and Gk are required");
+    MOMED_REQUIRE(ncc == p->Nc_conserve && ncc >= 1 && ncc <= kMaxComp, MOMED_EINVAL,
+                  "length of N_each must equal Nc_conserve (<= 8)");
+    MOMED_REQUIRE(p->dim >= 1 && p->dim <= 3, MOMED_EINVAL, "dim must be 1..3");
+    const int dim = p->dim, Nk = p->Nk;
+    const int ncomp_bits = Nk * p->Nc_mix;
+    MOMED_REQUIRE((int64_t)ncomp_bits * ncc <= 64 && Nk >= 1, MOMED_EINVAL, "Nk * Nc must be <= 64");
+
+    EnumParams P{};
+    P.ncomp = ncc;
+    P.dim = dim;
+    for (int d = 0; d < dim; ++d) P.Gk[d] = (int32_t)p->Gk[d];
+
+    // components (component 0 = N_each[0] = lowest bits)
+    std::vector<int64_t> smask;
+    if (mask && mlen >= 0) { smask.assign(mask, mask + mlen); std::sort(smask.begin(), smask.end()); }
+    int64_t total = 1;
+    for (int c = 0; c < ncc; ++c) {
+        Comp& C = P.comp[c];
+        int64_t Nc = N_each[c];
+        C.t = (int32_t)(Nc < 0 ? -Nc : Nc);
+        C.shift = c * ncomp_bits;
+        if (mask && mlen >= 0) {
+            C.masked = 1;
+            C.len = 0;
+            for (int64_t m : smask) {
+                int64_t rel = m - (int64_t)c * ncomp_bits;
+                if (rel >= 1 && rel <= ncomp_bits) C.pos[C.len++] = (int8_t)(rel - 1);
+            }
+        } else {
+            C.masked = 0;
+            C.len = ncomp_bits;
+            for (int i = 0; i < ncomp_bits; ++i) C.pos[i] = (int8_t)i;
+        }
+        MOMED_REQUIRE(C.t <= ncomp_bits, MOMED_EINVAL, "Invalid number of electrons in one component");
+        C.count = hbinom(C.len, C.t);
+        C.stride = total;
+        MOMED_REQUIRE(C.count == 0 || total <= INT64_MAX / std::max<int64_t>(C.count, 1), MOMED_EINVAL,
+                      "combination space too large");
+        total *= C.count;
+        int sgn = Nc > 0 ? 1 : (Nc < 0 ? -1 : 0);
+        for (int i = 0; i < ncomp_bits; ++i) {
+            int ik = i % Nk;
+            for (int d = 0; d < dim; ++d) P.kv[C.shift + i][d] = sgn * (int32_t)p->k_list[d + dim * ik];
+        }
+    }
+    P.total = total;
+
+    // momentum list in the reference order
+    std::vector<int64_t> moms;   // [nsec * dim]
+    int64_t Ntot = 0;
+    for (int c = 0; c < ncc; ++c) Ntot += N_each[c];
+    if (nmom >= 0) {
+        for (int s = 0; s < nmom; ++s) {
+            int64_t r[3];
+            for (int d = 0; d < dim; ++d)
+                r[d] = p->Gk[d] == 0 ? momentum_list[s * dim + d] : jmod(momentum_list[s * dim + d], p->Gk[d]);
+            bool dup = false;
+            for (size_t u = 0; u < moms.size() / dim && !dup; ++u) {
+                bool eq = true;
+                for (int d = 0; d < dim; ++d) eq = eq && moms[u * dim + d] == r[d];
+                dup = eq;
+            }
+            if (!dup) moms.insert(moms.end(), r, r + dim);
+        }
+    } else {
+        int64_t lo[3], cnt[3];
+        int64_t nsec = 1;
+        for (int d = 0; d < dim; ++d) {
+            if (p->Gk[d] == 0) {
+                int64_t mn = INT64_MAX, mx = INT64_MIN;
+                for (int i = 0; i < Nk; ++i) { mn = std::min(mn, p->k_list[d + dim * i]); mx = std::max(mx, p->k_list[d + dim * i]); }
+                lo[d] = mn * Ntot;
+                cnt[d] = std::max<int64_t>(0, mx * Ntot - mn * Ntot + 1);
+            } else {
+                lo[d] = 0;
+                cnt[d] = p->Gk[d];
+            }
+            nsec *= cnt[d];
+        }
+        MOMED_REQUIRE(nsec <= (1 << 20), MOMED_EINVAL, "too many momentum sectors");
+        for (int64_t s = 0; s < nsec; ++s) {
+            int64_t r = s;
+            for (int d = 0; d < dim; ++d) { moms.push_back(lo[d] + r % cnt[d]); r /= cnt[d]; }
+        }
+    }
+    const int64_t nsec = (int64_t)moms.size() / dim;
+
+    // box of reachable (residue or raw) momenta and its sector table
+    int64_t box_n = 1;
+    for (int d = 0; d < dim; ++d) {
+        if (p->Gk[d] != 0) { P.box_lo[d] = 0; P.box_ext[d] = (int32_t)p->Gk[d]; }
+        else {
+            int64_t lo = 0, hi = 0;
+            for (int c = 0; c < ncc; ++c) {
+                std::vector<int64_t> v;
+                for (int i = 0; i < P.comp[c].len; ++i) v.push_back(P.kv[P.comp[c].shift + P.comp[c].pos[i]][d]);
+                std::sort(v.begin(), v.end());
+                for (int i = 0; i < P.comp[c].t && i < (int)v.size(); ++i) { lo += v[i]; hi += v[v.size() - 1 - i]; }
+            }
+            P.box_lo[d] = (int32_t)lo;
+            P.box_ext[d] = (int32_t)(hi - lo + 1);
+        }
+        box_n *= P.box_ext[d];
+    }
+    MOMED_REQUIRE(box_n <= (1 << 24), MOMED_EINVAL, "momentum box too large");
+    std::vector<int32_t> sec_of(box_n, -1);
+    for (int64_t s = 0; s < nsec; ++s) {
+        int64_t idx = 0, stride = 1;
+        bool in = true;
+        for (int d = 0; d < dim; ++d) {
+            int64_t v = moms[s * dim + d] - P.box_lo[d];
+            if (v < 0 || v >= P.box_ext[d]) { in = false; break; }
+            idx += v * stride;
+            stride *= P.box_ext[d];
+        }
+        if (in) sec_of[idx] = (int32_t)s;
+    }
+
+    cudaStream_t st = h->stream;
+    DevBuf<int32_t> d_sec;
+    d_sec.resize(box_n);
+    MOMED_CUDA_TRY(cudaMemcpyAsync(d_sec.p, sec_of.data(), box_n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    P.sec_of = d_sec.p;
+    std::vector<uint64_t> hb(65 * 65, 0);
+    for (int n = 0; n <= 64; ++n)
+        for (int k = 0; k <= n; ++k) hb[n * 65 + k] = (uint64_t)hbinom(n, k);
+    DevBuf<uint64_t> d_binom;
+    d_binom.resize(65 * 65);
+    MOMED_CUDA_TRY(cudaMemcpyAsync(d_binom.p, hb.data(), hb.size() * 8, cudaMemcpyHostToDevice, st));
+    P.binom = d_binom.p;
+
+    Enumeration& E = h->enumer;
+    E.dim = dim;
+    E.sizes.assign(nsec, 0);
+    E.offsets.assign(nsec + 1, 0);
+    E.sector_k.clear();
+    std::vector<std::vector<int64_t>> block_counts;
+    int nblocks = 1;
+    if (total > 0) {
+        int64_t threads_target = (int64_t)148 * 2048;
+        P.chunk = std::max<int64_t>(16, (total + threads_target - 1) / threads_target);
+        int64_t nthreads = (total + P.chunk - 1) / P.chunk;
+        nblocks = (int)((nthreads + kThreads - 1) / kThreads);
+    }
+    // pass 1: counts per window of sectors
+    std::vector<int64_t> counts(nsec * (int64_t)nblocks, 0);   // [sector][block]
+    if (total > 0) {
+        DevBuf<int32_t> d_cnt;
+        d_cnt.resize((size_t)kSecWin * nblocks);
+        std::vector<int32_t> hc((size_t)kSecWin * nblocks);
+        for (int64_t w0 = 0; w0 < nsec; w0 += kSecWin) {
+            int nwin = (int)std::min<int64_t>(kSecWin, nsec - w0);
+            k_enum_count<<<nblocks, kThreads, 0, st>>>(P, (int)w0, nwin, d_cnt.p);
+            MOMED_CUDA_TRY(cudaGetLastError());
+            MOMED_CUDA_TRY(cudaMemcpyAsync(hc.data(), d_cnt.p, (size_t)nwin * nblocks * 4, cudaMemcpyDeviceToHost, st));
+            MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+            for (int i = 0; i < nwin; ++i)
+                for (int b = 0; b < nblocks; ++b) counts[(w0 + i) * nblocks + b] = hc[(size_t)i * nblocks + b];
+        }
+    }
+    // sector sizes and block offsets (sector-major concatenation)
+    std::vector<int64_t> offs(counts.size(), 0);
+    int64_t run = 0;
+    for (int64_t s = 0; s < nsec; ++s) {
+        E.offsets[s] = run;
+        for (int b = 0; b < nblocks; ++b) { offs[s * nblocks + b] = run; run += counts[s * nblocks + b]; }
+        E.sizes[s] = run - E.offsets[s];
+    }
+    E.offsets[nsec] = run;
+    E.states.release();
+    if (run > 0) {
+        E.states.resize(run);
+        DevBuf<int64_t> d_off;
+        d_off.resize((size_t)kSecWin * nblocks);
+        for (int64_t w0 = 0; w0 < nsec; w0 += kSecWin) {
+            int nwin = (int)std::min<int64_t>(kSecWin, nsec - w0);
+            MOMED_CUDA_TRY(cudaMemcpyAsync(d_off.p, offs.data() + w0 * nblocks, (size_t)nwin * nblocks * 8,
+                                           cudaMemcpyHostToDevice, st));
+            k_enum_write<<<nblocks, kThreads, 0, st>>>(P, (int)w0, nwin, d_off.p, E.states.p);
+            MOMED_CUDA_TRY(cudaGetLastError());
+            MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+    }
+    // drop empty sectors (momentum_decomposition.jl:408-410)
+    std::vector<int64_t> ks, sz, of;
+    for (int64_t s = 0; s < nsec; ++s) {
+        if (E.sizes[s] == 0) continue;
+        ks.insert(ks.end(), moms.begin() + s * dim, moms.begin() + (s + 1) * dim);
+        sz.push_back(E.sizes[s]);
+        of.push_back(E.offsets[s]);
+    }
+    of.push_back(run);
+    E.sector_k = ks;
+    E.sizes = sz;
+    E.offsets = of;
+    MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+}
+
+}  // namespace momed

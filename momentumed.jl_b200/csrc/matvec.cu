@@ -1,0 +1,446 @@
+// Kernel (b): matrix-free Hamiltonian map y = H x over the Hermitian-completed
+// scatter list.
+//
+// Reference: ka_linearmap_kernel! (MomentumED/src/method/gpu_interface.jl:128-163)
+// gives every row all N_scat terms and binary-searches each hit; it computes
+// conj(H) x because it treats the row state as the term's input.  The CPU map
+// (linear_map.jl:100-118, with mbs_out * scat from EDCore/src/multiplication.jl:55-69)
+// computes H x, and that is what this kernel computes:
+//
+//   for row i with state s, for every term (amp, in, out, pm) with out within s:
+//     mid = s & ~out;  skip if mid & in;  t = mid | in
+//     sign = 1 - 2 (popcount(mid & pm) & 1);  j = index(t) (dropped if absent)
+//     y[i] += sign * amp * x[j]
+//
+// Layout and schedule (B200):
+//   - one warp per row, rows grid-strided so neighbouring warps work on
+//     neighbouring (similar) states and their x gathers share L2 lines;
+//   - terms are regrouped by `out`; a row only visits the groups whose `out`
+//     it contains, found by table lookup on its occupied orbitals (one-body)
+//     and orbital pairs (two-body): ~Ne + Ne(Ne-1)/2 lookups instead of N_scat
+//     mask tests;
+//   - the candidate terms of a batch of groups are flattened and dealt to the
+//     32 lanes, so work stays balanced however uneven the groups are;
+//   - the index of a target is two independent table reads (index.cuh);
+//   - lanes accumulate privately and reduce with shuffles: no atomics.
+#include <algorithm>
+
+#include "index.cuh"
+
+namespace momed {
+
+namespace {
+
+constexpr int kWarps = 8;          // warps per block (256 threads)
+constexpr unsigned kFull = 0xffffffffu;
+
+template <typename R> struct Cx;
+template <> struct Cx<double> { using T = double2; };
+template <> struct Cx<float> { using T = float2; };
+
+struct WarpScratch {
+    uint64_t out[32];
+    int32_t start[32];
+    int32_t pref[33];
+};
+
+template <typename R> struct HitScratch {
+    uint32_t j[32];
+    typename Cx<R>::T a[32];
+    typename Cx<R>::T b[32];
+};
+
+__device__ __forceinline__ double2 load_amp(const double2* p, int t) { return __ldg(p + t); }
+__device__ __forceinline__ float2 load_amp(const float2* p, int t) { return __ldg(p + t); }
+
+template <typename R> __device__ __forceinline__ const typename Cx<R>::T* amp_a(const OpView& ov);
+template <> __device__ __forceinline__ const double2* amp_a<double>(const OpView& ov) { return ov.t_amp; }
+template <> __device__ __forceinline__ const float2* amp_a<float>(const OpView& ov) { return ov.t_amp32; }
+template <typename R> __device__ __forceinline__ const typename Cx<R>::T* amp_b(const OpView& ov);
+template <> __device__ __forceinline__ const double2* amp_b<double>(const OpView& ov) { return ov.t_ampb; }
+template <> __device__ __forceinline__ const float2* amp_b<float>(const OpView& ov) { return ov.t_ampb32; }
+
+struct SharedTables {
+    uint32_t binom[33 * 33];
+    uint32_t base_hi[34];
+    uint32_t base_lo[34];
+};
+
+__device__ __forceinline__ void stage_tables(SharedTables& sh, const IndexView& iv) {
+    for (int i = threadIdx.x; i < 33 * 33; i += blockDim.x) sh.binom[i] = __ldg(iv.binom + i);
+    if (threadIdx.x < 34) {
+        sh.base_hi[threadIdx.x] = iv.hi.base[threadIdx.x];
+        sh.base_lo[threadIdx.x] = iv.lo.base[threadIdx.x];
+    }
+    __syncthreads();
+}
+
+// Position of the l-th (0-based) set bit of s, for l = lane and l = lane + 32.
+__device__ __forceinline__ void occupied_positions(uint64_t s, int lane, int& pos0, int& pos1) {
+    uint32_t lo32 = (uint32_t)s, hi32 = (uint32_t)(s >> 32);
+    int clo = __popc(lo32);
+    pos0 = lane < clo ? (int)__fns(lo32, 0, lane + 1) : 32 + (int)__fns(hi32, 0, lane - clo + 1);
+    int l1 = lane + 32;
+    pos1 = l1 < clo ? (int)__fns(lo32, 0, l1 + 1) : 32 + (int)__fns(hi32, 0, l1 - clo + 1);
+}
+
+__device__ __forceinline__ int pos_of(int l, int pos0, int pos1) {
+    int a = __shfl_sync(kFull, pos0, l & 31);
+    int b = __shfl_sync(kFull, pos1, l & 31);
+    return l < 32 ? a : b;
+}
+
+// p-th pair (u < v) in the order (0,1), (0,2), (1,2), (0,3), ...: v(v-1)/2 <= p
+__device__ __forceinline__ void pair_of(int p, int& u, int& v) {
+    int w = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)p)) * 0.5f);
+    while (w * (w - 1) / 2 > p) --w;
+    while ((w + 1) * w / 2 <= p) ++w;
+    v = w;
+    u = p - w * (w - 1) / 2;
+}
+
+// Visit every candidate group of state s: calls f(g) once per lane per batch of 32 groups
+// (g = -1 for idle lanes); f must be warp-collective.
+template <typename F>
+__device__ __forceinline__ void for_each_group_batch(uint64_t s, const OpView& ov, F&& f) {
+    const int lane = threadIdx.x & 31;
+    int pos0, pos1;
+    occupied_positions(s, lane, pos0, pos1);
+    const int ne = __popcll(s);
+    for (int b0 = 0; b0 < ne; b0 += 32) {                       // one-body groups
+        int l = b0 + lane;
+        int g = (l < ne) ? __ldg(ov.single + (b0 == 0 ? pos0 : pos1)) : -1;
+        f(g);
+    }
+    const int np = ne * (ne - 1) / 2;
+    for (int b0 = 0; b0 < np; b0 += 32) {                       // two-body groups
+        int p = b0 + lane;
+        int u = 0, v = 1;
+        if (p < np) pair_of(p, u, v);
+        int a = pos_of(u, pos0, pos1);
+        int b = pos_of(v, pos0, pos1);
+        int g = (p < np) ? __ldg(ov.pair + a * 64 + b) : -1;
+        f(g);
+    }
+    for (int b0 = 0; b0 < ov.ngeneric; b0 += 32) {             // other groups: direct test
+        int q = b0 + lane;
+        int g = -1;
+        if (q < ov.ngeneric) {
+            g = __ldg(ov.generic + q);
+            uint64_t om = __ldg(ov.g_out + g);
+            if ((s & om) != om) g = -1;
+        }
+        f(g);
+    }
+}
+
+// Compact the batch's groups into warp scratch; returns the flattened term count.
+__device__ __forceinline__ int stage_batch(int g, const OpView& ov, WarpScratch& ws) {
+    const int lane = threadIdx.x & 31;
+    unsigned m = __ballot_sync(kFull, g >= 0);
+    if (m == 0) return 0;
+    int slot = __popc(m & ((1u << lane) - 1u));
+    int sz = 0;
+    if (g >= 0) {
+        int st = __ldg(ov.g_start + g);
+        sz = __ldg(ov.g_start + g + 1) - st;
+        ws.out[slot] = __ldg(ov.g_out + g);
+        ws.start[slot] = st;
+    }
+    int incl = sz;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (g >= 0) ws.pref[slot + 1] = incl;
+    if (lane == 0) ws.pref[0] = 0;
+    int total = __shfl_sync(kFull, incl, 31);
+    __syncwarp();
+    return total;
+}
+
+// Evaluate the term at flattened position f of the staged batch: returns j (or -1) and the sign.
+__device__ __forceinline__ int64_t eval_term(int f, int& gi, uint64_t s, int64_t row, const OpView& ov,
+                                             const IndexView& iv, const WarpScratch& ws, const SharedTables& sh,
+                                             int& t, bool& neg) {
+    while (ws.pref[gi + 1] <= f) ++gi;
+    t = ws.start[gi] + (f - ws.pref[gi]);
+    uint64_t om = ws.out[gi];
+    uint64_t tin = __ldg(ov.t_in + t);
+    uint64_t mid = s & ~om;
+    neg = false;
+    if ((mid & tin) != 0) return -1;
+    if (tin == om) return row;                                    // diagonal term
+    neg = (__popcll(mid & __ldg(ov.t_pm + t)) & 1) != 0;
+    return lookup_index(iv, mid | tin, sh.base_hi, sh.base_lo, sh.binom);
+}
+
+template <typename R, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+         const R* __restrict__ u_ptr, int64_t rows) {
+    using C2 = typename Cx<R>::T;
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpScratch& ws = s_ws[wid];
+    const R u = HAS_B ? *u_ptr : R(0);
+    const C2* __restrict__ A = amp_a<R>(ov);
+    const C2* __restrict__ B = amp_b<R>(ov);
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        R ar = 0, ai = 0;
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                if (f < total) {
+                    int t;
+                    bool neg;
+                    int64_t j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
+                    if (j >= 0) {
+                        C2 a = load_amp(A, t);
+                        if (HAS_B) {
+                            C2 b = load_amp(B, t);
+                            a.x += u * b.x;
+                            a.y += u * b.y;
+                        }
+                        C2 xv = x[j];
+                        R pr = a.x * xv.x - a.y * xv.y;
+                        R pi = a.x * xv.y + a.y * xv.x;
+                        if (neg) { ar -= pr; ai -= pi; } else { ar += pr; ai += pi; }
+                    }
+                }
+            }
+            __syncwarp();
+        });
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ar += __shfl_xor_sync(kFull, ar, o);
+            ai += __shfl_xor_sync(kFull, ai, o);
+        }
+        if (lane == 0) {
+            C2 out;
+            out.x = ar;
+            out.y = ai;
+            y[row] = out;
+        }
+    }
+}
+
+// Counts hits (targets found) and misses (targets outside the basis) without touching x.
+__global__ void __launch_bounds__(kWarps * 32)
+k_count(IndexView iv, OpView ov, unsigned long long* hits, unsigned long long* misses, int64_t rows) {
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpScratch& ws = s_ws[wid];
+    unsigned long long nh = 0, nm = 0;
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                if (f < total) {
+                    int t;
+                    bool neg;
+                    // decide "mask-compatible" separately from "found"
+                    while (ws.pref[gi + 1] <= f) ++gi;
+                    t = ws.start[gi] + (f - ws.pref[gi]);
+                    uint64_t om = ws.out[gi];
+                    uint64_t tin = __ldg(ov.t_in + t);
+                    uint64_t mid = s & ~om;
+                    (void)neg;
+                    if ((mid & tin) == 0) {
+                        int64_t j = (tin == om) ? row : lookup_index(iv, mid | tin, sh.base_hi, sh.base_lo, sh.binom);
+                        if (j >= 0) ++nh; else ++nm;
+                    }
+                }
+            }
+            __syncwarp();
+        });
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        nh += __shfl_xor_sync(kFull, nh, o);
+        nm += __shfl_xor_sync(kFull, nm, o);
+    }
+    if (lane == 0) {
+        if (nh) atomicAdd(hits, nh);
+        if (nm) atomicAdd(misses, nm);
+    }
+}
+
+// Block map: NB right-hand sides interleaved as x[row * NB + b], operator H_b = A + u[b] B.
+// Lanes first evaluate 32 candidate terms (index lookup once per hit), then sweep the
+// compacted hits with lane = right-hand side, so every gather reads NB contiguous values.
+template <typename R, int NB, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_block_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+               const R* __restrict__ u, int64_t rows) {
+    using C2 = typename Cx<R>::T;
+    static_assert(NB >= 1 && NB <= 32 && (NB & (NB - 1)) == 0, "NB must be a power of two <= 32");
+    constexpr int NSUB = 32 / NB;
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    __shared__ HitScratch<R> s_hits[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int r = lane % NB, sub = lane / NB;
+    WarpScratch& ws = s_ws[wid];
+    HitScratch<R>& hs = s_hits[wid];
+    const R ur = HAS_B ? u[r] : R(0);
+    const C2* __restrict__ A = amp_a<R>(ov);
+    const C2* __restrict__ B = amp_b<R>(ov);
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        R ar = 0, ai = 0;
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                int64_t j = -1;
+                int t = 0;
+                bool neg = false;
+                if (f < total) j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
+                unsigned hm = __ballot_sync(kFull, j >= 0);
+                if (j >= 0) {
+                    int k = __popc(hm & ((1u << lane) - 1u));
+                    C2 a = load_amp(A, t);
+                    C2 b;
+                    b.x = 0; b.y = 0;
+                    if (HAS_B) b = load_amp(B, t);
+                    if (neg) { a.x = -a.x; a.y = -a.y; b.x = -b.x; b.y = -b.y; }
+                    hs.j[k] = (uint32_t)j;
+                    hs.a[k] = a;
+                    hs.b[k] = b;
+                }
+                __syncwarp();
+                const int nh = __popc(hm);
+#pragma unroll 4
+                for (int k = sub; k < nh; k += NSUB) {
+                    uint32_t jj = hs.j[k];
+                    C2 a = hs.a[k];
+                    if (HAS_B) {
+                        C2 b = hs.b[k];
+                        a.x += ur * b.x;
+                        a.y += ur * b.y;
+                    }
+                    C2 xv = x[(int64_t)jj * NB + r];
+                    ar += a.x * xv.x - a.y * xv.y;
+                    ai += a.x * xv.y + a.y * xv.x;
+                }
+                __syncwarp();
+            }
+        });
+#pragma unroll
+        for (int o = NB; o < 32; o <<= 1) {
+            ar += __shfl_xor_sync(kFull, ar, o);
+            ai += __shfl_xor_sync(kFull, ai, o);
+        }
+        if (sub == 0) {
+            C2 out;
+            out.x = ar;
+            out.y = ai;
+            y[row * NB + r] = out;
+        }
+    }
+}
+
+template <typename K>
+int persistent_grid(K kernel, int64_t rows) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, 0);
+    if (per_sm <= 0) per_sm = 1;
+    int64_t need = (rows + kWarps - 1) / kWarps;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * per_sm));
+}
+
+}  // namespace
+
+void launch_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y, const double* u_scale,
+                        int64_t rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    if (u_scale && ov.t_ampb) {
+        auto k = k_matvec<double, true>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u_scale, rows);
+    } else {
+        auto k = k_matvec<double, false>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
+    }
+    MOMED_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y, const float* u_scale,
+                       int64_t rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    if (u_scale && ov.t_ampb32) {
+        auto k = k_matvec<float, true>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u_scale, rows);
+    } else {
+        auto k = k_matvec<float, false>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
+    }
+    MOMED_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_count_hits(const IndexView& iv, const OpView& ov, unsigned long long* hits, unsigned long long* misses,
+                       int64_t rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    k_count<<<persistent_grid(k_count, rows), kWarps * 32, 0, st>>>(iv, ov, hits, misses, rows);
+    MOMED_CUDA_TRY(cudaGetLastError());
+}
+
+template <typename R>
+static void block_dispatch(const IndexView& iv, const OpView& ov, const typename Cx<R>::T* x, typename Cx<R>::T* y,
+                           const R* u, int32_t nb, int64_t rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
+#define MOMED_BLK(NBV)                                                                                   \
+    case NBV:                                                                                            \
+        if (hb) {                                                                                        \
+            auto k = k_block_matvec<R, NBV, true>;                                                       \
+            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);                  \
+        } else {                                                                                         \
+            auto k = k_block_matvec<R, NBV, false>;                                                      \
+            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);                  \
+        }                                                                                                \
+        break;
+    switch (nb) {
+        MOMED_BLK(1)
+        MOMED_BLK(2)
+        MOMED_BLK(4)
+        MOMED_BLK(8)
+        MOMED_BLK(16)
+        MOMED_BLK(32)
+        default:
+            throw Error{MOMED_EINVAL, "block width must be a power of two <= 32"};
+    }
+#undef MOMED_BLK
+    MOMED_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y, const float* u,
+                             int32_t nb, int64_t rows, cudaStream_t st) {
+    block_dispatch<float>(iv, ov, x, y, u, nb, rows, st);
+}
+void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y, const double* u,
+                              int32_t nb, int64_t rows, cudaStream_t st) {
+    block_dispatch<double>(iv, ov, x, y, u, nb, rows, st);
+}
+
+}  // namespace momed

@@ -1,0 +1,223 @@
+// Internal declarations of libmomed_b200: the handle, device data layouts and
+// the kernels' host-side launchers.  Not part of the public ABI (include/momed.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/momed.h"
+
+namespace momed {
+
+// ---------------------------------------------------------------- errors
+struct Error {
+    int code;
+    std::string msg;
+};
+
+#define MOMED_CUDA_TRY(expr)                                                                 \
+    do {                                                                                     \
+        cudaError_t _e = (expr);                                                             \
+        if (_e != cudaSuccess) {                                                             \
+            throw ::momed::Error{MOMED_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)}; \
+        }                                                                                    \
+    } while (0)
+
+#define MOMED_REQUIRE(cond, code, text)                       \
+    do {                                                      \
+        if (!(cond)) throw ::momed::Error{(code), (text)};    \
+    } while (0)
+
+// ---------------------------------------------------------------- device buffer
+// Owning device allocation (cudaMalloc / cudaFree); moves only.
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) { release(); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    void resize(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) return;
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            throw Error{MOMED_ENOMEM, std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
+                                          " bytes failed: " + cudaGetErrorString(e)};
+        }
+        n = count;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ---------------------------------------------------------------- index tables
+// A basis state is split into a high part (bits >= L) and a low part (bits < L).
+// Each part maps to a table slot either directly (slot = bits) or through its
+// combinadic rank: slot = base[popcount - cmin] + sum_k C(pos_k, k) over the set
+// bits (colex rank among patterns of equal popcount).
+enum PartMode : int32_t { PART_DIRECT = 0, PART_COMBINADIC = 1 };
+
+struct PartDesc {
+    int32_t shift;      // first bit of the part
+    int32_t width;      // bits in the part (<= 32 for combinadic, <= 24 direct)
+    int32_t mode;       // PartMode
+    int32_t cmin, cmax; // popcount range present in the basis
+    uint32_t size;      // table entries
+    uint32_t base[34];  // base[c - cmin] for combinadic
+};
+
+enum IndexMode : int32_t { INDEX_RANKED = 0, INDEX_CHECKED = 1, INDEX_SEARCH = 2 };
+
+static constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+
+struct IndexView {       // passed by value to kernels
+    const uint64_t* basis;
+    int64_t n;
+    const uint32_t* off_hi;   // [hi.size]  first basis index of each high pattern (kInvalid: absent)
+    const uint32_t* rank_lo;  // [lo.size]  rank of the low pattern inside its high group
+    PartDesc hi, lo;
+    int32_t mode;             // IndexMode
+    const uint32_t* binom;    // [33 * 33] C(n, k) for n, k <= 32
+};
+
+// ---------------------------------------------------------------- operator terms
+// The Hermitian-completed term list regrouped by the creation mask `out`: a row
+// state s meets the terms of group g only when out_g is a subset of s.  Groups
+// with |out| = 1 or 2 are found by table lookup; other groups are tested directly.
+struct OpView {
+    int32_t ngroups;
+    const uint64_t* g_out;     // [ngroups]
+    const int32_t* g_start;    // [ngroups + 1] term ranges
+    const int32_t* single;     // [64]        group of out = {a} or -1
+    const int32_t* pair;       // [64 * 64]   group of out = {a, b}, a < b, or -1
+    const int32_t* generic;    // [ngeneric]  other groups
+    int32_t ngeneric;
+    const uint64_t* t_in;      // [nterms]
+    const uint64_t* t_pm;      // [nterms]
+    const double2* t_amp;      // [nterms] c128 (A part)
+    const float2* t_amp32;     // [nterms] c64  (A part)
+    const double2* t_ampb;     // [nterms] c128 B part (parametrised operators) or null
+    const float2* t_ampb32;    // [nterms] c64 B part or null
+    int32_t nterms;
+    int32_t max_groups_per_row;   // bound on candidate groups of one row
+};
+
+// ---------------------------------------------------------------- handle
+struct Enumeration {
+    int32_t dim = 0;
+    std::vector<int64_t> sector_k;     // [nsec * dim]
+    std::vector<int64_t> sizes;        // [nsec]
+    std::vector<int64_t> offsets;      // [nsec + 1]
+    DevBuf<uint64_t> states;           // concatenated sectors
+};
+
+struct Operator {
+    int64_t nterms = 0;
+    int32_t ngroups = 0, ngeneric = 0, max_groups = 0;
+    bool has_b = false;
+    DevBuf<uint64_t> g_out, t_in, t_pm;
+    DevBuf<int32_t> g_start, single, pair, generic;
+    DevBuf<double2> amp, ampb;
+    DevBuf<float2> amp32, ampb32;
+    OpView view() const;
+};
+
+struct Index {
+    int32_t mode = INDEX_SEARCH;
+    PartDesc hi{}, lo{};
+    DevBuf<uint32_t> off_hi, rank_lo;
+    int64_t misses_checked = -1;   // misses found by the validation pass (-1: not run)
+};
+
+}  // namespace momed
+
+struct momed_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    int64_t hbm_budget = 0;
+
+    int64_t n = 0;                         // basis size
+    momed::DevBuf<uint64_t> basis;
+    uint64_t basis_or = 0;                 // OR of all basis states
+    momed::Index index;
+    bool index_dirty = true;
+    uint64_t index_bits = 0;               // bits the index tables cover
+    momed::Operator op;
+    bool op_set = false;
+    bool op_validated = false;
+    uint64_t op_mask_or = 0;               // OR of all term masks
+    int64_t nnz = 0;                       // (row, term) hits of the validated operator
+    momed::DevBuf<double> u_dev;           // parameter u of H(u) = A + u B
+    momed::DevBuf<float> u_dev32;
+    momed::DevBuf<uint32_t> binom;         // C(n, k), n, k <= 32
+
+    momed::Enumeration enumer;
+
+    // scratch reused across calls
+    momed::DevBuf<double2> xbuf, ybuf;
+    momed::DevBuf<float2> xbuf32, ybuf32;
+    momed::DevBuf<unsigned long long> counters;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_kernel_ms = 0.f;
+};
+
+namespace momed {
+
+// binomial table C(n, k), n, k in [0, 32], on the device (built once per process per device)
+const uint32_t* device_binomials();
+
+// index.cu
+void build_index(momed_handle* h);
+IndexView index_view(const momed_handle* h);
+int64_t validate_operator(momed_handle* h);   // counts (row, term) targets missing from the basis
+
+// matvec.cu
+void launch_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y,
+                        const double* u_scale, int64_t rows, cudaStream_t st);
+void launch_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y,
+                       const float* u_scale, int64_t rows, cudaStream_t st);
+void launch_count_hits(const IndexView& iv, const OpView& ov, unsigned long long* hits,
+                       unsigned long long* misses, int64_t rows, cudaStream_t st);
+// block matvec: nb right-hand sides interleaved [row][nb], H_u = A + u[b] B
+void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y,
+                             const float* u, int32_t nb, int64_t rows, cudaStream_t st);
+void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y,
+                              const double* u, int32_t nb, int64_t rows, cudaStream_t st);
+
+// operator.cpp-side (in abi.cu)
+void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, const uint64_t* in,
+                     const uint64_t* out, const uint64_t* parity, int64_t nscat);
+
+// enumerate.cu
+void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each, int ncc, const int64_t* mask,
+                     int mlen, const int64_t* momentum_list, int nmom);
+
+// small dense symmetric eigensolver (host, FP64): A n x n row-major (destroyed),
+// eigenvalues ascending in w, eigenvectors as columns of V (row-major n x n)
+void symeig(int n, double* A, double* w, double* V);
+
+}  // namespace momed
+
+// Lanczos drivers (lanczos.cu)
+int momed_eigsolve_impl(momed_handle* h, const momed_solve_opts* o, const double* vec0, double* vals, double* resid,
+                        void* vecs, momed_info* info);
+int momed_batch_solve_impl(momed_handle* h, const momed_solve_opts* o, const double* u, int32_t nu, double* vals,
+                           double* resid, double* vecs, momed_info* info);

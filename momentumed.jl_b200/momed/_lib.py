@@ -1,0 +1,251 @@
+"""ctypes bindings of libmomed_b200.so (include/momed.h).
+
+The shared library is built in-tree by ``make -C momentumed.jl_b200`` (or
+``__graft_entry__.build()``) into ``momentumed.jl_b200/lib/``.  There is no
+CPU fallback: if the library or a CUDA device is missing, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libmomed_b200.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ENOTCONV, ETIMEOUT, ESTATE, ENODEV = range(8)
+C128, C64 = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+
+class MomedError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"momed error {code}: {msg}")
+        self.code = code
+
+
+class NotConverged(MomedError):
+    pass
+
+
+class Para(C.Structure):
+    _fields_ = [("dim", C.c_int32), ("Nk", C.c_int32), ("Nc_mix", C.c_int32), ("Nc_conserve", C.c_int32),
+                ("k_list", C.POINTER(C.c_int64)), ("Gk", C.POINTER(C.c_int64))]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("nev", C.c_int32), ("krylovdim", C.c_int32), ("maxiter", C.c_int32), ("precision", C.c_int32),
+                ("tol", C.c_double), ("seed", C.c_uint64), ("want_vectors", C.c_int32),
+                ("vecs_on_device", C.c_int32)]
+
+
+class Info(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("restarts", C.c_int32), ("matvecs", C.c_int64),
+                ("matvecs_fp64", C.c_int64), ("seconds", C.c_double)]
+
+
+_lib = None
+
+# every symbol include/momed.h declares, with its ctypes signature
+SIGNATURES = {
+    "momed_version": (C.c_char_p, []),
+    "momed_create": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "momed_destroy": (C.c_int, [C.c_void_p]),
+    "momed_last_error": (C.c_char_p, [C.c_void_p]),
+    "momed_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "momed_set_hbm_budget": (C.c_int, [C.c_void_p, C.c_int64]),
+    "momed_enumerate_basis": (C.c_int, [C.c_void_p, C.POINTER(Para), C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                                        C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "momed_enumeration_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
+    "momed_select_sector": (C.c_int, [C.c_void_p, C.c_int64]),
+    "momed_set_basis": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
+    "momed_set_scatter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
+    "momed_set_scatter_pair": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_int64]),
+    "momed_set_param": (C.c_int, [C.c_void_p, C.c_double]),
+    "momed_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
+    "momed_eigsolve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.POINTER(Info)]),
+    "momed_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_int32, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.POINTER(Info)]),
+    "momed_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "momed_last_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+}
+
+
+def lib():
+    """Load the library (raises when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise MomedError(ENODEV, f"{LIB_PATH} is missing: build it with `make -C momentumed.jl_b200` "
+                                     "(this backend has no CPU fallback)")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def version() -> str:
+    return lib().momed_version().decode()
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Handle:
+    """One device context of the library: a working basis, an operator and scratch buffers."""
+
+    def __init__(self, device: int = 0):
+        L = lib()
+        h = C.c_void_p()
+        rc = L.momed_create(device, C.byref(h))
+        if rc != OK:
+            raise MomedError(rc, L.momed_last_error(None).decode())
+        self._h = h
+        self.n = 0
+
+    # ---------------------------------------------------------------- plumbing
+    def _check(self, rc: int):
+        if rc == OK:
+            return
+        msg = lib().momed_last_error(self._h).decode()
+        if rc == ENOTCONV:
+            raise NotConverged(rc, msg or "not converged")
+        raise MomedError(rc, msg)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().momed_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr: int):
+        self._check(lib().momed_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    # ---------------------------------------------------------------- basis
+    def enumerate_basis(self, k_list: np.ndarray, Gk, Nc_mix: int, Nc_conserve: int, N_each, mask=None,
+                        momentum_list=None):
+        k_list = np.asarray(k_list, np.int64)
+        dim, Nk = k_list.shape
+        kl = np.ascontiguousarray(k_list.T).reshape(-1)
+        g = np.asarray(Gk, np.int64)
+        para = Para(dim, Nk, Nc_mix, Nc_conserve, kl.ctypes.data_as(C.POINTER(C.c_int64)),
+                    g.ctypes.data_as(C.POINTER(C.c_int64)))
+        ne = np.asarray(N_each, np.int64)
+        marr = None if mask is None else np.asarray(sorted(mask), np.int64)
+        mom = None if momentum_list is None else np.asarray(momentum_list, np.int64).reshape(-1)
+        nsec, ntot = C.c_int64(), C.c_int64()
+        self._check(lib().momed_enumerate_basis(self._h, C.byref(para), _p(ne), len(ne), _p(marr),
+                                                -1 if marr is None else len(marr), _p(mom),
+                                                -1 if mom is None else len(mom) // dim, C.byref(nsec),
+                                                C.byref(ntot)))
+        ks = np.zeros(max(nsec.value * dim, 1), np.int64)
+        sizes = np.zeros(max(nsec.value, 1), np.int64)
+        basis = np.zeros(max(ntot.value, 1), np.uint64)
+        self._check(lib().momed_enumeration_copy(self._h, _p(ks), _p(sizes), _p(basis), 0))
+        out, off = [], 0
+        for s in range(nsec.value):
+            out.append((tuple(int(v) for v in ks[s * dim:(s + 1) * dim]), basis[off:off + sizes[s]]))
+            off += int(sizes[s])
+        return out
+
+    def select_sector(self, s: int, n: int):
+        self._check(lib().momed_select_sector(self._h, s))
+        self.n = n
+
+    def set_basis(self, basis, on_device: bool = False, n: int | None = None):
+        if on_device:
+            self._check(lib().momed_set_basis(self._h, C.c_void_p(basis), n, 1))
+            self.n = n
+        else:
+            b = np.ascontiguousarray(basis, np.uint64)
+            self._check(lib().momed_set_basis(self._h, _p(b), len(b), 0))
+            self.n = len(b)
+
+    # ---------------------------------------------------------------- operator
+    def set_scatter(self, amp: np.ndarray, in_: np.ndarray, out: np.ndarray, parity: np.ndarray | None = None):
+        a = np.ascontiguousarray(amp, np.complex128)
+        i = np.ascontiguousarray(in_, np.uint64)
+        o = np.ascontiguousarray(out, np.uint64)
+        p = None if parity is None else np.ascontiguousarray(parity, np.uint64)
+        self._check(lib().momed_set_scatter(self._h, _p(a), _p(i), _p(o), _p(p), len(a)))
+
+    def set_scatter_pair(self, amp_a, amp_b, in_, out, parity=None):
+        a = np.ascontiguousarray(amp_a, np.complex128)
+        b = np.ascontiguousarray(amp_b, np.complex128)
+        i = np.ascontiguousarray(in_, np.uint64)
+        o = np.ascontiguousarray(out, np.uint64)
+        p = None if parity is None else np.ascontiguousarray(parity, np.uint64)
+        self._check(lib().momed_set_scatter_pair(self._h, _p(a), _p(b), _p(i), _p(o), _p(p), len(a)))
+
+    def set_param(self, u: float):
+        self._check(lib().momed_set_param(self._h, float(u)))
+
+    # ---------------------------------------------------------------- compute
+    def matvec(self, x: np.ndarray) -> np.ndarray:
+        """y = H x with host arrays (complex128 or complex64)."""
+        prec = C64 if x.dtype == np.complex64 else C128
+        x = np.ascontiguousarray(x, np.complex64 if prec == C64 else np.complex128)
+        y = np.empty_like(x)
+        self._check(lib().momed_matvec(self._h, _p(x), _p(y), prec, 0))
+        return y
+
+    def matvec_device(self, x_ptr: int, y_ptr: int, precision: int = C128):
+        self._check(lib().momed_matvec(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), precision, 1))
+
+    def last_kernel_ms(self) -> float:
+        v = C.c_double()
+        self._check(lib().momed_last_kernel_ms(self._h, C.byref(v)))
+        return v.value
+
+    def stats(self):
+        nnz, mode, tb = C.c_int64(), C.c_int32(), C.c_int64()
+        self._check(lib().momed_stats(self._h, C.byref(nnz), C.byref(mode), C.byref(tb)))
+        return {"nnz": nnz.value, "index_mode": mode.value, "table_bytes": tb.value}
+
+    def eigsolve(self, nev: int, krylovdim: int = 30, tol: float = 1e-12, maxiter: int = 100,
+                 vec0: np.ndarray | None = None, seed: int = 0, precision: int = PREC_FP64,
+                 want_vectors: bool = True, raise_on_notconv: bool = False):
+        n = self.n
+        nev_eff = min(nev, n)
+        opts = SolveOpts(nev, krylovdim, maxiter, precision, tol, seed, int(want_vectors), 0)
+        vals = np.zeros(nev_eff)
+        resid = np.zeros(nev_eff)
+        vecs = np.zeros((nev_eff, n), np.complex128) if want_vectors else None
+        v0 = None if vec0 is None else np.ascontiguousarray(vec0, np.complex128)
+        info = Info()
+        rc = lib().momed_eigsolve(self._h, C.byref(opts), _p(v0), _p(vals), _p(resid), _p(vecs), C.byref(info))
+        if rc not in (OK, ENOTCONV) or (rc == ENOTCONV and raise_on_notconv):
+            self._check(rc)
+        return vals, vecs, resid, {"converged": info.converged, "restarts": info.restarts,
+                                   "matvecs": info.matvecs, "matvecs_fp64": info.matvecs_fp64,
+                                   "seconds": info.seconds}
+
+    def batch_solve(self, u: np.ndarray, nev: int, krylovdim: int = 30, tol: float = 1e-12, maxiter: int = 100,
+                    seed: int = 0, precision: int = PREC_MIXED, want_vectors: bool = False):
+        u = np.ascontiguousarray(u, np.float64)
+        n = self.n
+        nev_eff = min(nev, n)
+        opts = SolveOpts(nev, krylovdim, maxiter, precision, tol, seed, int(want_vectors), 0)
+        vals = np.zeros((len(u), nev_eff))
+        resid = np.zeros((len(u), nev_eff))
+        vecs = np.zeros((len(u), nev_eff, n), np.complex128) if want_vectors else None
+        info = Info()
+        rc = lib().momed_batch_solve(self._h, C.byref(opts), _p(u), len(u), _p(vals), _p(resid), _p(vecs),
+                                     C.byref(info))
+        if rc not in (OK, ENOTCONV):
+            self._check(rc)
+        return vals, vecs, resid, {"converged": info.converged, "restarts": info.restarts,
+                                   "matvecs": info.matvecs, "matvecs_fp64": info.matvecs_fp64,
+                                   "seconds": info.seconds}

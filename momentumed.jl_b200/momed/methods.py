@@ -1,0 +1,187 @@
+"""Host mirror of MomentumED's matrix-free methods, backed by libmomed_b200.
+
+  - ``LinearMap`` ........... MomentumED/src/method/linear_map.jl:18-42 (Hermitian completion + sort)
+  - GPU plugin hooks ........ MomentumED/src/method/gpu_interface.jl:13-94
+      GPU_AVAILABLE, DEFAULT_GPU, activate_gpu_device, create_gpu_linearmap,
+      krylov_map_solve, release_gpu_memory
+  - ``EDsolve`` ............. MomentumED/src/MomentumED.jl:375-480 (method=:map, device=:gpu)
+
+The device map computes H x (the CPU LinearMap semantics, linear_map.jl:100-118);
+the reference's KernelAbstractions kernel computes conj(H) x, so its eigenvectors
+are the complex conjugates of these.  Eigenvalues are identical.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib
+from .core import HilbertSubspace, MBOperator, MBS64Vector, ScatterList, hermitian_complete
+
+GPU_AVAILABLE = {"cuda": False, "oneapi": False, "metal": False, "multi_cuda": False, "b200": False}
+DEFAULT_GPU = ["nogpu"]
+GPU_RESTART_CHUNKSIZE = [262144]   # kept for API parity; the device restart needs no chunking
+GPU_MEMORY_MONITOR = [False]
+
+
+def activate_b200(device: int = 0, set_default_gpu: bool = True) -> bool:
+    """Probe the B200 backend (loads the library and opens a device context)."""
+    try:
+        h = _lib.Handle(device)
+        h.close()
+        GPU_AVAILABLE["b200"] = True
+        if set_default_gpu or DEFAULT_GPU[0] == "nogpu":
+            DEFAULT_GPU[0] = "b200"
+    except _lib.MomedError:
+        GPU_AVAILABLE["b200"] = False
+    return GPU_AVAILABLE["b200"]
+
+
+def activate_gpu_device(device: str, set_default_gpu: bool = True):
+    if device not in GPU_AVAILABLE:
+        raise ValueError(f"Unknown GPU {device}. Valid options are: {list(GPU_AVAILABLE)}.")
+    if device in ("b200", "cuda"):
+        return activate_b200(set_default_gpu=set_default_gpu)
+    GPU_AVAILABLE[device] = False
+    return False
+
+
+def _throw_gpu_unavailable(device: str):
+    if GPU_AVAILABLE.get(device, False):
+        return
+    try:
+        activate_gpu_device(device, set_default_gpu=False)
+    except ValueError:
+        pass
+    if GPU_AVAILABLE.get(device, False):
+        return
+    raise ValueError(f"device=:{device} requires functional GPU(s) of the type. "
+                     "Load the required package(s) and verify GPU availability.")
+
+
+class LinearMap:
+    """Matrix-free map: the Hermitian-completed sorted term list over a subspace (linear_map.jl:18-42)."""
+
+    def __init__(self, op: MBOperator, space: HilbertSubspace):
+        et = op.scats.element_type
+        if et not in (np.complex128, np.complex64):
+            raise AssertionError(f"element_type={et}. Use Complex of Float64, Float32.")
+        self.scat_list: ScatterList = hermitian_complete(op)
+        self.space = space
+        self.element_type = et
+
+    @property
+    def size(self):
+        n = len(self.space)
+        return (n, n)
+
+
+class B200LinearMap:
+    """The device map (the role of CuLinearMap, MomentumEDCUDAExt.jl:55-139)."""
+
+    def __init__(self, A: LinearMap, device: int = 0, handle: _lib.Handle | None = None):
+        self.space = A.space
+        self.element_type = A.element_type
+        self.handle = handle or _lib.Handle(device)
+        self.handle.set_basis(A.space.list)
+        s = A.scat_list
+        self.handle.set_scatter(s.amp.astype(np.complex128), s.in_, s.out, s.pm)
+
+    @property
+    def size(self):
+        n = len(self.space)
+        return (n, n)
+
+    @property
+    def eltype(self):
+        return self.element_type
+
+    def __call__(self, x, y=None):
+        prec_dtype = np.complex64 if self.element_type is np.complex64 else np.complex128
+        out = self.handle.matvec(np.asarray(x, prec_dtype))
+        if y is not None:
+            y[...] = out
+            return y
+        return out
+
+    def adjoint(self):
+        return self        # the map of a Hermitian-completed operator is self-adjoint
+
+    def release(self):
+        self.handle.close()
+
+
+def create_gpu_linearmap(A: LinearMap, device: str = "b200") -> B200LinearMap:
+    return B200LinearMap(A)
+
+
+def krylov_map_solve(H: B200LinearMap, N_eigen: int, *, ishermitian: bool = True, vec0=None,
+                     krylovdim: int = 30, tol: float = 1e-12, maxiter: int = 100, seed: int = 0,
+                     precision: str = "fp64", verbosity: int = 0):
+    """Lowest N_eigen eigenpairs (:SR) of the device map; returns (vals, vecs, info)."""
+    if not ishermitian:
+        raise NotImplementedError("the non-Hermitian map is not part of this backend")
+    m = len(H.space)
+    N_eigen = min(N_eigen, m)
+    prec = _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64
+    vals, vecs, resid, info = H.handle.eigsolve(N_eigen, krylovdim=krylovdim, tol=tol, maxiter=maxiter,
+                                                vec0=vec0, seed=seed, precision=prec)
+    info = dict(info)
+    info["residuals"] = resid
+    return vals, [vecs[i] for i in range(len(vals))], info
+
+
+def release_gpu_memory(device: str = "b200", level: int = 2):
+    """Device buffers belong to handles and are freed when a handle closes; nothing to collect."""
+    return None
+
+
+def EDsolve(subspace: HilbertSubspace, Hamiltonian: MBOperator, *, N: int, method: str = "map",
+            device: str = "gpu", showtime: bool = False, ishermitian: bool = True, element_type=None,
+            index_type=np.int32, map_warning_dim: int = 20000, method_info: bool = True, **krylovkit_kwargs):
+    """Lowest N eigenpairs of ``Hamiltonian`` in ``subspace`` (MomentumED.jl:375-480, :map on the GPU).
+
+    Returns ``(energies, vectors)`` with ``vectors`` a list of ``MBS64Vector``.
+    ``krylovkit_kwargs`` accepts krylovdim, tol, maxiter, vec0, seed and precision ("fp64"/"mixed").
+    """
+    import time
+    import warnings
+
+    if N < 1:
+        raise AssertionError("N should be at least 1.")
+    if len(subspace) > np.iinfo(index_type).max:
+        raise AssertionError(f"Hilbert space dimension {len(subspace)} exceeds limit of index_type={index_type}.")
+    if method not in ("sparse", "dense", "map"):
+        raise AssertionError(f"Unknown method: {method}. Use :sparse, :dense, :map.")
+    if device not in ("cpu", "gpu", "cuda", "oneapi", "metal", "multi_cuda", "b200"):
+        raise AssertionError(f"Unknown device: {device}.")
+    if ishermitian and not Hamiltonian.isupper():
+        raise AssertionError("Use upper_hermitian form of Hamiltonian operator when ishermitian = true.")
+    if method != "map" or device == "cpu":
+        raise NotImplementedError("this backend provides method=:map on the GPU; the sparse/dense and CPU "
+                                  "paths stay in the reference")
+    if len(subspace) < map_warning_dim and method_info:
+        warnings.warn(f"Linear map may be slow for dim={len(subspace)}. Consider using :sparse method.")
+    if device == "gpu":
+        if DEFAULT_GPU[0] == "nogpu":
+            activate_b200(set_default_gpu=True)
+        device = DEFAULT_GPU[0]
+        if device == "nogpu":
+            raise ValueError("No GPU available. Please load a supported GPU extension and verify availability.")
+    if device == "cuda":
+        device = "b200"
+    _throw_gpu_unavailable(device)
+    t0 = time.perf_counter()
+    H_map = LinearMap(Hamiltonian, subspace)
+    H_gpu = create_gpu_linearmap(H_map, device)
+    try:
+        vals, vecs, info = krylov_map_solve(H_gpu, N, ishermitian=ishermitian, **krylovkit_kwargs)
+    finally:
+        H_gpu.release()
+    if showtime:
+        print(f"EDsolve: {time.perf_counter() - t0:.4f} s ({info['matvecs']} matvecs, "
+              f"{info['restarts']} restarts)")
+    if len(vals) < N:
+        raise RuntimeError(f"Krylov method fails. Cannot find {N} eigenvectors.")
+    energies = np.asarray(vals[:N])
+    vectors = [MBS64Vector(vecs[i], subspace) for i in range(N)]
+    return energies, vectors

@@ -878,6 +878,41 @@ OR_API void or_matvec_c64(const uint64_t* basis, int64_t N, const or_scat* list,
     }
 }
 
+/* The same map evaluated on selected rows only (spot checks of large sectors). */
+OR_API void or_matvec_rows_c128(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat,
+                                const double* x, const int64_t* rows, int64_t nrows, double* y, int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+    #pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t r = 0; r < nrows; ++r) {
+        int64_t i = rows[r];
+        uint64_t st = basis[i];
+        double yr = 0.0, yi = 0.0;
+        for (int64_t s = 0; s < nscat; ++s) {
+            const or_scat* sc = &list[s];
+            if ((st & sc->out) != sc->out) continue;
+            double ar, ai;
+            uint64_t tgt;
+            if (sc->in == sc->out) { ar = sc->re; ai = sc->im; tgt = st; }
+            else {
+                uint64_t mid = st & ~sc->out;
+                if ((mid & sc->in) != 0) continue;
+                tgt = mid | sc->in;
+                int sign = 1 - 2 * (__builtin_popcountll(mid & sc->pm) & 1);
+                ar = sign * sc->re; ai = sign * sc->im;
+            }
+            int64_t j = searchsortedfirst(basis, N, tgt);
+            if (j < N && basis[j] == tgt) {
+                double pr, pi;
+                cmul(ar, ai, x[2 * j], x[2 * j + 1], &pr, &pi);
+                yr = yr + pr; yi = yi + pi;
+            }
+        }
+        y[2 * r] = yr; y[2 * r + 1] = yi;
+    }
+}
+
 /* Dense H[i][j] = <i|H|j> (row-major, interleaved complex) for small cross-checks. */
 OR_API void or_dense_hamiltonian(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat, double* H) {
     memset(H, 0, (size_t)N * N * 16);

@@ -358,6 +358,21 @@ def matvec(basis: np.ndarray, full_list: np.ndarray, x: np.ndarray, nthreads: in
     return y
 
 
+def matvec_rows(basis, full_list, x, rows, nthreads: int = 0) -> np.ndarray:
+    """(H x)[rows] for the given row indices (complex128)."""
+    basis = np.ascontiguousarray(basis, np.uint64)
+    full_list = np.ascontiguousarray(full_list, SCAT_DTYPE)
+    x = np.ascontiguousarray(x, np.complex128)
+    rows = np.ascontiguousarray(rows, np.int64)
+    y = np.zeros(len(rows), np.complex128)
+    L = lib()
+    L.or_matvec_rows_c128.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                      C.c_int64, C.c_void_p, C.c_int]
+    L.or_matvec_rows_c128(_ptr(basis), len(basis), _ptr(full_list), len(full_list), _ptr(x), _ptr(rows),
+                          len(rows), _ptr(y), nthreads)
+    return y
+
+
 def dense_hamiltonian(basis: np.ndarray, full_list: np.ndarray) -> np.ndarray:
     basis = np.ascontiguousarray(basis, np.uint64)
     full_list = np.ascontiguousarray(full_list, SCAT_DTYPE)
