@@ -1,0 +1,406 @@
+#!/usr/bin/env python
+"""Benchmark: batched eigensolves on B200 (the headline) with the plain GPU Lanczos beside it.
+
+Workload (synthetic, seeded; no dataset): 3x9 k-mesh, Ne=9 -> 27 momentum sectors of ~174k
+states.  H(U0) = H0 + U0 V (one-body band + random-phase two-body recipe, seed 2) with 32
+interaction strengths U0 evenly spaced in [0.5, 2.0]; the 4 lowest eigenpairs of each
+(sector, U0) to <= 1e-10 relative eigenvalue error.
+
+A step is one sector x 32 U0 values = 32 solves through the batched mixed-precision solver
+(c64 block matvec, FP64 recurrences, FP64 Rayleigh-Ritz).  `value` times K steps with the
+sector bases already in HBM (enumerated by the basis kernel before timing); `e2e` times the
+same steps through the public API with host buffers (basis + operator in, eigenvalues and
+eigenvectors out).  The plain comparison solves U0 values of one sector one at a time with the
+FP64 single-vector Lanczos.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun (N > 1) every rank runs its own sectors (replicas, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "momentumed.jl_b200"))
+
+MESH = (3, 9)
+NE = 9
+SEED = 2
+NEV = 4
+NU = 32
+KRYLOV = 30
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--plain", type=int, default=4, help="U0 values solved one at a time for the plain comparison")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--profile-only", action="store_true", help="one short run for ncu (no timing output)")
+    return ap.parse_args()
+
+
+def workload_operators():
+    """(para, pair arrays (amp_a, amp_b, in, out, pm), u grid) of the sweep."""
+    import momed
+    from momed.core import pair_operator
+    from momed.synthetic import mesh_para, u_grid
+
+    para, _ = mesh_para(*MESH, SEED)
+    A = momed.MBOperator(momed.ED_scatterlist_onebody(para), upper_hermitian=True)
+    B = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=True)
+    return para, pair_operator(A, B), u_grid(NU, 0.5, 2.0)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- distributed
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def all_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def all_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ----------------------------------------------------------------------------- CPU arm
+def cpu_reference_solve(basis, pair, u0, nthreads):
+    """The reference's CPU path restated (oracle): gather map over the full term list + FP64 Lanczos."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    amp_a, amp_b, in_, out, pm = pair
+    full = np.zeros(len(amp_a), O.SCAT_DTYPE)
+    amp = amp_a + u0 * amp_b
+    full["re"], full["im"], full["out"], full["in"], full["pm"] = amp.real, amp.imag, out, in_, pm
+    t0 = time.perf_counter()
+    vals, _, _, info = O.eigsolve(basis, full, NEV, krylovdim=KRYLOV, tol=1e-12, seed=1, nthreads=nthreads,
+                                  want_vectors=True)
+    return time.perf_counter() - t0, vals, info
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference CPU path (oracle restatement, all host threads) on this workload."""
+    if rank != 0:
+        return
+    import momed
+    para, pair, u = workload_operators()
+    h = momed.Handle(0) if _has_gpu() else None
+    if h is not None:
+        sectors = h.enumerate_basis(para.k_list, para.Gk, 1, 1, (NE,))
+    else:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        b, ks = O.momentum_subspaces(para.k_list, para.Gk, (NE,))
+        sectors = list(zip(ks, b))
+    nthreads = os.cpu_count() or 1
+    times = []
+    budget = 150.0
+    t_start = time.perf_counter()
+    for k in range(max(args.steps, 1)):
+        basis = sectors[k % len(sectors)][1]
+        dt, vals, info = cpu_reference_solve(basis, pair, float(u[k % NU]), nthreads)
+        times.append(dt)
+        if time.perf_counter() - t_start > budget:
+            break
+    value = len(times) / sum(times)
+    line = {
+        "impl": "reference", "metric": "batched solves/s at <=1e-10 eigenvalue error", "value": value,
+        "unit": "solves/s", "n_gpus": 0, "steps": len(times), "warmup": 0,
+        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": f"3x9 mesh Ne=9 sectors (~174k states) x U0 in [0.5,2]; nev={NEV}; one "
+                               "(sector, U0) solve per step", "solver": "reference CPU map + FP64 Lanczos"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "port",
+                         "sample": f"{len(times)} full (sector, U0) solves, {len(sectors[0][1])}-state sector"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+# ----------------------------------------------------------------------------- our arm
+def block_bytes(N: int, nnz: int, nscat: int, nb: int, s: int) -> float:
+    """Algorithmic bytes of one block matvec launch: basis keys, x stream read and y write for nb
+    right-hand sides, one nb-wide gather per (row, term) hit, and the term list (two amplitudes
+    and three masks per term)."""
+    return N * (8 + 2 * s * nb) + nnz * s * nb + nscat * (2 * s + 24)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+
+    import momed
+    from momed import _lib
+
+    torch.cuda.set_device(local)
+    para, pair, u = workload_operators()
+    amp_a, amp_b, in_, out, pm = pair
+    h = momed.Handle(local)
+    stream = torch.cuda.Stream(device=local)
+    h.set_stream(stream.cuda_stream)
+    sectors = h.enumerate_basis(para.k_list, para.Gk, 1, 1, (NE,))        # kernel (a), outside timing
+    nsec = len(sectors)
+    h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+    W, K = max(args.warmup, 0), max(args.steps, 1)
+    order = [(rank + world * i) % nsec for i in range(W + K)]
+
+    def step_device(sidx):
+        h.select_sector(sidx, len(sectors[sidx][1]))
+        vals, _, res, info = h.batch_solve(u, NEV, krylovdim=KRYLOV, tol=1e-12, precision=_lib.PREC_MIXED)
+        return vals, res, info
+
+    if args.profile_only:
+        step_device(order[0])
+        return
+
+    for i in range(W):
+        step_device(order[i])
+    torch.cuda.synchronize()
+    # ---------------------------------------------------------------- value: inputs resident in HBM
+    launches0 = _lib.kernel_launches()
+    h.profile(True)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+    per_step_nnz, per_step_n, infos, all_vals = [], [], [], []
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        ev[0].record(stream)
+        for i in range(K):
+            sidx = order[W + i]
+            vals, res, info = step_device(sidx)
+            ev[i + 1].record(stream)
+            infos.append(info)
+            all_vals.append((sidx, vals, res))
+        torch.cuda.synchronize()
+    barrier(world)
+    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(K)]
+    elapsed = sum(step_ms) / 1e3
+    n_mv, ms_mv = h.profile_read(_lib.KERNEL_BLOCK_MATVEC_C64)
+    h.profile(False)
+    launches = _lib.kernel_launches() - launches0
+    # algorithmic bytes of the dominant kernel (c64 block matvec), averaged over the timed sectors
+    mv_bytes = []
+    for sidx, _, _ in all_vals:
+        h.select_sector(sidx, len(sectors[sidx][1]))
+        st = h.stats()
+        mv_bytes.append(block_bytes(len(sectors[sidx][1]), st["nnz"], len(amp_a), 32, 8))
+    bytes_per_launch = float(np.mean(mv_bytes))
+    solves_local = K * NU
+    elapsed_max = all_max(elapsed, world)
+    solves_total = all_sum(solves_local, world)
+    value = solves_total / elapsed_max
+
+    # ---------------------------------------------------------------- e2e: public API, host buffers
+    host_inputs = [(sectors[order[W + i]][1].copy()) for i in range(K)]
+    h2d = [b.nbytes + amp_a.nbytes + amp_b.nbytes + in_.nbytes + out.nbytes + pm.nbytes for b in host_inputs]
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    e2e_ev[0].record(stream)
+    d2h = []
+    for i in range(K):
+        h.set_basis(host_inputs[i])
+        h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+        vals, vecs, res, info = h.batch_solve(u, NEV, krylovdim=KRYLOV, tol=1e-12, precision=_lib.PREC_MIXED,
+                                              want_vectors=True)
+        d2h.append(vals.nbytes + res.nbytes + vecs.nbytes)
+    e2e_ev[1].record(stream)
+    torch.cuda.synchronize()
+    e2e_elapsed = all_max(e2e_ev[0].elapsed_time(e2e_ev[1]) / 1e3, world)
+    e2e_value = all_sum(solves_local, world) / e2e_elapsed
+
+    # ---------------------------------------------------------------- plain one-at-a-time FP64 GPU Lanczos
+    plain = None
+    if rank == 0 and args.plain > 0:
+        sidx, bvals, _ = all_vals[0]
+        h.select_sector(sidx, len(sectors[sidx][1]))
+        h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+        pe = [torch.cuda.Event(enable_timing=True) for _ in range(args.plain + 1)]
+        torch.cuda.synchronize()
+        pe[0].record(stream)
+        errs = []
+        for j in range(args.plain):
+            h.set_param(float(u[j]))
+            pv, _, pr, pinfo = h.eigsolve(NEV, krylovdim=KRYLOV, tol=1e-12, seed=1, want_vectors=False,
+                                          precision=_lib.PREC_FP64)
+            pe[j + 1].record(stream)
+            errs.append(float(np.max(np.abs(bvals[j] - pv) / np.maximum(np.abs(pv), 1.0))))
+        torch.cuda.synchronize()
+        lat = [pe[j].elapsed_time(pe[j + 1]) for j in range(args.plain)]
+        h.set_param(1.0)
+        plain = {"solves_per_s": 1e3 * args.plain / sum(lat), "latency_ms_p50": float(np.percentile(lat, 50)),
+                 "latency_ms_p99": float(np.percentile(lat, 99)), "solves": args.plain,
+                 "max_rel_eig_err_batched_vs_fp64": max(errs)}
+
+    # ---------------------------------------------------------------- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        basis = sectors[order[W]][1]
+        nthreads = os.cpu_count() or 1
+        dt, _, _ = cpu_reference_solve(basis, pair, float(u[0]), nthreads)
+        cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": nthreads, "kind": "port",
+               "sample": f"1 full FP64 solve (reference CPU map + Lanczos) of one (sector, U0) pair, "
+                         f"{len(basis)} states, U0={u[0]:.3f}"}
+
+    if rank == 0:
+        avg_ms = ms_mv / max(n_mv, 1)
+        achieved = bytes_per_launch / (avg_ms * 1e-3) / 1e9
+        peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        peak, peak_src = 6650.0, "fallback"
+        if os.path.exists(peaks_path):
+            try:
+                peak = float(json.load(open(peaks_path))["hbm_gbs"])
+                peak_src = "measured"
+            except Exception:
+                pass
+        lat = sorted(step_ms)
+        line = {
+            "metric": "batched solves/s, p50/p99 latency vs plain GPU Lanczos at <=1e-10 eig error",
+            "value": value, "unit": "solves/s", "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": elapsed_max * 1e3 / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 matvec / f64 recurrences + f64 Rayleigh-Ritz", "data": "synthetic",
+            "config": {"workload": f"3x9 mesh Ne=9, one sector (~174k states) x {NU} U0 in [0.5,2] per step, "
+                                   f"nev={NEV}, krylovdim={KRYLOV}, tol 1e-12",
+                       "global_batch": NU * world, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (Krylov basis ~1.4 GB per step)"},
+            "latency_ms": {"per_batch_p50": float(np.percentile(lat, 50)),
+                           "per_batch_p99": float(np.percentile(lat, 99)),
+                           "per_solve_p50": float(np.percentile(lat, 50)),
+                           "per_solve_p99": float(np.percentile(lat, 99))},
+            "plain_gpu_lanczos": plain,
+            "speedup_vs_plain": (value / world) / plain["solves_per_s"] if plain else None,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                         "kernel": "block matvec c64 x32 (k_block_matvec<float,32>)",
+                         "launches": n_mv, "avg_launch_ms": avg_ms,
+                         "algorithmic_bytes_per_launch": bytes_per_launch},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(np.mean(h2d)),
+                    "d2h_bytes_per_step": int(np.mean(d2h))},
+            "gpu_launches": int(all_sum(launches, world)),
+            "clocks": clk.summary(),
+            "solver": {"matvecs_per_step": int(np.mean([i["matvecs"] for i in infos])),
+                       "restarts_per_step": float(np.mean([i["restarts"] for i in infos])),
+                       "converged_min": int(min(i["converged"] for i in infos)),
+                       "max_residual": float(max(float(np.max(r)) for _, _, r in all_vals))},
+        }
+        print(json.dumps(line), flush=True)
+    h.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

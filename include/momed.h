@@ -137,6 +137,19 @@ MOMED_API int  momed_stats(momed_handle* h, int64_t* nnz, int32_t* index_mode, i
 /* Device time (ms) of the last matvec kernel launch on the handle's stream. */
 MOMED_API int  momed_last_kernel_ms(momed_handle* h, double* ms);
 
+/* Kernels this library has launched in the process so far (all handles). */
+MOMED_API int64_t momed_kernel_launches(void);
+
+/* Per-launch device timing of the matvec kernels (CUDA events on the handle's stream).
+ * momed_profile(h, 1) starts a fresh record; momed_profile_read returns, for one kernel
+ * kind, the launches recorded since and their summed device time in ms. */
+#define MOMED_KERNEL_MATVEC_C128        0
+#define MOMED_KERNEL_MATVEC_C64         1
+#define MOMED_KERNEL_BLOCK_MATVEC_C64   2
+#define MOMED_KERNEL_BLOCK_MATVEC_C128  3
+MOMED_API int  momed_profile(momed_handle* h, int32_t enable);
+MOMED_API int  momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms);
+
 #ifdef __cplusplus
 }
 #endif

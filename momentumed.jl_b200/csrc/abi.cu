@@ -3,6 +3,7 @@
 // Every entry point catches momed::Error and CUDA failures and turns them into
 // an int status plus momed_last_error(h); nothing throws across the boundary.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <numeric>
 
@@ -13,6 +14,43 @@
 using namespace momed;
 
 namespace momed {
+
+static std::atomic<int64_t> g_launches{0};
+void note_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+int64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+
+// Fold the elapsed time of recorded event pairs into prof_ms and recycle them.
+static void prof_drain(momed_handle* h) {
+    if (h->prof_used == 0) return;
+    MOMED_CUDA_TRY(cudaEventSynchronize(h->prof_ev[h->prof_used - 1]));
+    for (size_t i = 0; i + 1 < h->prof_used; i += 2) {
+        float ms = 0.f;
+        MOMED_CUDA_TRY(cudaEventElapsedTime(&ms, h->prof_ev[i], h->prof_ev[i + 1]));
+        h->prof_ms[h->prof_kind[i / 2]] += ms;
+    }
+    h->prof_used = 0;
+}
+
+void prof_begin(momed_handle* h) {
+    if (!h->prof) return;
+    if (h->prof_used + 2 > h->prof_ev.size()) {
+        if (h->prof_ev.size() >= 4096) prof_drain(h);   // bounded pool
+        while (h->prof_used + 2 > h->prof_ev.size()) {
+            cudaEvent_t e;
+            MOMED_CUDA_TRY(cudaEventCreate(&e));
+            h->prof_ev.push_back(e);
+        }
+        h->prof_kind.resize(h->prof_ev.size() / 2 + 1, 0);
+    }
+    MOMED_CUDA_TRY(cudaEventRecord(h->prof_ev[h->prof_used++], h->stream));
+}
+
+void prof_end(momed_handle* h, int kind) {
+    if (!h->prof) return;
+    h->prof_kind[(h->prof_used - 1) / 2] = kind;
+    MOMED_CUDA_TRY(cudaEventRecord(h->prof_ev[h->prof_used++], h->stream));
+    ++h->prof_launches[kind & 3];
+}
 
 OpView Operator::view() const {
     OpView v{};
@@ -265,6 +303,7 @@ int momed_destroy(momed_handle* h) {
     if (!h) return MOMED_OK;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     cudaStream_t st = h->own_stream ? h->stream : nullptr;
@@ -450,6 +489,29 @@ int momed_last_kernel_ms(momed_handle* h, double* ms) {
     if (!h || !ms) return MOMED_EINVAL;
     *ms = h->last_kernel_ms;
     return MOMED_OK;
+}
+
+int64_t momed_kernel_launches(void) { return launches_total(); }
+
+int momed_profile(momed_handle* h, int32_t enable) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->prof_used = 0;
+        for (int k = 0; k < 4; ++k) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; }
+        h->prof = enable != 0;
+        return MOMED_OK;
+    });
+}
+
+int momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms) {
+    if (!h || kind < 0 || kind > 3) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        prof_drain(h);
+        if (launches) *launches = h->prof_launches[kind];
+        if (total_ms) *total_ms = h->prof_ms[kind];
+        return MOMED_OK;
+    });
 }
 
 }  // extern "C"

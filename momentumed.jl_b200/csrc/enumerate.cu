@@ -49,14 +49,51 @@ struct EnumParams {
     int32_t box_ext[3];
     const int32_t* sec_of; // [prod box_ext] sector id or -1
     const uint64_t* binom;  // [65 * 65] C(n, k) as uint64
+    int64_t box_n;          // entries of sec_of
+    int64_t out_cap;        // entries of the output buffer (write pass)
+    unsigned long long* err; // [8]: count of out-of-range accesses found and skipped (must stay 0),
+                             //      then kind, a, b, c of the first one
 };
 
-__device__ __forceinline__ uint64_t dbinom(const uint64_t* b, int n, int k) {
+__host__ __device__ __forceinline__ void note_err(const EnumParams& P, long long kind = 0, long long a = 0,
+                                                  long long b = 0, long long c = 0) {
+#ifdef __CUDA_ARCH__
+    if (P.err) {
+        if (atomicAdd(P.err, 1ull) == 0ull) {
+            P.err[1] = (unsigned long long)kind;
+            P.err[2] = (unsigned long long)a;
+            P.err[3] = (unsigned long long)b;
+            P.err[4] = (unsigned long long)c;
+        }
+    }
+#else
+    if (P.err && (*P.err)++ == 0) { P.err[1] = kind; P.err[2] = a; P.err[3] = b; P.err[4] = c; }
+#endif
+}
+
+// Helpers are host-callable too so the index arithmetic can be exercised on the CPU.
+__host__ __device__ __forceinline__ int ffs64(uint64_t x) {
+#ifdef __CUDA_ARCH__
+    return __ffsll((long long)x);
+#else
+    return __builtin_ffsll((long long)x);
+#endif
+}
+template <typename T>
+__host__ __device__ __forceinline__ T ld_ro(const T* p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+
+__host__ __device__ __forceinline__ uint64_t dbinom(const uint64_t* b, int n, int k) {
     return (k < 0 || n < 0 || k > n) ? 0ull : b[n * 65 + k];
 }
 
 // pattern (over len positions, t set bits) of the rank-th combination in colex order
-__device__ uint64_t unrank_pattern(const uint64_t* binom, int len, int t, int64_t rank) {
+__host__ __device__ uint64_t unrank_pattern(const uint64_t* binom, int len, int t, int64_t rank) {
     uint64_t pat = 0;
     int64_t x = rank;
     for (int i = t; i >= 1; --i) {
@@ -69,28 +106,28 @@ __device__ uint64_t unrank_pattern(const uint64_t* binom, int len, int t, int64_
 }
 
 // next larger integer with the same popcount
-__device__ __forceinline__ uint64_t next_comb(uint64_t x) {
+__host__ __device__ __forceinline__ uint64_t next_comb(uint64_t x) {
     uint64_t c = x & (~x + 1ull);
     uint64_t r = x + c;
-    return r | (((x ^ r) >> 2) >> (__ffsll((long long)c) - 1));
+    return r | (((x ^ r) >> 2) >> (ffs64(c) - 1));
 }
 
-__device__ __forceinline__ uint64_t deposit(const Comp& c, uint64_t pat) {
+__host__ __device__ __forceinline__ uint64_t deposit(const Comp& c, uint64_t pat) {
     if (!c.masked) return pat << c.shift;
     uint64_t out = 0;
     while (pat) {
-        int p = __ffsll((long long)pat) - 1;
+        int p = ffs64(pat) - 1;
         out |= 1ull << (c.shift + c.pos[p]);
         pat &= pat - 1ull;
     }
     return out;
 }
 
-__device__ __forceinline__ int sector_of(const EnumParams& P, uint64_t s) {
+__host__ __device__ __forceinline__ int sector_of(const EnumParams& P, uint64_t s) {
     int k[3] = {0, 0, 0};
     while (s) {
-        int o = __ffsll((long long)s) - 1;
-        for (int d = 0; d < P.dim; ++d) k[d] += P.kv[o][d];
+        int o = ffs64(s) - 1;
+        for (int d = 0; d < P.dim && d < 3; ++d) k[d] += P.kv[o][d];
         s &= s - 1ull;
     }
     int64_t idx = 0, stride = 1;
@@ -102,30 +139,30 @@ __device__ __forceinline__ int sector_of(const EnumParams& P, uint64_t s) {
         idx += (int64_t)v * stride;
         stride *= P.box_ext[d];
     }
-    return __ldg(P.sec_of + idx);
+    if (idx < 0 || idx >= P.box_n) { note_err(P, 1, idx, P.box_n, (long long)s); return -1; }
+    return ld_ro(P.sec_of + idx);
 }
 
-// Walk ranks [r0, r1) calling f(state) in order.
-template <typename F>
-__device__ void walk(const EnumParams& P, int64_t r0, int64_t r1, F&& f) {
-    if (r0 >= r1) return;
-    uint64_t pat[kMaxComp];
+// Iterator over ranks in increasing order (component 0 fastest, with carry).
+struct Walker {
+    uint64_t pat[kMaxComp], part[kMaxComp];
     int64_t rk[kMaxComp];
-    uint64_t part[kMaxComp];
-    int64_t rem = r0;
-    for (int c = P.ncomp - 1; c >= 0; --c) {
-        rk[c] = rem / P.comp[c].stride;
-        rem -= rk[c] * P.comp[c].stride;
+    uint64_t state;
+
+    __host__ __device__ void init(const EnumParams& P, int64_t r0) {
+        int64_t rem = r0;
+        for (int c = P.ncomp - 1; c >= 0; --c) {
+            rk[c] = rem / P.comp[c].stride;
+            rem -= rk[c] * P.comp[c].stride;
+        }
+        state = 0;
+        for (int c = 0; c < P.ncomp; ++c) {
+            pat[c] = unrank_pattern(P.binom, P.comp[c].len, P.comp[c].t, rk[c]);
+            part[c] = deposit(P.comp[c], pat[c]);
+            state |= part[c];
+        }
     }
-    uint64_t state = 0;
-    for (int c = 0; c < P.ncomp; ++c) {
-        pat[c] = unrank_pattern(P.binom, P.comp[c].len, P.comp[c].t, rk[c]);
-        part[c] = deposit(P.comp[c], pat[c]);
-        state |= part[c];
-    }
-    for (int64_t r = r0; r < r1; ++r) {
-        f(state);
-        // advance component 0 with carry
+    __host__ __device__ void advance(const EnumParams& P) {
         for (int c = 0; c < P.ncomp; ++c) {
             state &= ~part[c];
             if (rk[c] + 1 < P.comp[c].count) {
@@ -133,7 +170,7 @@ __device__ void walk(const EnumParams& P, int64_t r0, int64_t r1, F&& f) {
                 pat[c] = next_comb(pat[c]);
                 part[c] = deposit(P.comp[c], pat[c]);
                 state |= part[c];
-                break;
+                return;
             }
             rk[c] = 0;
             pat[c] = P.comp[c].t ? ((1ull << P.comp[c].t) - 1ull) : 0ull;
@@ -141,74 +178,84 @@ __device__ void walk(const EnumParams& P, int64_t r0, int64_t r1, F&& f) {
             state |= part[c];
         }
     }
+};
+
+__host__ __device__ __forceinline__ void thread_ranks(const EnumParams& P, int64_t tid, int64_t& r0, int64_t& r1) {
+    r0 = tid * P.chunk;
+    r1 = r0 + P.chunk;
+    if (r1 > P.total) r1 = P.total;
+    if (r0 > r1) r0 = r1;
 }
 
-__global__ void __launch_bounds__(kThreads)
-k_enum_count(EnumParams P, int win0, int nwin, int32_t* block_counts /* [nwin][nblocks] */) {
-    __shared__ int32_t sc[kSecWin];
-    if (threadIdx.x < kSecWin) sc[threadIdx.x] = 0;
-    __syncthreads();
-    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t r0 = tid * P.chunk, r1 = min(P.total, r0 + P.chunk);
-    int32_t cnt[kSecWin];
-#pragma unroll
-    for (int i = 0; i < kSecWin; ++i) cnt[i] = 0;
-    walk(P, r0, r1, [&](uint64_t s) {
-        int sec = sector_of(P, s) - win0;
-        if (sec >= 0 && sec < nwin) {
-#pragma unroll
-            for (int i = 0; i < kSecWin; ++i) cnt[i] += (i == sec);
-        }
-    });
-    for (int i = 0; i < nwin; ++i)
-        if (cnt[i]) atomicAdd(&sc[i], cnt[i]);
-    __syncthreads();
-    if (threadIdx.x < nwin) block_counts[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = sc[threadIdx.x];
-}
+// Per-thread sector counts of the block live in shared memory: cnt[sector][thread].
+struct EnumShared {
+    EnumParams P;
+    int32_t cnt[kSecWin][kThreads];
+};
 
-__global__ void __launch_bounds__(kThreads)
-k_enum_write(EnumParams P, int win0, int nwin, const int64_t* block_offsets /* [nwin][nblocks] */, uint64_t* out) {
-    __shared__ int32_t warp_tot[kThreads / 32];
-    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t r0 = tid * P.chunk, r1 = min(P.total, r0 + P.chunk);
-    int32_t cnt[kSecWin];
-#pragma unroll
-    for (int i = 0; i < kSecWin; ++i) cnt[i] = 0;
-    walk(P, r0, r1, [&](uint64_t s) {
-        int sec = sector_of(P, s) - win0;
-        if (sec >= 0 && sec < nwin) {
-#pragma unroll
-            for (int i = 0; i < kSecWin; ++i) cnt[i] += (i == sec);
-        }
-    });
-    // per-sector exclusive scan over the block's threads (thread order = rank order)
-    int64_t pos[kSecWin];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int i = 0; i < kSecWin; ++i) {
-        int v = (i < nwin) ? cnt[i] : 0;
-        int incl = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            int t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) warp_tot[wid] = incl;
-        __syncthreads();
-        int before = 0;
-        for (int w = 0; w < wid; ++w) before += warp_tot[w];
-        __syncthreads();
-        pos[i] = (i < nwin) ? block_offsets[(int64_t)i * gridDim.x + blockIdx.x] + before + (incl - v) : 0;
+__device__ void count_chunk(EnumShared& sh, int win0, int nwin, int64_t r0, int64_t r1) {
+    const int t = threadIdx.x;
+    for (int i = 0; i < kSecWin; ++i) sh.cnt[i][t] = 0;
+    if (r0 >= r1) return;
+    Walker w;
+    w.init(sh.P, r0);
+    for (int64_t r = r0; r < r1; ++r) {
+        int sec = sector_of(sh.P, w.state) - win0;
+        if (sec >= 0 && sec < nwin) sh.cnt[sec][t] += 1;
+        if (r + 1 < r1) w.advance(sh.P);
     }
-    walk(P, r0, r1, [&](uint64_t s) {
-        int sec = sector_of(P, s) - win0;
-        if (sec >= 0 && sec < nwin) {
-            int64_t p = 0;
-#pragma unroll
-            for (int i = 0; i < kSecWin; ++i) {
-                if (i == sec) { p = pos[i]; pos[i] = p + 1; }
-            }
-            out[p] = s;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_enum_count(EnumParams Pp, int win0, int nwin, int32_t* block_counts /* [kSecWin][nblocks] */) {
+    __shared__ EnumShared sh;
+    if (threadIdx.x == 0) sh.P = Pp;
+    __syncthreads();
+    int64_t r0, r1;
+    thread_ranks(sh.P, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, r0, r1);
+    count_chunk(sh, win0, nwin, r0, r1);
+    __syncthreads();
+    if (threadIdx.x < nwin) {
+        int32_t s = 0;
+        for (int t = 0; t < kThreads; ++t) s += sh.cnt[threadIdx.x][t];
+        block_counts[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_enum_write(EnumParams Pp, int win0, int nwin, const int64_t* block_offsets /* [kSecWin][nblocks] */, uint64_t* out) {
+    __shared__ EnumShared sh;
+    if (threadIdx.x == 0) sh.P = Pp;
+    __syncthreads();
+    int64_t r0, r1;
+    thread_ranks(sh.P, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, r0, r1);
+    count_chunk(sh, win0, nwin, r0, r1);
+    __syncthreads();
+    // exclusive scan of each sector's row over the block's threads (thread order = rank order)
+    if (threadIdx.x < nwin) {
+        int32_t run = 0;
+        for (int t = 0; t < kThreads; ++t) {
+            int32_t v = sh.cnt[threadIdx.x][t];
+            sh.cnt[threadIdx.x][t] = run;
+            run += v;
         }
-    });
+    }
+    __syncthreads();
+    if (r0 >= r1) return;
+    const int t = threadIdx.x;
+    Walker w;
+    w.init(sh.P, r0);
+    for (int64_t r = r0; r < r1; ++r) {
+        uint64_t s = w.state;
+        int sec = sector_of(sh.P, s) - win0;
+        if (sec >= 0 && sec < nwin) {
+            int64_t p = block_offsets[(int64_t)sec * gridDim.x + blockIdx.x] + sh.cnt[sec][t];
+            sh.cnt[sec][t] += 1;
+            if (p >= 0 && p < sh.P.out_cap) out[p] = s;
+            else note_err(sh.P, 2, p, sh.P.out_cap, sec);
+        }
+        if (r + 1 < r1) w.advance(sh.P);
+    }
 }
 
 int64_t hbinom(int n, int k) {
@@ -223,8 +270,21 @@ int64_t jmod(int64_t a, int64_t g) { int64_t r = a % g; return r < 0 ? r + g : r
 
 }  // namespace
 
-void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each, int ncc, const int64_t* mask,
-                     int mlen, const int64_t* momentum_list, int nmom) {
+// Host-side plan of one enumeration: kernel parameters (device pointers left null),
+// the sector momenta in the reference order, the momentum-box -> sector table and
+// the launch shape.
+struct EnumPlan {
+    EnumParams P{};
+    int dim = 0;
+    std::vector<int64_t> moms;      // [nsec * dim]
+    int64_t nsec = 0;
+    std::vector<int32_t> sec_of;    // [box_n]
+    std::vector<uint64_t> binom;    // [65 * 65]
+    int nblocks = 1;
+};
+
+EnumPlan plan_enumeration(const momed_para* p, const int64_t* N_each, int ncc, const int64_t* mask, int mlen,
+                          const int64_t* momentum_list, int nmom) {
     MOMED_REQUIRE(p && p->k_list && p->Gk, MOMED_EINVAL, "para, k_list and Gk are required");
     MOMED_REQUIRE(ncc == p->Nc_conserve && ncc >= 1 && ncc <= kMaxComp, MOMED_EINVAL,
                   "length of N_each must equal Nc_conserve (<= 8)");
@@ -233,7 +293,9 @@ void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each
     const int ncomp_bits = Nk * p->Nc_mix;
     MOMED_REQUIRE((int64_t)ncomp_bits * ncc <= 64 && Nk >= 1, MOMED_EINVAL, "Nk * Nc must be <= 64");
 
-    EnumParams P{};
+    EnumPlan plan{};
+    plan.dim = dim;
+    EnumParams& P = plan.P;
     P.ncomp = ncc;
     P.dim = dim;
     for (int d = 0; d < dim; ++d) P.Gk[d] = (int32_t)p->Gk[d];
@@ -343,33 +405,54 @@ void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each
         }
         if (in) sec_of[idx] = (int32_t)s;
     }
+    plan.binom.assign(65 * 65, 0);
+    for (int n = 0; n <= 64; ++n)
+        for (int k = 0; k <= n; ++k) plan.binom[n * 65 + k] = (uint64_t)hbinom(n, k);
+    plan.nblocks = 1;
+    P.chunk = 16;
+    if (total > 0) {
+        int64_t threads_target = (int64_t)148 * 2048;
+        P.chunk = std::max<int64_t>(16, (total + threads_target - 1) / threads_target);
+        int64_t nthreads = (total + P.chunk - 1) / P.chunk;
+        plan.nblocks = (int)((nthreads + kThreads - 1) / kThreads);
+    }
+    plan.moms = std::move(moms);
+    plan.nsec = nsec;
+    plan.sec_of = std::move(sec_of);
+    return plan;
+}
 
+void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each, int ncc, const int64_t* mask,
+                     int mlen, const int64_t* momentum_list, int nmom) {
+    EnumPlan plan = plan_enumeration(p, N_each, ncc, mask, mlen, momentum_list, nmom);
+    EnumParams& P = plan.P;
+    const int dim = plan.dim;
+    const int64_t nsec = plan.nsec;
+    const int64_t total = P.total;
+    const int nblocks = plan.nblocks;
+    const std::vector<int64_t>& moms = plan.moms;
     cudaStream_t st = h->stream;
     DevBuf<int32_t> d_sec;
-    d_sec.resize(box_n);
-    MOMED_CUDA_TRY(cudaMemcpyAsync(d_sec.p, sec_of.data(), box_n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    d_sec.resize(plan.sec_of.size());
+    MOMED_CUDA_TRY(cudaMemcpyAsync(d_sec.p, plan.sec_of.data(), plan.sec_of.size() * sizeof(int32_t),
+                                   cudaMemcpyHostToDevice, st));
     P.sec_of = d_sec.p;
-    std::vector<uint64_t> hb(65 * 65, 0);
-    for (int n = 0; n <= 64; ++n)
-        for (int k = 0; k <= n; ++k) hb[n * 65 + k] = (uint64_t)hbinom(n, k);
     DevBuf<uint64_t> d_binom;
-    d_binom.resize(65 * 65);
-    MOMED_CUDA_TRY(cudaMemcpyAsync(d_binom.p, hb.data(), hb.size() * 8, cudaMemcpyHostToDevice, st));
+    d_binom.resize(plan.binom.size());
+    MOMED_CUDA_TRY(cudaMemcpyAsync(d_binom.p, plan.binom.data(), plan.binom.size() * 8, cudaMemcpyHostToDevice, st));
     P.binom = d_binom.p;
+    P.box_n = (int64_t)plan.sec_of.size();
+    P.out_cap = 0;
+    DevBuf<unsigned long long> d_err;
+    d_err.resize(8);
+    MOMED_CUDA_TRY(cudaMemsetAsync(d_err.p, 0, 8 * sizeof(unsigned long long), st));
+    P.err = d_err.p;
 
     Enumeration& E = h->enumer;
     E.dim = dim;
     E.sizes.assign(nsec, 0);
     E.offsets.assign(nsec + 1, 0);
     E.sector_k.clear();
-    std::vector<std::vector<int64_t>> block_counts;
-    int nblocks = 1;
-    if (total > 0) {
-        int64_t threads_target = (int64_t)148 * 2048;
-        P.chunk = std::max<int64_t>(16, (total + threads_target - 1) / threads_target);
-        int64_t nthreads = (total + P.chunk - 1) / P.chunk;
-        nblocks = (int)((nthreads + kThreads - 1) / kThreads);
-    }
     // pass 1: counts per window of sectors
     std::vector<int64_t> counts(nsec * (int64_t)nblocks, 0);   // [sector][block]
     if (total > 0) {
@@ -396,6 +479,7 @@ void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each
     }
     E.offsets[nsec] = run;
     E.states.release();
+    P.out_cap = run;
     if (run > 0) {
         E.states.resize(run);
         DevBuf<int64_t> d_off;
@@ -421,7 +505,19 @@ void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each
     E.sector_k = ks;
     E.sizes = sz;
     E.offsets = of;
+    unsigned long long herr[8] = {0};
+    MOMED_CUDA_TRY(cudaMemcpyAsync(herr, d_err.p, sizeof(herr), cudaMemcpyDeviceToHost, st));
     MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+    if (herr[0] != 0) {
+        std::string msg = "basis enumeration skipped " + std::to_string(herr[0]) + " out-of-range accesses; first: kind " +
+                          std::to_string((long long)herr[1]) + " values " + std::to_string((long long)herr[2]) + " " +
+                          std::to_string((long long)herr[3]) + " " + std::to_string((long long)herr[4]) +
+                          "; sector sizes:";
+        for (size_t s = 0; s < E.sizes.size() && s < 40; ++s) msg += " " + std::to_string(E.sizes[s]);
+        msg += "; chunk " + std::to_string(P.chunk) + " blocks " + std::to_string(nblocks) + " total " +
+               std::to_string(total);
+        throw Error{MOMED_ECUDA, msg};
+    }
 }
 
 }  // namespace momed

@@ -44,11 +44,21 @@ template <> struct Prec<double2> { static constexpr int value = MOMED_C128; };
 template <> struct Prec<float2> { static constexpr int value = MOMED_C64; };
 
 void apply_h(momed_handle* h, const double2* x, double2* y) {
+    prof_begin(h);
     launch_matvec_c128(index_view(h), h->op.view(), x, y, h->op.has_b ? h->u_dev.p : nullptr, h->n, h->stream);
+    prof_end(h, MOMED_KERNEL_MATVEC_C128);
 }
 void apply_h(momed_handle* h, const float2* x, float2* y) {
+    prof_begin(h);
     launch_matvec_c64(index_view(h), h->op.view(), x, y, h->op.has_b ? h->u_dev32.p : nullptr, h->n, h->stream);
+    prof_end(h, MOMED_KERNEL_MATVEC_C64);
 }
+
+}  // namespace
+
+void apply_h_fp64(momed_handle* h, const double2* x, double2* y) { apply_h(h, x, y); }
+
+namespace {
 
 struct RunOut {
     std::vector<double> theta, resid;   // all m Ritz values / residual estimates of the final cycle
@@ -87,6 +97,7 @@ struct Lanczos {
         vec_proj<VT>(v, N, 0, v, partial.p, grid, nullptr, st);
         vec_reduce(partial.p, grid, 1, coefA.p, nullptr, st);
         k_inv_sqrt<<<1, 32, 0, st>>>(coefA.p, scal.p);
+        note_launches(1);
         vec_scale<VT>(v, N, scal.p, st);
     }
     // orthogonalise v against columns [0, ncols) twice, then normalise
@@ -221,6 +232,8 @@ int pick_m(int64_t N, int nev, int krylovdim) {
     return std::max(m, 1);
 }
 
+}  // namespace
+
 // Generalised Hermitian eigenproblem G y = theta S y (k x k, column-major complex) on the host:
 // S = L L^H (Cholesky), C = L^-1 G L^-H, embed C in a real symmetric 2k x 2k matrix, pick
 // one eigenvector per eigenvalue pair, Y = L^-H z.  Returns false if S is not positive definite.
@@ -314,8 +327,6 @@ bool gen_herm_eig(int k, const std::vector<std::complex<double>>& G, const std::
         }
     return true;
 }
-
-}  // namespace
 
 // FP64 Rayleigh-Ritz on the k columns of X (device c128, [k][N]): writes refined values,
 // residual norms and (in place) refined vectors; W is scratch [k][N].

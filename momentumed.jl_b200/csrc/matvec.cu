@@ -383,6 +383,7 @@ void launch_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x,
         k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
     }
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 
 void launch_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y, const float* u_scale,
@@ -396,6 +397,7 @@ void launch_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, f
         k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
     }
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 
 void launch_count_hits(const IndexView& iv, const OpView& ov, unsigned long long* hits, unsigned long long* misses,
@@ -403,6 +405,7 @@ void launch_count_hits(const IndexView& iv, const OpView& ov, unsigned long long
     if (rows <= 0) return;
     k_count<<<persistent_grid(k_count, rows), kWarps * 32, 0, st>>>(iv, ov, hits, misses, rows);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 
 template <typename R>
@@ -432,6 +435,7 @@ static void block_dispatch(const IndexView& iv, const OpView& ov, const typename
     }
 #undef MOMED_BLK
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 
 void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y, const float* u,

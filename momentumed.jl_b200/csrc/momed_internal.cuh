@@ -177,6 +177,14 @@ struct momed_handle {
     momed::DevBuf<unsigned long long> counters;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     float last_kernel_ms = 0.f;
+
+    // optional per-launch timing of the matvec kernels
+    bool prof = false;
+    std::vector<cudaEvent_t> prof_ev;      // pairs (start, stop)
+    std::vector<int> prof_kind;            // kind of each pair
+    size_t prof_used = 0;                  // events used in the current record
+    int64_t prof_launches[4] = {0, 0, 0, 0};
+    double prof_ms[4] = {0, 0, 0, 0};      // folded-in time of pairs already read
 };
 
 namespace momed {
@@ -209,6 +217,17 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
 // enumerate.cu
 void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each, int ncc, const int64_t* mask,
                      int mlen, const int64_t* momentum_list, int nmom);
+
+// y = H x in FP64 on the working basis/operator (parameter u from the handle)
+void apply_h_fp64(momed_handle* h, const double2* x, double2* y);
+
+// bracket a matvec launch with timing events when profiling is on (abi.cu)
+void prof_begin(momed_handle* h);
+void prof_end(momed_handle* h, int kind);
+
+// process-wide count of kernel launches issued by this library (diagnostics)
+void note_launches(int64_t n);
+int64_t launches_total();
 
 // small dense symmetric eigensolver (host, FP64): A n x n row-major (destroyed),
 // eigenvalues ascending in w, eigenvectors as columns of V (row-major n x n)

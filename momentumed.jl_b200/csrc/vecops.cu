@@ -297,36 +297,43 @@ void vec_proj(const VT* V, int64_t N, int ncols, const VT* w, double2* partial, 
     MOMED_REQUIRE(ncols <= kMaxCols, MOMED_EINVAL, "krylovdim too large");
     k_proj<VT><<<grid, kVecThreads, 0, st>>>(V, N, ncols, w, partial, active);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 void vec_reduce(const double2* partial, int grid, int ncols1, double2* out, const int* active, cudaStream_t st) {
     k_reduce<<<1, 256, 0, st>>>(partial, grid, ncols1, out, active);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 template <typename VT>
 void vec_update(const VT* V, int64_t N, int ncols, const double2* coef, VT* w, double2* partial, int grid,
                 const int* active, cudaStream_t st) {
     k_update<VT><<<grid, kVecThreads, 0, st>>>(V, N, ncols, coef, w, partial, active);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 void vec_decide(const double2* coefA, int ncols, const double2* partial, int grid, int* flag, double* scal,
                 cudaStream_t st) {
     k_decide<<<1, 32, 0, st>>>(coefA, ncols, partial, grid, flag, scal);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 void vec_finalize(const double2* coefA, const double2* coefB, int ncols, const double2* partial2, int grid,
                   const int* flag, double* scal, double* alpha, double* beta, int j, cudaStream_t st) {
     k_finalize<<<1, 32, 0, st>>>(coefA, coefB, ncols, partial2, grid, flag, scal, alpha, beta, j);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 template <typename VT>
 void vec_scale(VT* v, int64_t N, const double* scal, cudaStream_t st) {
     k_scale<VT><<<flat_grid(N), kVecThreads, 0, st>>>(v, N, scal);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 template <typename VT>
 void vec_random(VT* v, int64_t N, uint64_t seed, cudaStream_t st) {
     k_random<VT><<<flat_grid(N), kVecThreads, 0, st>>>(v, N, seed);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 template <typename VIN, typename VOUT>
 void vec_combine(const VIN* V, int64_t N, int m, const double* U, int nout, VOUT* out, int64_t out_ld, int copy_col,
@@ -348,20 +355,24 @@ void vec_combine(const VIN* V, int64_t N, int m, const double* U, int nout, VOUT
         k<<<grid, kVecThreads, smem, st>>>(V, N, m, U, nout, out, out_ld, copy_col);
     }
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 void vec_combine_complex(const double2* X, int64_t N, int k, const double2* Y, double2* out, cudaStream_t st) {
     k_combine_complex<<<flat_grid(N), kVecThreads, 0, st>>>(X, N, k, Y, out);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 template <typename VT>
 void vec_copy_convert(const VT* src, double2* dst, int64_t n, cudaStream_t st) {
     k_to_d2<VT><<<flat_grid(n), kVecThreads, 0, st>>>(src, dst, n);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 template <typename VT>
 void vec_convert_from(const double2* src, VT* dst, int64_t n, cudaStream_t st) {
     k_from_d2<VT><<<flat_grid(n), kVecThreads, 0, st>>>(src, dst, n);
     MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
 }
 void vec_residual_norms(const double2* W, const double2* X, int64_t N, int k, const double* theta, double* out_norms,
                         cudaStream_t st) {

@@ -1,0 +1,124 @@
+# MomentumEDB200Ext — package extension that plugs libmomed_b200.so into MomentumED.jl's
+# GPU hooks (MomentumED/src/method/gpu_interface.jl:13-21) so that
+#     EDsolve(subspace, H::MBOperator; method=:map, device=:gpu, N=...)
+# runs on a B200.  No reference file is edited: the extension registers :b200 in the
+# mutable GPU_AVAILABLE dict and makes it the DEFAULT_GPU, and EDsolve resolves :gpu to it
+# (MomentumED.jl:446-453).
+#
+# Written against the C ABI in include/momed.h.  (This file is not executed by the test
+# suite of this repository: no Julia toolchain is available where it was built.)
+module MomentumEDB200Ext
+
+using MomentumED
+using MomentumED.Methods: GPU_AVAILABLE, DEFAULT_GPU, LinearMap, AbstractGPULinearMap
+import MomentumED.Methods: create_gpu_linearmap, krylov_map_solve, release_gpu_memory
+
+const libmomed = get(ENV, "MOMED_B200_LIB", joinpath(@__DIR__, "..", "lib", "libmomed_b200.so"))
+
+struct MomedSolveOpts
+    nev::Int32
+    krylovdim::Int32
+    maxiter::Int32
+    precision::Int32
+    tol::Float64
+    seed::UInt64
+    want_vectors::Int32
+    vecs_on_device::Int32
+end
+
+mutable struct MomedInfo
+    converged::Int32
+    restarts::Int32
+    matvecs::Int64
+    matvecs_fp64::Int64
+    seconds::Float64
+end
+MomedInfo() = MomedInfo(0, 0, 0, 0, 0.0)
+
+function check(h::Ptr{Cvoid}, rc::Cint)
+    rc == 0 && return nothing
+    msg = unsafe_string(ccall((:momed_last_error, libmomed), Cstring, (Ptr{Cvoid},), h))
+    rc == 4 && (@warn "B200 eigensolver: $msg"; return nothing)      # MOMED_ENOTCONV
+    error("libmomed_b200 error $rc: $msg")
+end
+
+function __init__()
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    rc = try
+        ccall((:momed_create, libmomed), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, h)
+    catch
+        Cint(7)
+    end
+    if rc == 0
+        ccall((:momed_destroy, libmomed), Cint, (Ptr{Cvoid},), h[])
+        GPU_AVAILABLE[:b200] = Ref(true)
+        DEFAULT_GPU[] = :b200
+        @info "MomentumED B200 extension loaded ($(unsafe_string(ccall((:momed_version, libmomed), Cstring, ()))))."
+    else
+        GPU_AVAILABLE[:b200] = Ref(false)
+    end
+end
+
+# The device map: one library handle holding the sorted basis and the completed term list.
+mutable struct B200LinearMap{bits, F <: AbstractFloat} <: AbstractGPULinearMap{bits, F}
+    handle::Ptr{Cvoid}
+    space::HilbertSubspace{bits}
+end
+
+Base.size(A::B200LinearMap) = (length(A.space), length(A.space))
+Base.eltype(::B200LinearMap{bits, F}) where {bits, F} = Complex{F}
+Base.adjoint(A::B200LinearMap) = A      # the completed list is Hermitian
+
+# create_gpu_linearmap hook (pattern of MomentumEDCUDAExt.jl:94-113): flatten and upload.
+function create_gpu_linearmap(A::LinearMap{bits, F}, ::Val{:b200}) where {bits, F}
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(C_NULL, ccall((:momed_create, libmomed), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, h))
+    basis = UInt64[mbs.n for mbs in A.space.list]
+    check(h[], ccall((:momed_set_basis, libmomed), Cint, (Ptr{Cvoid}, Ptr{UInt64}, Int64, Int32),
+                     h[], basis, length(basis), 0))
+    amp = ComplexF64[ComplexF64(s.Amp) for s in A.scat_list]
+    inm = UInt64[s.in.n for s in A.scat_list]
+    outm = UInt64[s.out.n for s in A.scat_list]
+    par = UInt64[s.parity_mask for s in A.scat_list]
+    check(h[], ccall((:momed_set_scatter, libmomed), Cint,
+                     (Ptr{Cvoid}, Ptr{ComplexF64}, Ptr{UInt64}, Ptr{UInt64}, Ptr{UInt64}, Int64),
+                     h[], amp, inm, outm, par, length(amp)))
+    M = B200LinearMap{bits, F}(h[], A.space)
+    finalizer(m -> (m.handle != C_NULL && ccall((:momed_destroy, libmomed), Cint, (Ptr{Cvoid},), m.handle);
+                    m.handle = C_NULL), M)
+    return M
+end
+
+# callable (y, x): H*x with host vectors (the CPU LinearMap convention, linear_map.jl:100-118)
+function (A::B200LinearMap{bits, F})(y::Vector{Complex{F}}, x::Vector{Complex{F}}) where {bits, F}
+    prec = F === Float64 ? Int32(0) : Int32(1)
+    check(A.handle, ccall((:momed_matvec, libmomed), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}, Int32, Int32),
+                          A.handle, x, y, prec, 0))
+    return y
+end
+(A::B200LinearMap{bits, F})(x::Vector{Complex{F}}) where {bits, F} = A(similar(x), x)
+
+# krylov_map_solve hook: the device-resident Lanczos; vecs are host vectors (Array(vecs[i]) works).
+function krylov_map_solve(H::B200LinearMap{bits, F}, N_eigen::Int64; ishermitian::Bool = true,
+                          vec0 = nothing, krylovdim::Int = 30, tol::Real = 1e-12, maxiter::Int = 100,
+                          seed::Integer = 0, precision::Symbol = :fp64, kwargs...) where {bits, F}
+    ishermitian || error("the B200 map solves Hermitian problems")
+    m = length(H.space)
+    nev = min(N_eigen, m)
+    opts = MomedSolveOpts(nev, krylovdim, maxiter, precision === :mixed ? 1 : 0, tol, seed, 1, 0)
+    vals = zeros(Float64, nev)
+    resid = zeros(Float64, nev)
+    vecs = zeros(ComplexF64, m, nev)            # column i = eigenvector i (layout [nev][N] in C)
+    v0 = vec0 === nothing ? C_NULL : pointer(ComplexF64.(vec0))
+    info = MomedInfo()
+    check(H.handle, ccall((:momed_eigsolve, libmomed), Cint,
+                          (Ptr{Cvoid}, Ref{MomedSolveOpts}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{ComplexF64},
+                           Ref{MomedInfo}),
+                          H.handle, opts, v0, vals, resid, vecs, info))
+    return vals, [Vector{Complex{F}}(vecs[:, i]) for i in 1:nev], info
+end
+
+# release_gpu_memory hook: device buffers belong to handles (freed by their finalizers).
+release_gpu_memory(::Val{:b200}, level::Int64 = 2) = (level >= 1 && GC.gc(); nothing)
+
+end # module

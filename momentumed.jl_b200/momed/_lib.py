@@ -71,7 +71,17 @@ SIGNATURES = {
                                     C.c_void_p, C.c_void_p, C.POINTER(Info)]),
     "momed_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "momed_last_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "momed_kernel_launches": (C.c_int64, []),
+    "momed_profile": (C.c_int, [C.c_void_p, C.c_int32]),
+    "momed_profile_read": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
 }
+
+KERNEL_MATVEC_C128, KERNEL_MATVEC_C64, KERNEL_BLOCK_MATVEC_C64, KERNEL_BLOCK_MATVEC_C128 = range(4)
+
+
+def kernel_launches() -> int:
+    """Kernels the library has launched in this process."""
+    return int(lib().momed_kernel_launches())
 
 
 def lib():
@@ -208,6 +218,15 @@ class Handle:
         v = C.c_double()
         self._check(lib().momed_last_kernel_ms(self._h, C.byref(v)))
         return v.value
+
+    def profile(self, enable: bool = True):
+        self._check(lib().momed_profile(self._h, int(enable)))
+
+    def profile_read(self, kind: int = KERNEL_BLOCK_MATVEC_C64):
+        """(launches, summed device ms) of one matvec kernel kind since profile(True)."""
+        n, ms = C.c_int64(), C.c_double()
+        self._check(lib().momed_profile_read(self._h, kind, C.byref(n), C.byref(ms)))
+        return n.value, ms.value
 
     def stats(self):
         nnz, mode, tb = C.c_int64(), C.c_int32(), C.c_int64()

@@ -360,6 +360,27 @@ def hermitian_complete(op: MBOperator) -> ScatterList:
     return ScatterList(amp[order], out[order], in_[order], pm[order], s.bits, s.element_type)
 
 
+def pair_operator(A: MBOperator, B: MBOperator):
+    """Term arrays of H(u) = A + u B on the union of both completed term lists, sorted by (in, out):
+    returns (amp_a, amp_b, in, out, parity).  A term present in one operator only gets amplitude 0
+    in the other.  Used by the batched solver, where u is an interaction strength."""
+    fa, fb = hermitian_complete(A), hermitian_complete(B)
+    keys_a = {(int(i), int(o)): k for k, (i, o) in enumerate(zip(fa.in_, fa.out))}
+    keys_b = {(int(i), int(o)): k for k, (i, o) in enumerate(zip(fb.in_, fb.out))}
+    keys = sorted(set(keys_a) | set(keys_b))
+    amp_a = np.zeros(len(keys), np.complex128)
+    amp_b = np.zeros(len(keys), np.complex128)
+    for n, key in enumerate(keys):
+        if key in keys_a:
+            amp_a[n] = fa.amp[keys_a[key]]
+        if key in keys_b:
+            amp_b[n] = fb.amp[keys_b[key]]
+    in_ = np.array([k[0] for k in keys], np.uint64)
+    out = np.array([k[1] for k in keys], np.uint64)
+    pm = np.array([parity_mask(int(o)) ^ parity_mask(int(i)) for i, o in keys], np.uint64)
+    return amp_a, amp_b, in_, out, pm
+
+
 # ------------------------------------------------------------------------------- containers
 class HilbertSubspace:
     """Sorted list of basis states (hilbert_subspace.jl:19-30); ``list`` is a uint64 array."""

@@ -259,3 +259,65 @@ def test_eigsolve_small_sector_krylov_exhausts(h):
     load(h, basis, full)
     vals, vecs, resid, info = h.eigsolve(len(basis), krylovdim=30, tol=1e-12, seed=4)
     check_eigs(vals, vecs, O.dense_hamiltonian(basis, ofull))
+
+
+# ------------------------------------------------------------------------------ batched solver
+def pair_lists(a, b, seed):
+    from momed.core import pair_operator
+    para, _ = mesh_para(a, b, seed)
+    A = momed.MBOperator(momed.ED_scatterlist_onebody(para), upper_hermitian=True)
+    B = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=True)
+    return pair_operator(A, B)
+
+
+def oracle_list(amp, in_, out, pm):
+    o = np.zeros(len(amp), O.SCAT_DTYPE)
+    o["re"], o["im"], o["out"], o["in"], o["pm"] = amp.real, amp.imag, out, in_, pm
+    return o
+
+
+def test_parametrised_matvec(h):
+    amp_a, amp_b, in_, out, pm = pair_lists(3, 5, 0)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    basis = ref[1]
+    h.set_basis(basis)
+    h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+    x = np.random.default_rng(7).normal(size=len(basis)) + 0.3j
+    for u0 in (0.5, 1.25, 2.0):
+        h.set_param(u0)
+        yo = O.matvec(basis, oracle_list(amp_a + u0 * amp_b, in_, out, pm), x)
+        assert rel(h.matvec(x), yo) < 1e-13
+    h.set_param(1.0)
+
+
+@pytest.mark.parametrize("precision", [momed._lib.PREC_MIXED, momed._lib.PREC_FP64])
+@pytest.mark.parametrize("nu", [8, 32, 5])
+def test_batch_solve_vs_lapack(h, precision, nu):
+    amp_a, amp_b, in_, out, pm = pair_lists(3, 5, 0)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    basis = ref[6]
+    h.set_basis(basis)
+    h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+    u = u_grid(nu, 0.5, 2.0)
+    vals, vecs, resid, info = h.batch_solve(u, 4, krylovdim=30, tol=1e-12, precision=precision, want_vectors=True)
+    assert vals.shape == (nu, 4)
+    for q in range(nu):
+        H = O.dense_hamiltonian(basis, oracle_list(amp_a + u[q] * amp_b, in_, out, pm))
+        check_eigs(vals[q], vecs[q], H, tol_rel=1e-10, overlap_tol=1e-6)
+        assert np.all(resid[q] < 1e-5)
+
+
+def test_batch_solve_3x8_matches_plain_fp64(h):
+    """The 32-wide mixed-precision batch on a 3x8 sector agrees with one-at-a-time FP64 solves."""
+    amp_a, amp_b, in_, out, pm = pair_lists(3, 8, 4)
+    got = h.enumerate_basis(O.mesh_klist(3, 8), (3, 8), 1, 1, (8,), momentum_list=[(0, 2)])
+    basis = got[0][1]
+    h.set_basis(basis)
+    h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+    u = u_grid(32, 0.5, 2.0)
+    vals, _, resid, info = h.batch_solve(u, 4, krylovdim=30, tol=1e-12, precision=momed._lib.PREC_MIXED)
+    for q in (0, 13, 31):
+        h.set_param(float(u[q]))
+        pv, _, pr, pinfo = h.eigsolve(4, krylovdim=30, tol=1e-12, seed=5, want_vectors=False)
+        assert np.max(np.abs(vals[q] - pv) / np.abs(pv)) < 1e-10
+    h.set_param(1.0)
