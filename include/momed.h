@@ -137,6 +137,28 @@ MOMED_API int  momed_stats(momed_handle* h, int64_t* nnz, int32_t* index_mode, i
 /* Device time (ms) of the last matvec kernel launch on the handle's stream. */
 MOMED_API int  momed_last_kernel_ms(momed_handle* h, double* ms);
 
+/* Serving form: a continuous-batching solve server (no reference counterpart: the reference
+ * runs one EDsolve at a time).  `slots` worker contexts, each with its own stream, take
+ * queued requests in arrival order as soon as a slot is free and the request's HBM estimate
+ * fits the budget (0 = 85% of free memory); admitted solves run concurrently on the device.
+ * Requests larger than the budget fail at once with MOMED_ENOMEM.  poll waits at most
+ * wait_ms and returns MOMED_ETIMEOUT when the request is still queued or running;
+ * status: 0 queued, 1 running, 2 done, 3 failed (return code is the failure's), 4 cancelled. */
+typedef struct momed_server momed_server;
+MOMED_API int  momed_serve_start(int device, int32_t slots, int64_t hbm_budget, momed_server** out);
+MOMED_API int  momed_serve_register_operator(momed_server* s, const double* amp_a, const double* amp_b,
+                                             const uint64_t* in, const uint64_t* out, const uint64_t* parity,
+                                             int64_t nscat, int32_t* op_id);
+MOMED_API int  momed_serve_submit(momed_server* s, int32_t op_id, const uint64_t* basis, int64_t n, double u,
+                                  const momed_solve_opts* opts, int64_t* request_id);
+MOMED_API int  momed_serve_cancel(momed_server* s, int64_t request_id);
+MOMED_API int  momed_serve_poll(momed_server* s, int64_t request_id, int32_t wait_ms, int32_t* status,
+                                double* vals, double* resid, momed_info* info, double* queue_s, double* latency_s);
+MOMED_API int  momed_serve_stats(momed_server* s, int64_t* queued, int64_t* completed, int64_t* failed,
+                                 int64_t* hbm_used, int64_t* hbm_budget);
+MOMED_API const char* momed_serve_last_error(momed_server* s);
+MOMED_API int  momed_serve_stop(momed_server* s);
+
 /* Kernels this library has launched in the process so far (all handles). */
 MOMED_API int64_t momed_kernel_launches(void);
 

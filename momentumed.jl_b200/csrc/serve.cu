@@ -1,0 +1,306 @@
+// Serving form: a continuous-batching eigensolve server.
+//
+// Requests (operator id, sector basis, parameter u, nev, tolerance, precision) arrive at any
+// time.  A fixed set of worker slots, each with its own library handle and CUDA stream,
+// takes requests in arrival order as soon as (a) a slot is free and (b) the request's HBM
+// estimate fits the server's budget; every admitted solve keeps its Krylov basis and
+// recurrence coefficients in HBM for its whole life, and the slots' kernels overlap on the
+// device.  A request larger than the whole budget fails at once with MOMED_ENOMEM; a request
+// can be cancelled while queued; every wait the API offers is bounded and returns
+// MOMED_ETIMEOUT when it runs out.
+//
+// A solve is deterministic (seeded start vector, fixed reduction order), so a request's
+// result is the same alone and in any mix.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "momed_internal.cuh"
+
+namespace momed {
+void ensure_ready(momed_handle* h);
+}
+
+using namespace momed;
+
+namespace {
+
+using clock_t_ = std::chrono::steady_clock;
+
+struct HostOperator {
+    std::vector<double> amp_a, amp_b;
+    std::vector<uint64_t> in, out, parity;
+    bool has_b = false;
+};
+
+struct Request {
+    int64_t id = 0;
+    int32_t op = 0;
+    std::vector<uint64_t> basis;
+    double u = 1.0;
+    momed_solve_opts opts{};
+    int64_t bytes = 0;
+    clock_t_::time_point arrival, start, done;
+    int32_t status = 0;          // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
+    int32_t rc = MOMED_OK;
+    std::string err;
+    std::vector<double> vals, resid;
+    momed_info info{};
+};
+
+}  // namespace
+
+struct momed_server {
+    int device = 0;
+    int64_t budget = 0;
+    int64_t used = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<Request>> queue;
+    std::unordered_map<int64_t, std::shared_ptr<Request>> all;
+    std::vector<HostOperator> ops;
+    std::vector<std::thread> workers;
+    std::vector<momed_handle*> handles;
+    int64_t next_id = 1;
+    bool stopping = false;
+    std::string last_error;
+    int64_t completed = 0, failed = 0;
+};
+
+namespace {
+
+// HBM a solve needs: basis, index tables (bounded), Krylov basis, Ritz/refinement buffers.
+int64_t estimate_bytes(int64_t N, const momed_solve_opts& o) {
+    int64_t m = o.krylovdim > 0 ? o.krylovdim : 30;
+    if (m > N) m = N;
+    int64_t nev = o.nev;
+    const bool mixed = o.precision == MOMED_PREC_MIXED;
+    int64_t s = mixed ? 8 : 16;
+    int64_t k1 = nev + (mixed ? 4 : 0);
+    int64_t b = 8 * N;                                // basis
+    b += (m + 1) * N * s;                             // Krylov basis
+    b += (mixed ? 3 * k1 : 0) * N * 16;               // refinement X, W, scratch
+    b += 2 * std::max<int64_t>(nev, 1) * N * 16;      // output vectors + residual workspace
+    b += 16ll << 20;                                  // index tables, term lists, partial sums
+    return b;
+}
+
+void worker_loop(momed_server* S, int slot) {
+    momed_handle* h = S->handles[slot];
+    for (;;) {
+        std::shared_ptr<Request> r;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            // FIFO admission: the head request starts when it fits the free budget
+            S->cv_work.wait(lk, [&] {
+                if (S->stopping) return true;
+                while (!S->queue.empty() && S->queue.front()->status == 4) S->queue.pop_front();
+                return !S->queue.empty() && S->used + S->queue.front()->bytes <= S->budget;
+            });
+            if (S->stopping) return;
+            r = S->queue.front();
+            S->queue.pop_front();
+            S->used += r->bytes;
+            r->status = 1;
+            r->start = clock_t_::now();
+        }
+        int rc = MOMED_OK;
+        std::string err;
+        try {
+            cudaSetDevice(S->device);
+            const HostOperator& op = S->ops[r->op];
+            const int64_t N = (int64_t)r->basis.size();
+            h->basis.resize(std::max<int64_t>(N, 1));
+            MOMED_CUDA_TRY(cudaMemcpyAsync(h->basis.p, r->basis.data(), N * 8, cudaMemcpyHostToDevice, h->stream));
+            h->n = N;
+            h->index_dirty = true;
+            h->op_validated = false;
+            h->basis_or = 0;
+            for (uint64_t v : r->basis) h->basis_or |= v;
+            upload_operator(h, op.amp_a.data(), op.has_b ? op.amp_b.data() : nullptr, op.in.data(), op.out.data(),
+                            op.parity.empty() ? nullptr : op.parity.data(), (int64_t)op.in.size());
+            double u = r->u;
+            float uf = (float)u;
+            MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
+            MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(uf), cudaMemcpyHostToDevice, h->stream));
+            MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+            int nev = (int)std::min<int64_t>(r->opts.nev, N);
+            r->vals.assign(nev, 0.0);
+            r->resid.assign(nev, 0.0);
+            momed_solve_opts o = r->opts;
+            o.want_vectors = 0;
+            rc = momed_eigsolve_impl(h, &o, nullptr, r->vals.data(), r->resid.data(), nullptr, &r->info);
+            if (rc == MOMED_ENOTCONV) rc = MOMED_OK;   // results written; info.converged tells
+        } catch (const Error& e) {
+            rc = e.code;
+            err = e.msg;
+        } catch (const std::exception& e) {
+            rc = MOMED_EINVAL;
+            err = e.what();
+        }
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            r->done = clock_t_::now();
+            r->rc = rc;
+            r->err = err;
+            r->status = rc == MOMED_OK ? 2 : 3;
+            S->used -= r->bytes;
+            if (rc == MOMED_OK) ++S->completed; else ++S->failed;
+        }
+        S->cv_done.notify_all();
+        S->cv_work.notify_all();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+MOMED_API int momed_serve_start(int device, int32_t slots, int64_t hbm_budget, momed_server** out) {
+    if (!out || slots < 1 || slots > 64) return MOMED_EINVAL;
+    *out = nullptr;
+    momed_server* S = new momed_server();
+    S->device = device;
+    size_t freeb = 0, totalb = 0;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) {
+        delete S;
+        return MOMED_ENODEV;
+    }
+    S->budget = hbm_budget > 0 ? std::min<int64_t>(hbm_budget, (int64_t)(freeb * 0.9)) : (int64_t)(freeb * 0.85);
+    for (int i = 0; i < slots; ++i) {
+        momed_handle* h = nullptr;
+        int rc = momed_create(device, &h);
+        if (rc != MOMED_OK) {
+            for (auto* x : S->handles) momed_destroy(x);
+            delete S;
+            return rc;
+        }
+        S->handles.push_back(h);
+    }
+    for (int i = 0; i < slots; ++i) S->workers.emplace_back(worker_loop, S, i);
+    *out = S;
+    return MOMED_OK;
+}
+
+MOMED_API int momed_serve_register_operator(momed_server* S, const double* amp_a, const double* amp_b,
+                                            const uint64_t* in, const uint64_t* out, const uint64_t* parity,
+                                            int64_t nscat, int32_t* op_id) {
+    if (!S || !amp_a || !in || !out || nscat < 0 || !op_id) return MOMED_EINVAL;
+    HostOperator op;
+    op.amp_a.assign(amp_a, amp_a + 2 * nscat);
+    if (amp_b) { op.amp_b.assign(amp_b, amp_b + 2 * nscat); op.has_b = true; }
+    op.in.assign(in, in + nscat);
+    op.out.assign(out, out + nscat);
+    if (parity) op.parity.assign(parity, parity + nscat);
+    else op.parity.clear();
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->ops.push_back(std::move(op));
+    *op_id = (int32_t)S->ops.size() - 1;
+    return MOMED_OK;
+}
+
+MOMED_API int momed_serve_submit(momed_server* S, int32_t op_id, const uint64_t* basis, int64_t n, double u,
+                                 const momed_solve_opts* opts, int64_t* request_id) {
+    if (!S || !basis || n <= 0 || !opts || !request_id || opts->nev < 1) return MOMED_EINVAL;
+    auto r = std::make_shared<Request>();
+    r->op = op_id;
+    r->basis.assign(basis, basis + n);
+    r->u = u;
+    r->opts = *opts;
+    r->bytes = estimate_bytes(n, *opts);
+    r->arrival = clock_t_::now();
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (op_id < 0 || op_id >= (int32_t)S->ops.size()) {
+        S->last_error = "unknown operator id";
+        return MOMED_EINVAL;
+    }
+    r->id = S->next_id++;
+    *request_id = r->id;
+    S->all[r->id] = r;
+    if (r->bytes > S->budget) {   // can never be admitted: refuse now
+        r->status = 3;
+        r->rc = MOMED_ENOMEM;
+        r->err = "request needs " + std::to_string(r->bytes) + " bytes of HBM, budget is " + std::to_string(S->budget);
+        r->done = r->arrival;
+        ++S->failed;
+        S->cv_done.notify_all();
+        return MOMED_OK;
+    }
+    S->queue.push_back(r);
+    S->cv_work.notify_all();
+    return MOMED_OK;
+}
+
+MOMED_API int momed_serve_cancel(momed_server* S, int64_t request_id) {
+    if (!S) return MOMED_EINVAL;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->all.find(request_id);
+    if (it == S->all.end()) return MOMED_EINVAL;
+    if (it->second->status != 0) return MOMED_ESTATE;   // only queued requests can be cancelled
+    it->second->status = 4;
+    it->second->done = clock_t_::now();
+    S->cv_done.notify_all();
+    return MOMED_OK;
+}
+
+// Wait up to wait_ms for the request to finish.  status: 0 queued, 1 running, 2 done,
+// 3 failed, 4 cancelled.  Times in seconds from arrival.  vals/resid (nev each) may be NULL.
+MOMED_API int momed_serve_poll(momed_server* S, int64_t request_id, int32_t wait_ms, int32_t* status, double* vals,
+                               double* resid, momed_info* info, double* queue_s, double* latency_s) {
+    if (!S || !status) return MOMED_EINVAL;
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->all.find(request_id);
+    if (it == S->all.end()) return MOMED_EINVAL;
+    auto r = it->second;
+    auto finished = [&] { return r->status >= 2; };
+    if (wait_ms > 0) S->cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), finished);
+    *status = r->status;
+    if (!finished()) return wait_ms > 0 ? MOMED_ETIMEOUT : MOMED_OK;
+    if (r->status == 3) {
+        S->last_error = r->err;
+        return r->rc;
+    }
+    if (r->status == 2) {
+        for (size_t i = 0; i < r->vals.size(); ++i) {
+            if (vals) vals[i] = r->vals[i];
+            if (resid) resid[i] = r->resid[i];
+        }
+        if (info) *info = r->info;
+    }
+    if (queue_s) *queue_s = std::chrono::duration<double>(r->start - r->arrival).count();
+    if (latency_s) *latency_s = std::chrono::duration<double>(r->done - r->arrival).count();
+    return MOMED_OK;
+}
+
+MOMED_API int momed_serve_stats(momed_server* S, int64_t* queued, int64_t* completed, int64_t* failed,
+                                int64_t* hbm_used, int64_t* hbm_budget) {
+    if (!S) return MOMED_EINVAL;
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (queued) *queued = (int64_t)S->queue.size();
+    if (completed) *completed = S->completed;
+    if (failed) *failed = S->failed;
+    if (hbm_used) *hbm_used = S->used;
+    if (hbm_budget) *hbm_budget = S->budget;
+    return MOMED_OK;
+}
+
+MOMED_API const char* momed_serve_last_error(momed_server* S) { return S ? S->last_error.c_str() : ""; }
+
+MOMED_API int momed_serve_stop(momed_server* S) {
+    if (!S) return MOMED_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stopping = true;
+    }
+    S->cv_work.notify_all();
+    for (auto& t : S->workers) t.join();
+    for (auto* h : S->handles) momed_destroy(h);
+    delete S;
+    return MOMED_OK;
+}
+
+}  // extern "C"

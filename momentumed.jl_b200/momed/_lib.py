@@ -76,7 +76,90 @@ SIGNATURES = {
     "momed_profile_read": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
 }
 
+SIGNATURES.update({
+    "momed_serve_start": (C.c_int, [C.c_int, C.c_int32, C.c_int64, C.POINTER(C.c_void_p)]),
+    "momed_serve_register_operator": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p, C.c_int64, C.POINTER(C.c_int32)]),
+    "momed_serve_submit": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_int64, C.c_double,
+                                     C.POINTER(SolveOpts), C.POINTER(C.c_int64)]),
+    "momed_serve_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
+    "momed_serve_poll": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p,
+                                   C.POINTER(Info), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "momed_serve_stats": (C.c_int, [C.c_void_p] + [C.POINTER(C.c_int64)] * 5),
+    "momed_serve_last_error": (C.c_char_p, [C.c_void_p]),
+    "momed_serve_stop": (C.c_int, [C.c_void_p]),
+})
+
 KERNEL_MATVEC_C128, KERNEL_MATVEC_C64, KERNEL_BLOCK_MATVEC_C64, KERNEL_BLOCK_MATVEC_C128 = range(4)
+QUEUED, RUNNING, DONE, FAILED, CANCELLED = range(5)
+
+
+class Server:
+    """Continuous-batching solve server (momed_serve_*): submit requests any time, poll results."""
+
+    def __init__(self, device: int = 0, slots: int = 4, hbm_budget: int = 0):
+        s = C.c_void_p()
+        rc = lib().momed_serve_start(device, slots, hbm_budget, C.byref(s))
+        if rc != OK:
+            raise MomedError(rc, "momed_serve_start failed")
+        self._s = s
+
+    def _err(self, rc):
+        raise MomedError(rc, lib().momed_serve_last_error(self._s).decode())
+
+    def register_operator(self, amp_a, amp_b, in_, out, parity=None) -> int:
+        a = np.ascontiguousarray(amp_a, np.complex128)
+        b = None if amp_b is None else np.ascontiguousarray(amp_b, np.complex128)
+        i = np.ascontiguousarray(in_, np.uint64)
+        o = np.ascontiguousarray(out, np.uint64)
+        p = None if parity is None else np.ascontiguousarray(parity, np.uint64)
+        op = C.c_int32()
+        rc = lib().momed_serve_register_operator(self._s, _p(a), _p(b), _p(i), _p(o), _p(p), len(a), C.byref(op))
+        if rc != OK:
+            self._err(rc)
+        return op.value
+
+    def submit(self, op_id: int, basis, u: float, nev: int, tol: float = 1e-12, krylovdim: int = 30,
+               maxiter: int = 100, precision: int = PREC_FP64, seed: int = 0) -> int:
+        b = np.ascontiguousarray(basis, np.uint64)
+        opts = SolveOpts(nev, krylovdim, maxiter, precision, tol, seed, 0, 0)
+        rid = C.c_int64()
+        rc = lib().momed_serve_submit(self._s, op_id, _p(b), len(b), float(u), C.byref(opts), C.byref(rid))
+        if rc != OK:
+            self._err(rc)
+        return rid.value
+
+    def cancel(self, rid: int) -> int:
+        return lib().momed_serve_cancel(self._s, rid)
+
+    def poll(self, rid: int, nev: int, wait_ms: int = 0):
+        """(status, vals, resid, info, queue_s, latency_s); raises on a failed request."""
+        st = C.c_int32()
+        vals, resid = np.zeros(nev), np.zeros(nev)
+        info = Info()
+        q, lat = C.c_double(), C.c_double()
+        rc = lib().momed_serve_poll(self._s, rid, wait_ms, C.byref(st), _p(vals), _p(resid), C.byref(info),
+                                    C.byref(q), C.byref(lat))
+        if rc not in (OK, ETIMEOUT):
+            self._err(rc)
+        return st.value, vals, resid, {"converged": info.converged, "matvecs": info.matvecs,
+                                       "seconds": info.seconds}, q.value, lat.value
+
+    def stats(self):
+        v = [C.c_int64() for _ in range(5)]
+        lib().momed_serve_stats(self._s, *[C.byref(x) for x in v])
+        return dict(zip(("queued", "completed", "failed", "hbm_used", "hbm_budget"), (x.value for x in v)))
+
+    def stop(self):
+        if getattr(self, "_s", None):
+            lib().momed_serve_stop(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.stop()
+        except Exception:
+            pass
 
 
 def kernel_launches() -> int:
