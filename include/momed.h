@@ -94,6 +94,21 @@ MOMED_API int  momed_enumeration_copy(momed_handle* h, int64_t* sector_k, int64_
 /* Use sector s of the last enumeration as the working basis (device to device). */
 MOMED_API int  momed_select_sector(momed_handle* h, int64_t s);
 
+/* The basis of ONE momentum sector (total momentum `momentum[dim]`, no mask) written into the
+ * caller's device buffer out_dev[out_capacity], allocating no device memory: for callers that
+ * cannot call cudaMalloc (device memory owned by another allocator such as a Julia CUDA.jl
+ * pool, or services that reserve all HBM up front).  No counterpart in the reference, whose
+ * enumeration runs on the host.  Runs on the current device and the given stream (NULL: the
+ * default stream) and returns after the stream has finished it.  Working space is a static
+ * 148,608-byte device array per GPU, kept until process exit; the first call on a device
+ * looks its address up and should come before any stream capture; calls that overlap on the
+ * GPU race on it.  Limits: momentum box (product of Gk, or of the momentum ranges where
+ * Gk == 0) <= 4096 entries.  *n_states receives the sector size; when it exceeds
+ * out_capacity nothing is written and MOMED_EINVAL is returned. */
+MOMED_API int  momed_enumerate_sector_noalloc(const momed_para* p, const int64_t* N_each, int32_t ncc,
+                                              const int64_t* momentum, uint64_t* out_dev, int64_t out_capacity,
+                                              int64_t* n_states, void* cuda_stream);
+
 /* Working basis: the sorted HilbertSubspace list (hilbert_subspace.jl:19-30), uploaded as in
  * create_gpu_linearmap (MomentumEDCUDAExt.jl:94-113). */
 MOMED_API int  momed_set_basis(momed_handle* h, const uint64_t* basis, int64_t n, int32_t on_device);

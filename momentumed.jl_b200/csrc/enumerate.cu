@@ -16,6 +16,7 @@
 // block and writes every state at its final position.
 #include <algorithm>
 #include <climits>
+#include <mutex>
 #include <numeric>
 
 #include "momed_internal.cuh"
@@ -520,4 +521,202 @@ void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Enumeration of one sector that allocates no device memory.
+//
+// For callers that cannot call cudaMalloc: hosts whose device memory is owned by another
+// allocator (a Julia CUDA.jl memory pool, a framework's caching allocator) that hands this
+// library only the output buffer, and services that reserve all of HBM up front for their
+// solve slots and allow no allocation afterwards.  The caller passes the output buffer; the
+// working space (binomial table, momentum-to-sector table, per-block counts and offsets,
+// error counters and the state count) lives in the static array below, 148,608 bytes that
+// every GPU that loads the library keeps until the process exits.
+//
+// The first call on a device looks the array's device address up (cudaGetSymbolAddress,
+// with that device current); make that first call before any stream capture.  Every call
+// shares the array and it keeps the last call's contents: the error counters and the count
+// are cleared at the start of each call, and calls that overlap on the GPU (two streams, two
+// host threads) race on it.
+// ---------------------------------------------------------------------------------------
+namespace {
+
+constexpr int kNoAllocMaxBox = 4096;      // momentum-box entries (sector table)
+constexpr int kNoAllocMaxBlocks = 8192;   // grid blocks of the count / write passes
+constexpr size_t kNoAllocBinomOff = 0;                                            // uint64 [65 * 65]
+constexpr size_t kNoAllocSecOff = 34048;                                          // int32  [kNoAllocMaxBox]
+constexpr size_t kNoAllocCntOff = kNoAllocSecOff + 4 * kNoAllocMaxBox;            // int32  [kNoAllocMaxBlocks]
+constexpr size_t kNoAllocOffOff = kNoAllocCntOff + 4 * kNoAllocMaxBlocks;         // int64  [kNoAllocMaxBlocks]
+constexpr size_t kNoAllocErrOff = kNoAllocOffOff + 8 * kNoAllocMaxBlocks;         // uint64 [8] errors, [8] total
+constexpr size_t kNoAllocBytes = kNoAllocErrOff + 16 * 8;                         // 148,608 bytes
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// exclusive scan of the per-block counts (one block; nblocks <= kNoAllocMaxBlocks)
+__global__ void k_noalloc_scan(const int32_t* counts, int nblocks, int64_t* offsets, unsigned long long* total) {
+    __shared__ int64_t part[1024];
+    const int t = threadIdx.x;
+    const int per = (nblocks + 1023) / 1024;
+    int64_t s = 0;
+    for (int i = t * per; i < min(nblocks, (t + 1) * per); ++i) s += counts[i];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        int64_t run = 0;
+        for (int i = 0; i < 1024; ++i) { int64_t v = part[i]; part[i] = run; run += v; }
+        *total = (unsigned long long)run;
+    }
+    __syncthreads();
+    int64_t run = part[t];
+    for (int i = t * per; i < min(nblocks, (t + 1) * per); ++i) { offsets[i] = run; run += counts[i]; }
+}
+
+// Device address of the scratch array, looked up once per device (with that device current).
+unsigned char* noalloc_scratch(int dev) {
+    static std::mutex mu;
+    static unsigned char* addr[64] = {nullptr};
+    std::lock_guard<std::mutex> lk(mu);
+    MOMED_REQUIRE(dev >= 0 && dev < 64, MOMED_ENODEV, "device index out of range");
+    if (!addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            throw Error{MOMED_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e)};
+        addr[dev] = static_cast<unsigned char*>(p);
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
 }  // namespace momed
+
+extern "C" MOMED_API int momed_enumerate_sector_noalloc(const momed_para* p, const int64_t* N_each, int32_t ncc,
+                                                        const int64_t* momentum, uint64_t* out_dev,
+                                                        int64_t out_capacity, int64_t* n_states, void* cuda_stream) {
+    using namespace momed;
+    try {
+        MOMED_REQUIRE(p && p->k_list && p->Gk && N_each && momentum && n_states, MOMED_EINVAL, "null argument");
+        MOMED_REQUIRE(ncc == p->Nc_conserve && ncc >= 1 && ncc <= kMaxComp, MOMED_EINVAL,
+                      "length of N_each must equal Nc_conserve (<= 8)");
+        MOMED_REQUIRE(p->dim >= 1 && p->dim <= 3, MOMED_EINVAL, "dim must be 1..3");
+        const int dim = p->dim, Nk = p->Nk, ncomp_bits = Nk * p->Nc_mix;
+        MOMED_REQUIRE(Nk >= 1 && (int64_t)ncomp_bits * ncc <= 64, MOMED_EINVAL, "Nk * Nc must be <= 64");
+        int dev = 0;
+        MOMED_CUDA_TRY(cudaGetDevice(&dev));
+        unsigned char* scratch = noalloc_scratch(dev);
+        cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+
+        // kernel parameters, planned on the stack (no heap, no device allocation)
+        EnumParams P{};
+        P.ncomp = ncc;
+        P.dim = dim;
+        for (int d = 0; d < dim; ++d) P.Gk[d] = (int32_t)p->Gk[d];
+        int64_t total = 1;
+        for (int c = 0; c < ncc; ++c) {
+            Comp& C = P.comp[c];
+            int64_t Nc = N_each[c];
+            C.t = (int32_t)(Nc < 0 ? -Nc : Nc);
+            C.shift = c * ncomp_bits;
+            C.masked = 0;
+            C.len = ncomp_bits;
+            for (int i = 0; i < ncomp_bits; ++i) C.pos[i] = (int8_t)i;
+            MOMED_REQUIRE(C.t <= ncomp_bits, MOMED_EINVAL, "Invalid number of electrons in one component");
+            C.count = hbinom(C.len, C.t);
+            C.stride = total;
+            MOMED_REQUIRE(C.count == 0 || total <= (int64_t(1) << 62) / std::max<int64_t>(C.count, 1), MOMED_EINVAL,
+                          "combination space too large");
+            total *= C.count;
+            int sgn = Nc > 0 ? 1 : (Nc < 0 ? -1 : 0);
+            for (int i = 0; i < ncomp_bits; ++i)
+                for (int d = 0; d < dim; ++d) P.kv[C.shift + i][d] = sgn * (int32_t)p->k_list[d + dim * (i % Nk)];
+        }
+        P.total = total;
+        int64_t box_n = 1;
+        int64_t target = 0, tstride = 1;
+        bool target_in = true;
+        for (int d = 0; d < dim; ++d) {
+            if (p->Gk[d] != 0) {
+                P.box_lo[d] = 0;
+                P.box_ext[d] = (int32_t)p->Gk[d];
+            } else {
+                int64_t lo = 0, hi = 0;
+                for (int c = 0; c < ncc; ++c) {
+                    int64_t v[64];
+                    int nv = P.comp[c].len;
+                    for (int i = 0; i < nv; ++i) v[i] = P.kv[P.comp[c].shift + i][d];
+                    for (int a = 1; a < nv; ++a) {   // insertion sort
+                        int64_t x = v[a];
+                        int b = a - 1;
+                        while (b >= 0 && v[b] > x) { v[b + 1] = v[b]; --b; }
+                        v[b + 1] = x;
+                    }
+                    for (int i = 0; i < P.comp[c].t && i < nv; ++i) { lo += v[i]; hi += v[nv - 1 - i]; }
+                }
+                P.box_lo[d] = (int32_t)lo;
+                P.box_ext[d] = (int32_t)(hi - lo + 1);
+            }
+            box_n *= P.box_ext[d];
+            MOMED_REQUIRE(box_n <= kNoAllocMaxBox, MOMED_EINVAL,
+                          "momentum box exceeds the 4096-entry table of the no-allocation enumerator");
+            int64_t k = p->Gk[d] == 0 ? momentum[d] : jmod(momentum[d], p->Gk[d]);
+            int64_t v = k - P.box_lo[d];
+            if (v < 0 || v >= P.box_ext[d]) target_in = false;
+            target += v * tstride;
+            tstride *= P.box_ext[d];
+        }
+        int32_t sec_of[kNoAllocMaxBox];
+        for (int64_t i = 0; i < box_n; ++i) sec_of[i] = -1;
+        if (target_in) sec_of[target] = 0;
+        uint64_t binom[65 * 65];
+        for (int n = 0; n <= 64; ++n)
+            for (int k = 0; k <= 64; ++k) binom[n * 65 + k] = k <= n ? (uint64_t)hbinom(n, k) : 0ull;
+        int nblocks = 1;
+        P.chunk = 16;
+        if (total > 0) {
+            P.chunk = std::max<int64_t>(16, (total + (int64_t)kNoAllocMaxBlocks * kThreads - 1) /
+                                                ((int64_t)kNoAllocMaxBlocks * kThreads));
+            int64_t nthreads = (total + P.chunk - 1) / P.chunk;
+            nblocks = (int)((nthreads + kThreads - 1) / kThreads);
+        }
+        MOMED_REQUIRE(nblocks <= kNoAllocMaxBlocks, MOMED_EINVAL, "combination space too large for the scratch");
+
+        auto* d_binom = reinterpret_cast<uint64_t*>(scratch + kNoAllocBinomOff);
+        auto* d_sec = reinterpret_cast<int32_t*>(scratch + kNoAllocSecOff);
+        auto* d_cnt = reinterpret_cast<int32_t*>(scratch + kNoAllocCntOff);
+        auto* d_off = reinterpret_cast<int64_t*>(scratch + kNoAllocOffOff);
+        auto* d_err = reinterpret_cast<unsigned long long*>(scratch + kNoAllocErrOff);
+        MOMED_CUDA_TRY(cudaMemcpyAsync(d_binom, binom, sizeof(binom), cudaMemcpyHostToDevice, st));
+        MOMED_CUDA_TRY(cudaMemcpyAsync(d_sec, sec_of, box_n * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        MOMED_CUDA_TRY(cudaMemsetAsync(d_err, 0, 16 * 8, st));   // the previous call's errors and total
+        P.binom = d_binom;
+        P.sec_of = d_sec;
+        P.box_n = box_n;
+        P.out_cap = 0;
+        P.err = d_err;
+        unsigned long long res[16] = {0};
+        if (total > 0 && target_in) {
+            k_enum_count<<<nblocks, kThreads, 0, st>>>(P, 0, 1, d_cnt);
+            k_noalloc_scan<<<1, 1024, 0, st>>>(d_cnt, nblocks, d_off, d_err + 8);
+            MOMED_CUDA_TRY(cudaGetLastError());
+            note_launches(2);
+            MOMED_CUDA_TRY(cudaMemcpyAsync(res, d_err, sizeof(res), cudaMemcpyDeviceToHost, st));
+            MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+        const int64_t n = (int64_t)res[8];
+        *n_states = n;
+        if (n > out_capacity) return MOMED_EINVAL;   // *n_states tells the caller the size needed
+        if (n > 0) {
+            MOMED_REQUIRE(out_dev, MOMED_EINVAL, "null output buffer");
+            P.out_cap = out_capacity;
+            k_enum_write<<<nblocks, kThreads, 0, st>>>(P, 0, 1, d_off, out_dev);
+            MOMED_CUDA_TRY(cudaGetLastError());
+            note_launches(1);
+            MOMED_CUDA_TRY(cudaMemcpyAsync(res, d_err, 8 * 8, cudaMemcpyDeviceToHost, st));
+            MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+            MOMED_REQUIRE(res[0] == 0, MOMED_ECUDA, "basis enumeration skipped out-of-range accesses");
+        }
+        return MOMED_OK;
+    } catch (const Error& e) {
+        return e.code;
+    }
+}

@@ -59,6 +59,8 @@ SIGNATURES = {
                                         C.c_void_p, C.c_int32, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
     "momed_enumeration_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]),
     "momed_select_sector": (C.c_int, [C.c_void_p, C.c_int64]),
+    "momed_enumerate_sector_noalloc": (C.c_int, [C.POINTER(Para), C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p,
+                                                 C.c_int64, C.POINTER(C.c_int64), C.c_void_p]),
     "momed_set_basis": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int32]),
     "momed_set_scatter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64]),
     "momed_set_scatter_pair": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
