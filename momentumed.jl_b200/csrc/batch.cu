@@ -104,19 +104,31 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ W
     }
 }
 
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// one warp per (column, right-hand side) element; fixed reduction order
 template <int NB>
 __global__ void k_breduce(const double2* partial, int grid, int ncols1, double2* out, const int* active_any) {
     if (active_any && *active_any == 0) return;
-    for (int e = threadIdx.x; e < ncols1 * NB; e += blockDim.x) {
-        double sx = 0.0, sy = 0.0;
-        for (int b = 0; b < grid; ++b) {
-            double2 v = partial[(int64_t)b * (kMaxCols + 1) * NB + e];
-            sx += v.x;
-            sy += v.y;
-        }
-        out[e] = make_double2(sx, sy);
+    const int lane = threadIdx.x & 31;
+    const int e = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (e >= ncols1 * NB) return;
+    double sx = 0.0, sy = 0.0;
+    for (int b = lane; b < grid; b += 32) {
+        double2 v = partial[(int64_t)b * (kMaxCols + 1) * NB + e];
+        sx += v.x;
+        sy += v.y;
     }
+    sx = wsum(sx);
+    sy = wsum(sy);
+    if (lane == 0) out[e] = make_double2(sx, sy);
 }
+
+inline int breduce_grid(int ncols1, int nb) { return (ncols1 * nb + 7) / 8; }
 
 // W[n][r] -= sum_i coef[i][r] V_i[n][r] for active r; per-block |W_r|^2 partials
 template <typename VT, int NB>
@@ -154,16 +166,18 @@ k_bupdate(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restr
     if (threadIdx.x < NB) npartial[(int64_t)blockIdx.x * NB + threadIdx.x] = nrm[threadIdx.x];
 }
 
+// launched with NB warps: warp r reduces the norm partials of right-hand side r
 template <int NB>
 __global__ void k_bdecide(const double2* coefA, int ncols, const double* npartial, int grid, int* flag, int* any,
                           double* after) {
     __shared__ int s_any;
     if (threadIdx.x == 0) s_any = 0;
     __syncthreads();
-    int r = threadIdx.x;
-    if (r < NB) {
-        double a = 0.0;
-        for (int b = 0; b < grid; ++b) a += npartial[(int64_t)b * NB + r];
+    const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+    double a = 0.0;
+    for (int b = lane; b < grid; b += 32) a += npartial[(int64_t)b * NB + r];
+    a = wsum(a);
+    if (lane == 0) {
         double before = coefA[ncols * NB + r].x;
         after[r] = a;
         int f = (a < 0.5 * before) ? 1 : 0;
@@ -178,16 +192,18 @@ template <int NB>
 __global__ void k_bfinalize(const double2* coefA, const double2* coefB, int ncols, const double* npartial2, int grid,
                             const int* flag, const int* any, const double* after, double* scal, double* alpha,
                             double* beta, int j, int m) {
-    int r = threadIdx.x;
-    if (r >= NB) return;
-    bool second = (*any != 0) && flag[r];
-    double a = coefA[(ncols - 1) * NB + r].x + (second ? coefB[(ncols - 1) * NB + r].x : 0.0);
-    double wn2 = after[r];
-    if (*any != 0) {
-        double s = 0.0;
-        for (int b = 0; b < grid; ++b) s += npartial2[(int64_t)b * NB + r];
-        wn2 = s;   // second pass recomputed every r's norm (inactive r unchanged)
+    // launched with NB warps: warp r finalises right-hand side r
+    const int lane = threadIdx.x & 31, r = threadIdx.x >> 5;
+    const bool anyp = *any != 0;
+    double s = 0.0;
+    if (anyp) {   // uniform: the second pass recomputed every r's norm (inactive r unchanged)
+        for (int b = lane; b < grid; b += 32) s += npartial2[(int64_t)b * NB + r];
+        s = wsum(s);
     }
+    if (lane != 0) return;
+    bool second = anyp && flag[r];
+    double a = coefA[(ncols - 1) * NB + r].x + (second ? coefB[(ncols - 1) * NB + r].x : 0.0);
+    double wn2 = anyp ? s : after[r];
     double bt = sqrt(max(wn2, 0.0));
     alpha[r * m + j] = a;
     beta[r * m + j] = bt;
@@ -218,13 +234,21 @@ __global__ void k_brandom(VT* v, int64_t total, uint64_t seed) {
     }
 }
 
-// out[i][n][r] = sum_a U[r][i][a] V[a][n][r]  (U: [NB][nout][m]), optionally out[nout] = V[copy_col]
-template <typename VIN, typename VOUT, int NB, int TR>
+// out[i][n][r] = sum_a U[i][a][r] V[a][n][r]  (U: [nout][m][NB], r fastest so a warp's coefficient
+// loads are coalesced), optionally out[nout] = V[copy_col].  A tile of TR rows x (m+1) columns is
+// staged in shared memory; each thread owns RPT rows of one right-hand side and accumulates OC
+// outputs at a time in registers.  In place (out == V) is safe: a tile is read whole before any
+// of its rows is written.
+template <typename VIN, typename VOUT, int NB, int RPT>
 __global__ void __launch_bounds__(kT)
 k_bcombine(const VIN* V, int64_t N, int m, const double* __restrict__ U, int nout, VOUT* out, int copy_col) {
+    constexpr int TPR = kT / NB;        // row slots per pass
+    constexpr int TR = TPR * RPT;       // rows per tile
+    constexpr int OC = 8;               // outputs per register chunk
     extern __shared__ unsigned char smem_raw[];
     VIN* tile = reinterpret_cast<VIN*>(smem_raw);   // [(m + 1)][TR][NB]
     const int ncopy = copy_col >= 0 ? 1 : 0;
+    const int r = threadIdx.x % NB, tl = threadIdx.x / NB;
     for (int64_t t0 = (int64_t)blockIdx.x * TR; t0 < N; t0 += (int64_t)gridDim.x * TR) {
         const int rows = (int)((N - t0) < TR ? (N - t0) : TR);
         for (int e = threadIdx.x; e < (m + ncopy) * TR * NB; e += kT) {
@@ -237,19 +261,37 @@ k_bcombine(const VIN* V, int64_t N, int m, const double* __restrict__ U, int nou
             tile[e] = (t < rows) ? V[(int64_t)col * N * NB + (t0 + t) * NB + (rem % NB)] : z;
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < nout * TR * NB; e += kT) {
-            int i = e / (TR * NB), rem = e % (TR * NB);
-            int t = rem / NB, r = rem % NB;
-            if (t < rows) {
-                const double* u = U + ((int64_t)r * nout + i) * m;
-                double sx = 0.0, sy = 0.0;
-                for (int a = 0; a < m; ++a) {
-                    double2 v = to2(tile[(a * TR + t) * NB + r]);
-                    double cf = __ldg(u + a);
-                    sx += cf * v.x;
-                    sy += cf * v.y;
+        for (int c0 = 0; c0 < nout; c0 += OC) {
+            double ax[RPT][OC], ay[RPT][OC];
+#pragma unroll
+            for (int j = 0; j < RPT; ++j)
+#pragma unroll
+                for (int k = 0; k < OC; ++k) { ax[j][k] = 0.0; ay[j][k] = 0.0; }
+            for (int a = 0; a < m; ++a) {
+                double u[OC];
+#pragma unroll
+                for (int k = 0; k < OC; ++k)
+                    u[k] = (c0 + k < nout) ? __ldg(U + ((int64_t)(c0 + k) * m + a) * NB + r) : 0.0;
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) {
+                    double2 v = to2(tile[(a * TR + tl + j * TPR) * NB + r]);
+#pragma unroll
+                    for (int k = 0; k < OC; ++k) {
+                        ax[j][k] += u[k] * v.x;
+                        ay[j][k] += u[k] * v.y;
+                    }
                 }
-                out[(int64_t)i * N * NB + (t0 + t) * NB + r] = fr2<VOUT>(make_double2(sx, sy));
+            }
+#pragma unroll
+            for (int j = 0; j < RPT; ++j) {
+                const int t = tl + j * TPR;
+                if (t < rows) {
+#pragma unroll
+                    for (int k = 0; k < OC; ++k)
+                        if (c0 + k < nout)
+                            out[(int64_t)(c0 + k) * N * NB + (t0 + t) * NB + r] =
+                                fr2<VOUT>(make_double2(ax[j][k], ay[j][k]));
+                }
             }
         }
         if (ncopy) {
@@ -345,7 +387,7 @@ struct BlockLanczos {
 
     void proj(int ncols, const VT* w, double2* out, const int* act) {
         k_bproj<VT, NB><<<grid, kT, 0, st>>>(V.p, N, ncols, w, partial.p, act);
-        k_breduce<NB><<<1, 256, 0, st>>>(partial.p, grid, ncols + 1, out, act);
+        k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(partial.p, grid, ncols + 1, out, act);
         launches += 2;
     }
     void update(int ncols, const double2* coef, VT* w, const int* active, const int* act) {
@@ -367,10 +409,10 @@ struct BlockLanczos {
         const int nc = j + 1;
         proj(nc, w, coefA.p, nullptr);
         update(nc, coefA.p, w, nullptr, nullptr);
-        k_bdecide<NB><<<1, 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p);
+        k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p);
         proj(nc, w, coefB.p, any.p);
         update(nc, coefB.p, w, flag.p, any.p);
-        k_bfinalize<NB><<<1, 32, 0, st>>>(coefA.p, coefB.p, nc, npart.p, ugrid, flag.p, any.p, after.p, scal.p,
+        k_bfinalize<NB><<<1, NB * 32, 0, st>>>(coefA.p, coefB.p, nc, npart.p, ugrid, flag.p, any.p, after.p, scal.p,
                                           alpha.p, beta.p, j, m);
         k_bscale<VT, NB><<<ugrid, kT, 0, st>>>(w, N, scal.p);
         launches += 3;
@@ -378,12 +420,25 @@ struct BlockLanczos {
     template <typename VOUT>
     void combine(const std::vector<double>& Uh, int nout, VOUT* out, int copy_col, int mm) {
         MOMED_CUDA_TRY(cudaMemcpyAsync(Ud.p, Uh.data(), Uh.size() * 8, cudaMemcpyHostToDevice, st));
-        constexpr int TR = (NB >= 16) ? 4 : 16;
-        size_t smem = (size_t)(mm + 1) * TR * NB * sizeof(VT);
-        auto k = k_bcombine<VT, VOUT, NB, TR>;
-        MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms() * 2));
-        k<<<g, kT, smem, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
+        constexpr int TPR = kT / NB;
+        const size_t per_row = (size_t)(mm + 1) * NB * sizeof(VT);
+        const size_t limit = 200 * 1024;
+        if (per_row * TPR * 2 <= limit) {
+            constexpr int TR = TPR * 2;
+            size_t smem = per_row * TR;
+            auto k = k_bcombine<VT, VOUT, NB, 2>;
+            MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms()));
+            k<<<g, kT, smem, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
+        } else {
+            constexpr int TR = TPR;
+            size_t smem = per_row * TR;
+            MOMED_REQUIRE(smem <= 227 * 1024, MOMED_EINVAL, "krylovdim too large for the batched restart tile");
+            auto k = k_bcombine<VT, VOUT, NB, 1>;
+            MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms()));
+            k<<<g, kT, smem, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
+        }
         MOMED_CUDA_TRY(cudaGetLastError());
         MOMED_CUDA_TRY(cudaStreamSynchronize(st));
         ++launches;
@@ -398,9 +453,12 @@ struct BlockLanczos {
     };
 
     // Lockstep thick-restart Lanczos for all NB right-hand sides.  vectors: [nwant][N][NB] c128.
-    Out run(int nev, int nu, double tol, double rel_floor, int maxiter, uint64_t seed, int nwant, double2* vectors) {
+    // start: optional device block [N][NB] of start vectors (normalised here); else random from seed
+    Out run(int nev, int nu, double tol, double rel_floor, int maxiter, uint64_t seed, int nwant, double2* vectors,
+            const VT* start = nullptr) {
         Out out;
-        k_brandom<VT><<<ugrid, kT, 0, st>>>(col(0), N * NB, seed);
+        if (start) MOMED_CUDA_TRY(cudaMemcpyAsync(col(0), start, (size_t)N * NB * sizeof(VT), cudaMemcpyDeviceToDevice, st));
+        else k_brandom<VT><<<ugrid, kT, 0, st>>>(col(0), N * NB, seed);
         normalize(col(0));
         std::vector<std::vector<double>> kept(NB), arrow(NB);
         std::vector<double> ha((size_t)NB * m), hb((size_t)NB * m);
@@ -463,7 +521,7 @@ struct BlockLanczos {
                     std::vector<double> Uh((size_t)NB * nv * m);
                     for (int r = 0; r < NB; ++r)
                         for (int i = 0; i < nv; ++i)
-                            for (int a = 0; a < m; ++a) Uh[((size_t)r * nv + i) * m + a] = U[r][(size_t)a * m + i];
+                            for (int a = 0; a < m; ++a) Uh[((size_t)i * m + a) * NB + r] = U[r][(size_t)a * m + i];
                     combine<double2>(Uh, nv, vectors, -1, m);
                 }
                 return out;
@@ -476,7 +534,7 @@ struct BlockLanczos {
             std::vector<double> Uh((size_t)NB * keep * m);
             for (int r = 0; r < NB; ++r) {
                 for (int i = 0; i < keep; ++i)
-                    for (int a = 0; a < m; ++a) Uh[((size_t)r * keep + i) * m + a] = U[r][(size_t)a * m + i];
+                    for (int a = 0; a < m; ++a) Uh[((size_t)i * m + a) * NB + r] = U[r][(size_t)a * m + i];
                 kept[r].assign(th[r].begin(), th[r].begin() + keep);
                 arrow[r].resize(keep);
                 double bl = hb[(size_t)r * m + m - 1];
@@ -506,6 +564,21 @@ __global__ void k_bcombine_c(const double2* __restrict__ X, int64_t N, int k, co
             }
             out[(int64_t)i * total + e] = make_double2(sx, sy);
         }
+    }
+}
+
+// out[n][r] = sum_{i < k} X[i][n][r]  (warm-start block from refined Ritz vectors)
+template <int NB>
+__global__ void k_bsum(const double2* __restrict__ X, int64_t N, int k, double2* __restrict__ out) {
+    const int64_t total = N * NB;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        double sx = 0.0, sy = 0.0;
+        for (int i = 0; i < k; ++i) {
+            double2 x = X[(int64_t)i * total + e];
+            sx += x.x;
+            sy += x.y;
+        }
+        out[e] = make_double2(sx, sy);
     }
 }
 
@@ -606,7 +679,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
             for (int i = 0; i < k1; ++i) {
                 const double2* rhs = (pass == 0 ? Wb.p : Xb.p) + (size_t)i * stride;
                 k_bproj<double2, NB><<<grid, kT, 0, st>>>(Xb.p, N, k1, rhs, part.p, nullptr);
-                k_breduce<NB><<<1, 256, 0, st>>>(part.p, grid, k1 + 1, red.p, nullptr);
+                k_breduce<NB><<<breduce_grid(k1 + 1, NB), 256, 0, st>>>(part.p, grid, k1 + 1, red.p, nullptr);
                 note_launches(2);
                 MOMED_CUDA_TRY(cudaMemcpyAsync(hr.data(), red.p, hr.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
                 MOMED_CUDA_TRY(cudaStreamSynchronize(st));
@@ -671,10 +744,11 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                 rs[q][i] = std::sqrt(s);
             }
     }
-    // acceptance per parameter; the rest is finished by the single-vector FP64 solver
+    // acceptance per parameter
     int converged_min = nev;
     DevBuf<double2> X1;
     X1.resize((size_t)std::max(k1, nev) * N);
+    std::vector<int> okv(NB, 0), convv(NB, 0);
     for (int q = 0; q < nu; ++q) {
         int conv = 0;
         bool ok = !broken[q];
@@ -696,11 +770,75 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                 ok = ok && good;
             }
         }
-        k_extract<NB><<<eg, 256, 0, st>>>(Xb.p, N, k1, q, X1.p);
+        okv[q] = ok ? 1 : 0;
+        convv[q] = conv;
+    }
+    // Parameters that missed the target are finished together: a lockstep FP64 block Lanczos
+    // warm-started, per parameter, from the sum of its refined Ritz vectors.
+    int nfail = 0;
+    for (int q = 0; q < nu; ++q) nfail += (!okv[q] && !broken[q]) ? 1 : 0;
+    DevBuf<double2> X3;
+    std::vector<std::vector<double>> th3, rs3(NB, std::vector<double>(nev, 0.0));
+    std::vector<int> nconv3(NB, 0), broken3(NB, 0);
+    if (nfail > 0) {
+        DevBuf<double2> v0;
+        v0.resize((size_t)stride);
+        k_bsum<NB><<<eg, 256, 0, st>>>(Xb.p, N, k1, v0.p);
+        MOMED_CUDA_TRY(cudaGetLastError());
+        X3.resize((size_t)nev * stride);
+        BlockLanczos<double2, NB> L3(h, m, uv);
+        auto r3 = L3.run(nev, nu, tol, 0.0, maxiter, o->seed, nev, X3.p, v0.p);
+        matvecs += r3.steps * nu;
+        matvecs64 += r3.steps * nu;
+        restarts += r3.restarts;
+        note_launches(L3.launches + 1);
+        th3 = r3.theta;
+        nconv3 = r3.nconv;
+        broken3 = r3.broken;
+        // FP64 residuals of the phase-3 pairs
+        for (int i = 0; i < nev; ++i)
+            BlockMv<double2>::run(h, X3.p + (size_t)i * stride, Wb.p + (size_t)i * stride, ud64.p, NB);
+        matvecs += (int64_t)nev * nu;
+        matvecs64 += (int64_t)nev * nu;
+        const int rg = std::max(1, std::min<int>((int)((stride + 255) / 256), 512));
+        DevBuf<double> thd, part;
+        thd.resize((size_t)NB * nev);
+        part.resize((size_t)rg * nev * NB);
+        std::vector<double> thh((size_t)NB * nev, 0.0);
+        for (int q = 0; q < nu; ++q)
+            for (int i = 0; i < nev; ++i) thh[(size_t)q * nev + i] = th3[q][i];
+        MOMED_CUDA_TRY(cudaMemcpyAsync(thd.p, thh.data(), thh.size() * 8, cudaMemcpyHostToDevice, st));
+        k_bresid<NB><<<rg, 256, 0, st>>>(Wb.p, X3.p, N, nev, thd.p, part.p);
+        note_launches(1);
+        MOMED_CUDA_TRY(cudaGetLastError());
+        std::vector<double> hp((size_t)rg * nev * NB);
+        MOMED_CUDA_TRY(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 8, cudaMemcpyDeviceToHost, st));
+        MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int q = 0; q < nu; ++q)
+            for (int i = 0; i < nev; ++i) {
+                double s = 0.0;
+                for (int b = 0; b < rg; ++b) s += hp[((size_t)b * nev + i) * NB + q];
+                rs3[q][i] = std::sqrt(s);
+            }
+    }
+    for (int q = 0; q < nu; ++q) {
+        const bool from3 = !okv[q] && !broken[q] && !broken3[q];
+        int conv = convv[q];
+        if (from3) {
+            k_extract<NB><<<eg, 256, 0, st>>>(X3.p, N, nev, q, X1.p);
+        } else {
+            k_extract<NB><<<eg, 256, 0, st>>>(Xb.p, N, k1, q, X1.p);
+        }
         note_launches(1);
         MOMED_CUDA_TRY(cudaGetLastError());
         std::vector<double> tq(th[q].begin(), th[q].begin() + nev), rq(rs[q].begin(), rs[q].begin() + nev);
-        if (!ok) {
+        if (from3) {
+            tq.assign(th3[q].begin(), th3[q].begin() + nev);
+            rq = rs3[q];
+            conv = 0;
+            while (conv < nev && (conv < nconv3[q] || rq[conv] <= tol)) ++conv;
+        } else if (!okv[q]) {
+            // invariant Krylov space: this parameter is solved on its own by the single-vector solver
             double uq = uv[q];
             float uf = (float)uq;
             MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &uq, sizeof(double), cudaMemcpyHostToDevice, st));
@@ -709,23 +847,8 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
             o2.precision = MOMED_PREC_FP64;
             o2.want_vectors = 1;
             o2.vecs_on_device = 1;
-            std::vector<double2> hx;
-            const double* v0 = nullptr;
-            if (!broken[q]) {   // warm start from the sum of this parameter's refined vectors
-                std::vector<double> ones(k1, 1.0);
-                DevBuf<double> od;
-                DevBuf<double2> v0d;
-                od.resize(k1);
-                v0d.resize(N);
-                MOMED_CUDA_TRY(cudaMemcpyAsync(od.p, ones.data(), k1 * 8, cudaMemcpyHostToDevice, st));
-                vec_combine<double2, double2>(X1.p, N, k1, od.p, 1, v0d.p, N, -1, st);
-                hx.resize(N);
-                MOMED_CUDA_TRY(cudaMemcpyAsync(hx.data(), v0d.p, N * sizeof(double2), cudaMemcpyDeviceToHost, st));
-                MOMED_CUDA_TRY(cudaStreamSynchronize(st));
-                v0 = reinterpret_cast<const double*>(hx.data());
-            }
             momed_info i2{};
-            momed_eigsolve_impl(h, &o2, v0, tq.data(), rq.data(), X1.p, &i2);
+            momed_eigsolve_impl(h, &o2, nullptr, tq.data(), rq.data(), X1.p, &i2);
             matvecs += i2.matvecs;
             matvecs64 += i2.matvecs_fp64;
             restarts += i2.restarts;

@@ -300,7 +300,9 @@ k_block_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x,
     const C2* __restrict__ B = amp_b<R>(ov);
     for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
         const uint64_t s = __ldg(iv.basis + row);
-        R ar = 0, ai = 0;
+        R ar = 0, ai = 0;        // A (and A + uB) contributions of this lane's right-hand side
+        R br = 0, bi = 0;        // B-only contributions, scaled by u at the end
+        R dax = 0, day = 0, dbx = 0, dby = 0;   // diagonal amplitudes met by this lane
         for_each_group_batch(s, ov, [&](int g) {
             int total = stage_batch(g, ov, ws);
             int gi = 0;
@@ -310,6 +312,17 @@ k_block_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x,
                 int t = 0;
                 bool neg = false;
                 if (f < total) j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
+                if (j == row) {   // diagonal term: its target is the row itself
+                    C2 a = load_amp(A, t);
+                    dax += a.x;
+                    day += a.y;
+                    if (HAS_B) {
+                        C2 b = load_amp(B, t);
+                        dbx += b.x;
+                        dby += b.y;
+                    }
+                    j = -1;
+                }
                 unsigned hm = __ballot_sync(kFull, j >= 0);
                 if (j >= 0) {
                     int k = __popc(hm & ((1u << lane) - 1u));
@@ -328,18 +341,47 @@ k_block_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x,
                 for (int k = sub; k < nh; k += NSUB) {
                     uint32_t jj = hs.j[k];
                     C2 a = hs.a[k];
+                    C2 xv = x[(int64_t)jj * NB + r];
                     if (HAS_B) {
                         C2 b = hs.b[k];
+                        if (a.x == R(0) && a.y == R(0)) {     // same hit on every lane: uniform branch
+                            br += b.x * xv.x - b.y * xv.y;
+                            bi += b.x * xv.y + b.y * xv.x;
+                            continue;
+                        }
                         a.x += ur * b.x;
                         a.y += ur * b.y;
                     }
-                    C2 xv = x[(int64_t)jj * NB + r];
                     ar += a.x * xv.x - a.y * xv.y;
                     ai += a.x * xv.y + a.y * xv.x;
                 }
                 __syncwarp();
             }
         });
+        if (HAS_B) {
+            ar += ur * br;
+            ai += ur * bi;
+        }
+        // diagonal part, applied once per row
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dax += __shfl_xor_sync(kFull, dax, o);
+            day += __shfl_xor_sync(kFull, day, o);
+            if (HAS_B) {
+                dbx += __shfl_xor_sync(kFull, dbx, o);
+                dby += __shfl_xor_sync(kFull, dby, o);
+            }
+        }
+        if (sub == 0) {
+            R cx = dax, cy = day;
+            if (HAS_B) {
+                cx += ur * dbx;
+                cy += ur * dby;
+            }
+            C2 xd = x[row * NB + r];
+            ar += cx * xd.x - cy * xd.y;
+            ai += cx * xd.y + cy * xd.x;
+        }
 #pragma unroll
         for (int o = NB; o < 32; o <<= 1) {
             ar += __shfl_xor_sync(kFull, ar, o);

@@ -90,17 +90,22 @@ k_proj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ w,
     }
 }
 
+// One warp per column: lanes stride over the blocks' partials, then a fixed shuffle tree
+// (deterministic order).
 __global__ void k_reduce(const double2* partial, int grid, int ncols1, double2* out, const int* active) {
     if (active && *active == 0) return;
-    for (int i = threadIdx.x; i < ncols1; i += blockDim.x) {
-        double sx = 0.0, sy = 0.0;
-        for (int b = 0; b < grid; ++b) {
-            double2 v = partial[(int64_t)b * (kMaxCols + 1) + i];
-            sx += v.x;
-            sy += v.y;
-        }
-        out[i] = make_double2(sx, sy);
+    const int lane = threadIdx.x & 31;
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (i >= ncols1) return;
+    double sx = 0.0, sy = 0.0;
+    for (int b = lane; b < grid; b += 32) {
+        double2 v = partial[(int64_t)b * (kMaxCols + 1) + i];
+        sx += v.x;
+        sy += v.y;
     }
+    sx = warp_sum(sx);
+    sy = warp_sum(sy);
+    if (lane == 0) out[i] = make_double2(sx, sy);
 }
 
 template <typename VT>
@@ -138,27 +143,31 @@ k_update(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restri
     }
 }
 
+// Warp-wide sum of the per-block norm partials (call with all 32 lanes).
 __device__ double sum_norm_partials(const double2* partial, int grid) {
     double s = 0.0;
-    for (int b = 0; b < grid; ++b) s += partial[(int64_t)b * (kMaxCols + 1)].x;
-    return s;
+    for (int b = threadIdx.x & 31; b < grid; b += 32) s += partial[(int64_t)b * (kMaxCols + 1)].x;
+    return warp_sum(s);
 }
 
 __global__ void k_decide(const double2* coefA, int ncols, const double2* partial, int grid, int* flag,
                          double* scal) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double before = coefA[ncols].x;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     double after = sum_norm_partials(partial, grid);
+    if (threadIdx.x != 0) return;
+    double before = coefA[ncols].x;
     scal[1] = after;
     *flag = (after < 0.5 * before) ? 1 : 0;
 }
 
 __global__ void k_finalize(const double2* coefA, const double2* coefB, int ncols, const double2* partial2, int grid,
                            const int* flag, double* scal, double* alpha, double* beta, int j) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
     const bool second = *flag != 0;
+    double s2 = second ? sum_norm_partials(partial2, grid) : 0.0;   // warp-uniform branch
+    if (threadIdx.x != 0) return;
     double a = coefA[ncols - 1].x + (second ? coefB[ncols - 1].x : 0.0);
-    double wn2 = second ? sum_norm_partials(partial2, grid) : scal[1];
+    double wn2 = second ? s2 : scal[1];
     double b = sqrt(max(wn2, 0.0));
     alpha[j] = a;
     beta[j] = b;
@@ -300,7 +309,7 @@ void vec_proj(const VT* V, int64_t N, int ncols, const VT* w, double2* partial, 
     note_launches(1);
 }
 void vec_reduce(const double2* partial, int grid, int ncols1, double2* out, const int* active, cudaStream_t st) {
-    k_reduce<<<1, 256, 0, st>>>(partial, grid, ncols1, out, active);
+    k_reduce<<<(ncols1 + 7) / 8, 256, 0, st>>>(partial, grid, ncols1, out, active);
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }
