@@ -33,6 +33,9 @@ namespace {
 
 constexpr int kT = 256;
 constexpr int kRowsTile = 64;   // rows of W staged per tile in k_bproj
+// Accepted eigenvalue error estimate (relative, r^2/gap) of the mixed-precision batch: 10x
+// below the 1e-10 target.
+constexpr double kEigTarget = 1e-11;
 
 __device__ __forceinline__ double2 to2(double2 v) { return v; }
 __device__ __forceinline__ double2 to2(float2 v) { return make_double2(v.x, v.y); }
@@ -454,8 +457,11 @@ struct BlockLanczos {
 
     // Lockstep thick-restart Lanczos for all NB right-hand sides.  vectors: [nwant][N][NB] c128.
     // start: optional device block [N][NB] of start vectors (normalised here); else random from seed
+    // eig_target > 0 also accepts a pair whose Rayleigh-quotient error estimate res^2 / gap is
+    // below eig_target * max(1, |theta|) (gap: distance to the nearest other Ritz value outside
+    // its degenerate cluster), i.e. converges on eigenvalue accuracy rather than residual size.
     Out run(int nev, int nu, double tol, double rel_floor, int maxiter, uint64_t seed, int nwant, double2* vectors,
-            const VT* start = nullptr) {
+            const VT* start = nullptr, double eig_target = 0.0) {
         Out out;
         if (start) MOMED_CUDA_TRY(cudaMemcpyAsync(col(0), start, (size_t)N * NB * sizeof(VT), cudaMemcpyDeviceToDevice, st));
         else k_brandom<VT><<<ugrid, kT, 0, st>>>(col(0), N * NB, seed);
@@ -495,8 +501,17 @@ struct BlockLanczos {
                 double eff = std::max(tol, rel_floor * tmax);
                 res[r].assign(m, 0.0);
                 for (int i = 0; i < m; ++i) res[r][i] = std::fabs(bl * U[r][(size_t)(m - 1) * m + i]);
+                auto good = [&](int i) {
+                    if (res[r][i] <= eff) return true;
+                    if (eig_target <= 0.0) return false;
+                    const double ti = th[r][i], scale = std::max(1.0, std::fabs(ti));
+                    double gap = 1e300;
+                    for (int j = 0; j < m; ++j)
+                        if (j != i && std::fabs(th[r][j] - ti) > 1e-9 * scale) gap = std::min(gap, std::fabs(th[r][j] - ti));
+                    return res[r][i] * res[r][i] <= eig_target * scale * gap;
+                };
                 int c = 0;
-                while (c < nev && c < m && res[r][c] <= eff) ++c;
+                while (c < nev && c < m && good(c)) ++c;
                 nconv[r] = c;
                 double sc = tmax > 0 ? tmax : 1.0;
                 for (int j = k; j + 1 < m; ++j)
@@ -762,7 +777,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                         if (j != i && std::fabs(th[q][j] - th[q][i]) > 1e-9 * std::max(1.0, std::fabs(th[q][i])))
                             gap = std::min(gap, std::fabs(th[q][j] - th[q][i]));
                     double est = rs[q][i] * rs[q][i] / std::max(gap, 1e-300);
-                    good = rs[q][i] <= tol || est <= 1e-11 * std::max(1.0, std::fabs(th[q][i]));
+                    good = rs[q][i] <= tol || est <= kEigTarget * std::max(1.0, std::fabs(th[q][i]));
                 } else {
                     good = i < nconv1[q] || rs[q][i] <= std::max(tol, 1e-10 * std::max(1.0, std::fabs(th[q][i])));
                 }
@@ -787,7 +802,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
         MOMED_CUDA_TRY(cudaGetLastError());
         X3.resize((size_t)nev * stride);
         BlockLanczos<double2, NB> L3(h, m, uv);
-        auto r3 = L3.run(nev, nu, tol, 0.0, maxiter, o->seed, nev, X3.p, v0.p);
+        auto r3 = L3.run(nev, nu, tol, 0.0, maxiter, o->seed, nev, X3.p, v0.p, kEigTarget);
         matvecs += r3.steps * nu;
         matvecs64 += r3.steps * nu;
         restarts += r3.restarts;

@@ -396,6 +396,168 @@ k_block_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x,
     }
 }
 
+// Block map specialised for 32 right-hand sides.  Candidate terms are evaluated as in
+// k_block_matvec (one index lookup per hit), but hits are compacted into three lists by
+// amplitude kind (B only, A only, both), and each hit's 32 values are read by LPH lanes with
+// RPL right-hand sides per lane (RPL = 4 for c64, 2 for c128, 16-byte loads), so one warp
+// iteration consumes HPI = 32 / LPH hits.  B-only hits accumulate into a separate sum that
+// is scaled by u once per row.
+template <typename R> struct Blk32;
+template <> struct Blk32<float> { static constexpr int RPL = 4; };
+template <> struct Blk32<double> { static constexpr int RPL = 2; };
+
+template <typename R> struct HitLists {
+    uint32_t j[3][32];
+    typename Cx<R>::T c[3][32];
+    typename Cx<R>::T cb[32];
+};
+
+template <typename R>
+__device__ __forceinline__ void load_rpl(const typename Cx<R>::T* __restrict__ p, typename Cx<R>::T* v);
+template <>
+__device__ __forceinline__ void load_rpl<float>(const float2* __restrict__ p, float2* v) {
+    float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    v[0] = make_float2(a.x, a.y);
+    v[1] = make_float2(a.z, a.w);
+    v[2] = make_float2(b.x, b.y);
+    v[3] = make_float2(b.z, b.w);
+}
+template <>
+__device__ __forceinline__ void load_rpl<double>(const double2* __restrict__ p, double2* v) {
+    v[0] = __ldg(p);
+    v[1] = __ldg(p + 1);
+}
+
+template <typename R, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_block_matvec32(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+                 const R* __restrict__ u, int64_t rows) {
+    using C2 = typename Cx<R>::T;
+    constexpr int NB = 32;
+    constexpr int RPL = Blk32<R>::RPL;
+    constexpr int LPH = NB / RPL;      // lanes per hit
+    constexpr int HPI = 32 / LPH;      // hits per warp iteration
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    __shared__ HitLists<R> s_hits[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int hslot = lane / LPH, r0 = (lane % LPH) * RPL;
+    WarpScratch& ws = s_ws[wid];
+    HitLists<R>& hl = s_hits[wid];
+    R ur[RPL];
+#pragma unroll
+    for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? u[r0 + q] : R(0);
+    const C2* __restrict__ A = amp_a<R>(ov);
+    const C2* __restrict__ B = amp_b<R>(ov);
+    const unsigned lt = (1u << lane) - 1u;
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        C2 aa[RPL], ab[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) { aa[q].x = 0; aa[q].y = 0; ab[q].x = 0; ab[q].y = 0; }
+        R dax = 0, day = 0, dbx = 0, dby = 0;
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                int64_t j = -1;
+                int t = 0;
+                bool neg = false;
+                if (f < total) j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
+                C2 a, b;
+                a.x = 0; a.y = 0; b.x = 0; b.y = 0;
+                if (j >= 0) {
+                    a = load_amp(A, t);
+                    if (HAS_B) b = load_amp(B, t);
+                    if (neg) { a.x = -a.x; a.y = -a.y; b.x = -b.x; b.y = -b.y; }
+                }
+                if (j == row) {   // diagonal term (its sign is +): folded into a per-row sum
+                    dax += a.x; day += a.y; dbx += b.x; dby += b.y;
+                    j = -1;
+                }
+                const bool za = (a.x == R(0) && a.y == R(0)), zb = (b.x == R(0) && b.y == R(0));
+                const int kind = !HAS_B ? 1 : (za ? 0 : (zb ? 1 : 2));
+                const unsigned m0 = __ballot_sync(kFull, j >= 0 && kind == 0);
+                const unsigned m1 = __ballot_sync(kFull, j >= 0 && kind == 1);
+                const unsigned m2 = __ballot_sync(kFull, j >= 0 && kind == 2);
+                if (j >= 0) {
+                    const unsigned mk = kind == 0 ? m0 : (kind == 1 ? m1 : m2);
+                    const int k = __popc(mk & lt);
+                    hl.j[kind][k] = (uint32_t)j;
+                    hl.c[kind][k] = kind == 0 ? b : a;
+                    if (kind == 2) hl.cb[k] = b;
+                }
+                __syncwarp();
+                C2 xv[RPL];
+                const int n0 = __popc(m0), n1 = __popc(m1), n2 = __popc(m2);
+                for (int k = hslot; k < n0; k += HPI) {          // B only: accumulate, scale by u later
+                    const C2 c = hl.c[0][k];
+                    load_rpl<R>(x + (int64_t)hl.j[0][k] * NB + r0, xv);
+#pragma unroll
+                    for (int q = 0; q < RPL; ++q) {
+                        ab[q].x += c.x * xv[q].x - c.y * xv[q].y;
+                        ab[q].y += c.x * xv[q].y + c.y * xv[q].x;
+                    }
+                }
+                for (int k = hslot; k < n1; k += HPI) {          // A only
+                    const C2 c = hl.c[1][k];
+                    load_rpl<R>(x + (int64_t)hl.j[1][k] * NB + r0, xv);
+#pragma unroll
+                    for (int q = 0; q < RPL; ++q) {
+                        aa[q].x += c.x * xv[q].x - c.y * xv[q].y;
+                        aa[q].y += c.x * xv[q].y + c.y * xv[q].x;
+                    }
+                }
+                for (int k = hslot; k < n2; k += HPI) {          // both: A + u B per right-hand side
+                    const C2 c = hl.c[2][k], cb = hl.cb[k];
+                    load_rpl<R>(x + (int64_t)hl.j[2][k] * NB + r0, xv);
+#pragma unroll
+                    for (int q = 0; q < RPL; ++q) {
+                        R cx = c.x + ur[q] * cb.x, cy = c.y + ur[q] * cb.y;
+                        aa[q].x += cx * xv[q].x - cy * xv[q].y;
+                        aa[q].y += cx * xv[q].y + cy * xv[q].x;
+                    }
+                }
+                __syncwarp();
+            }
+        });
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dax += __shfl_xor_sync(kFull, dax, o);
+            day += __shfl_xor_sync(kFull, day, o);
+            if (HAS_B) {
+                dbx += __shfl_xor_sync(kFull, dbx, o);
+                dby += __shfl_xor_sync(kFull, dby, o);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            aa[q].x += ur[q] * ab[q].x;
+            aa[q].y += ur[q] * ab[q].y;
+#pragma unroll
+            for (int o = LPH; o < 32; o <<= 1) {
+                aa[q].x += __shfl_xor_sync(kFull, aa[q].x, o);
+                aa[q].y += __shfl_xor_sync(kFull, aa[q].y, o);
+            }
+        }
+        if (hslot == 0) {
+            C2 xd[RPL];
+            load_rpl<R>(x + row * NB + r0, xd);
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) {
+                R cx = dax + ur[q] * dbx, cy = day + ur[q] * dby;
+                C2 o;
+                o.x = aa[q].x + cx * xd[q].x - cy * xd[q].y;
+                o.y = aa[q].y + cx * xd[q].y + cy * xd[q].x;
+                y[row * NB + r0 + q] = o;
+            }
+        }
+    }
+}
+
 template <typename K>
 int persistent_grid(K kernel, int64_t rows) {
     static int sms = 0;
@@ -471,7 +633,15 @@ static void block_dispatch(const IndexView& iv, const OpView& ov, const typename
         MOMED_BLK(4)
         MOMED_BLK(8)
         MOMED_BLK(16)
-        MOMED_BLK(32)
+        case 32:
+            if (hb) {
+                auto k = k_block_matvec32<R, true>;
+                k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);
+            } else {
+                auto k = k_block_matvec32<R, false>;
+                k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);
+            }
+            break;
         default:
             throw Error{MOMED_EINVAL, "block width must be a power of two <= 32"};
     }
