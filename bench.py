@@ -13,6 +13,13 @@ same steps through the public API with host buffers (basis + operator in, eigenv
 eigenvectors out).  The plain comparison solves U0 values of one sector one at a time with the
 FP64 single-vector Lanczos.
 
+Serving (rank 0, N = 1): a Poisson stream of solve requests at 50 req/s (seed 4; mesh uniform
+over --serve-meshes, uniform sector, U0 ~ U(0.5, 2), nev 1..20, tol 1e-10) through the
+continuous-batching server, and the same requests solved one at a time by the plain FP64 GPU
+Lanczos, both live against the arrival clock; latency is arrival -> eigenvalues on the host.
+The 4x9 Ne=12 mesh (~35M states per sector) is left out of the default stream because one of
+its solves alone takes tens of seconds; --serve-meshes 3x5,3x9,3x10,4x9 includes it.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun (N > 1) every rank runs its own sectors (replicas, no data-path collective).
 """
@@ -37,6 +44,10 @@ SEED = 2
 NEV = 4
 NU = 32
 KRYLOV = 30
+# DRAM bytes (read + write) of one c64 x32 block-map launch on this workload, from an ncu capture
+# of `bench.py --profile-only` (dram__bytes_read.sum + dram__bytes_write.sum = 46.5 + 28.8 MB): the
+# x block and the term tables stay in L2, so the per-hit gathers of the algorithmic count hit L2.
+MV_DRAM_BYTES = 75.3e6
 
 
 def parse():
@@ -48,6 +59,11 @@ def parse():
     ap.add_argument("--plain", type=int, default=4, help="U0 values solved one at a time for the plain comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     ap.add_argument("--profile-only", action="store_true", help="one short run for ncu (no timing output)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving stream")
+    ap.add_argument("--serve-requests", type=int, default=60)
+    ap.add_argument("--serve-meshes", default="3x5,3x9,3x10", help="subset of 3x5,3x9,3x10,4x9")
+    ap.add_argument("--serve-slots", type=int, default=8)
+    ap.add_argument("--serve-hbm-gb", type=float, default=100.0)
     return ap.parse_args()
 
 
@@ -220,6 +236,109 @@ def _has_gpu():
         return False
 
 
+# ----------------------------------------------------------------------------- serving
+def serve_krylovdim(nev: int) -> int:
+    return max(KRYLOV, 2 * nev + 12)
+
+
+def serve_bench(args, device: int):
+    """Serving form: the Poisson request stream through momed_serve_* (mixed precision,
+    `args.serve_slots` slots) and the same requests solved one at a time by the plain FP64 GPU
+    Lanczos, both live against the arrival clock; then the same requests as one burst at t=0
+    (capacity).  Latency is arrival -> eigenvalues on the host."""
+    import momed
+    from momed import _lib
+    from momed.core import pair_operator
+    from momed.synthetic import SERVE_MESHES, mesh_para, serve_requests
+
+    meshes = [m for m in args.serve_meshes.split(",") if m]
+    h = momed.Handle(device)
+    sectors, ops = {}, {}
+    for m in meshes:
+        ne, seed = SERVE_MESHES[m]
+        a, b = (int(x) for x in m.split("x"))
+        para, _ = mesh_para(a, b, seed)
+        sectors[m] = [s[1] for s in h.enumerate_basis(para.k_list, para.Gk, 1, 1, (ne,))]
+        A = momed.MBOperator(momed.ED_scatterlist_onebody(para), upper_hermitian=True)
+        B = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=True)
+        ops[m] = pair_operator(A, B)
+    reqs = serve_requests(args.serve_requests, meshes, {m: len(sectors[m]) for m in meshes})
+
+    def pct(x, q):
+        return float(np.percentile(np.asarray(x), q)) if len(x) else None
+
+    # plain: one request at a time, FP64 single-vector Lanczos, live against arrivals
+    plain_vals, plain_lat, plain_service = [], [], []
+    cur = None
+    t0 = time.perf_counter()
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if now < r["arrival"]:
+            time.sleep(r["arrival"] - now)
+        s0 = time.perf_counter()
+        if cur != r["mesh"]:
+            h.set_scatter_pair(*ops[r["mesh"]])
+            cur = r["mesh"]
+        h.set_basis(sectors[r["mesh"]][r["sector"]])
+        h.set_param(r["u"])
+        v, _, _, _ = h.eigsolve(r["nev"], krylovdim=serve_krylovdim(r["nev"]), tol=r["tol"], maxiter=300,
+                                want_vectors=False, precision=_lib.PREC_FP64)
+        s1 = time.perf_counter()
+        plain_vals.append(v)
+        plain_service.append(s1 - s0)
+        plain_lat.append(s1 - t0 - r["arrival"])
+    plain_span = time.perf_counter() - t0
+    h.close()
+
+    def run_server(burst: bool):
+        srv = momed.Server(device, slots=args.serve_slots, hbm_budget=int(args.serve_hbm_gb * (1 << 30)))
+        op_id = {m: srv.register_operator(*ops[m]) for m in meshes}
+        ids = []
+        t0 = time.perf_counter()
+        for r in reqs:
+            if not burst:
+                now = time.perf_counter() - t0
+                if now < r["arrival"]:
+                    time.sleep(r["arrival"] - now)
+            ids.append(srv.submit(op_id[r["mesh"]], sectors[r["mesh"]][r["sector"]], r["u"], r["nev"], tol=r["tol"],
+                                  krylovdim=serve_krylovdim(r["nev"]), maxiter=300, precision=_lib.PREC_MIXED))
+        vals, lat, conv = [], [], []
+        for rid, r in zip(ids, reqs):
+            while True:
+                st, v, res, info, q, l = srv.poll(rid, r["nev"], wait_ms=1000)
+                if st >= 2:
+                    break
+            vals.append(v)
+            lat.append(l)
+            conv.append(info["converged"] >= r["nev"])
+        span = time.perf_counter() - t0
+        srv.stop()
+        return vals, lat, conv, span
+
+    s_vals, s_lat, s_conv, s_span = run_server(burst=False)
+    b_vals, b_lat, b_conv, b_span = run_server(burst=True)
+    errs = [float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0))) for a, b in zip(s_vals, plain_vals)]
+    errs_b = [float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0))) for a, b in zip(b_vals, plain_vals)]
+    n = len(reqs)
+    sizes = {m: [len(x) for x in sectors[m]] for m in meshes}
+    return {
+        "stream": f"{n} requests, Poisson 50 req/s (seed 4), meshes {meshes}, uniform sector, U0~U(0.5,2), "
+                  f"nev 1..20, tol 1e-10",
+        "meshes_states_per_sector": {m: [min(v), max(v)] for m, v in sizes.items()},
+        "served": {"solves_per_s": n / s_span, "latency_ms_p50": 1e3 * pct(s_lat, 50),
+                   "latency_ms_p99": 1e3 * pct(s_lat, 99), "slots": args.serve_slots,
+                   "precision": "mixed (c64 map, f64 recurrences + f64 Rayleigh-Ritz)",
+                   "all_converged": bool(all(s_conv)), "max_rel_eig_err_vs_plain_fp64": max(errs)},
+        "plain_one_at_a_time": {"solves_per_s": n / plain_span, "latency_ms_p50": 1e3 * pct(plain_lat, 50),
+                                "latency_ms_p99": 1e3 * pct(plain_lat, 99),
+                                "service_ms_p50": 1e3 * pct(plain_service, 50), "precision": "fp64"},
+        "burst_capacity": {"served_solves_per_s": n / b_span, "plain_solves_per_s": n / sum(plain_service),
+                           "speedup": (n / b_span) / (n / sum(plain_service)),
+                           "latency_ms_p50": 1e3 * pct(b_lat, 50), "latency_ms_p99": 1e3 * pct(b_lat, 99),
+                           "all_converged": bool(all(b_conv)), "max_rel_eig_err_vs_plain_fp64": max(errs_b)},
+    }
+
+
 # ----------------------------------------------------------------------------- our arm
 def block_bytes(N: int, nnz: int, nscat: int, nb: int, s: int) -> float:
     """Algorithmic bytes of one block matvec launch: basis keys, x stream read and y write for nb
@@ -301,8 +420,28 @@ def main():
     value = solves_total / elapsed_max
 
     # ---------------------------------------------------------------- e2e: public API, host buffers
-    host_inputs = [(sectors[order[W + i]][1].copy()) for i in range(K)]
-    h2d = [b.nbytes + amp_a.nbytes + amp_b.nbytes + in_.nbytes + out.nbytes + pm.nbytes for b in host_inputs]
+    def pinned(shape, dtype):
+        t = torch.empty(int(np.prod(shape)) * np.dtype(dtype).itemsize, dtype=torch.uint8, pin_memory=True)
+        return t, t.numpy().view(dtype).reshape(shape)
+
+    keep_alive = []
+    host_inputs = []
+    for i in range(K):                                   # this step's inputs in pinned host memory
+        src = sectors[order[W + i]][1]
+        t, b = pinned(src.shape, np.uint64)
+        b[:] = src
+        keep_alive.append(t)
+        host_inputs.append(b)
+    pair_host = []
+    for a in (amp_a, amp_b, in_, out, pm):
+        t, b = pinned(a.shape, a.dtype)
+        b[:] = a
+        keep_alive.append(t)
+        pair_host.append(b)
+    nmax = max(len(b) for b in host_inputs)
+    t, vec_host = pinned((NU * NEV * nmax,), np.complex128)
+    keep_alive.append(t)
+    h2d = [b.nbytes + sum(a.nbytes for a in pair_host) for b in host_inputs]
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -311,9 +450,11 @@ def main():
     d2h = []
     for i in range(K):
         h.set_basis(host_inputs[i])
-        h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+        h.set_scatter_pair(*pair_host)
+        nb = len(host_inputs[i])
         vals, vecs, res, info = h.batch_solve(u, NEV, krylovdim=KRYLOV, tol=1e-12, precision=_lib.PREC_MIXED,
-                                              want_vectors=True)
+                                              want_vectors=True,
+                                              out_vecs=vec_host[:NU * NEV * nb].reshape(NU, NEV, nb))
         d2h.append(vals.nbytes + res.nbytes + vecs.nbytes)
     e2e_ev[1].record(stream)
     torch.cuda.synchronize()
@@ -326,6 +467,8 @@ def main():
         sidx, bvals, _ = all_vals[0]
         h.select_sector(sidx, len(sectors[sidx][1]))
         h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+        h.set_param(float(u[0]))                          # untimed: index and operator checks
+        h.eigsolve(NEV, krylovdim=KRYLOV, tol=1e-12, seed=1, want_vectors=False, precision=_lib.PREC_FP64)
         pe = [torch.cuda.Event(enable_timing=True) for _ in range(args.plain + 1)]
         torch.cuda.synchronize()
         pe[0].record(stream)
@@ -352,6 +495,10 @@ def main():
         cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": nthreads, "kind": "port",
                "sample": f"1 full FP64 solve (reference CPU map + Lanczos) of one (sector, U0) pair, "
                          f"{len(basis)} states, U0={u[0]:.3f}"}
+
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serve and args.serve_requests > 0:
+        serving = serve_bench(args, local)
 
     if rank == 0:
         avg_ms = ms_mv / max(n_mv, 1)
@@ -381,16 +528,18 @@ def main():
             "plain_gpu_lanczos": plain,
             "speedup_vs_plain": (value / world) / plain["solves_per_s"] if plain else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
-                         "kernel": "block matvec c64 x32 (k_block_matvec<float,32>)",
+                         "frac": achieved / peak, "traffic": MV_DRAM_BYTES, "peak_source": peak_src,
+                         "kernel": "block matvec c64 x32 (k_block_matvec32<float>)",
                          "launches": n_mv, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "cpu_baseline": cpu,
+            "serving": serving,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(np.mean(h2d)),
                     "d2h_bytes_per_step": int(np.mean(d2h))},
             "gpu_launches": int(all_sum(launches, world)),
             "clocks": clk.summary(),
             "solver": {"matvecs_per_step": int(np.mean([i["matvecs"] for i in infos])),
+                       "fp64_matvecs_per_step": int(np.mean([i["matvecs_fp64"] for i in infos])),
                        "restarts_per_step": float(np.mean([i["restarts"] for i in infos])),
                        "converged_min": int(min(i["converged"] for i in infos)),
                        "max_residual": float(max(float(np.max(r)) for _, _, r in all_vals))},

@@ -36,6 +36,8 @@ constexpr int kRowsTile = 64;   // rows of W staged per tile in k_bproj
 // Accepted eigenvalue error estimate (relative, r^2/gap) of the mixed-precision batch: 10x
 // below the 1e-10 target.
 constexpr double kEigTarget = 1e-11;
+// Anchored refinement cycles of the mixed-precision batch before the FP64 block Lanczos takes over.
+constexpr int kRefineCycles = 6;
 
 __device__ __forceinline__ double2 to2(double2 v) { return v; }
 __device__ __forceinline__ double2 to2(float2 v) { return make_double2(v.x, v.y); }
@@ -43,46 +45,83 @@ template <typename VT> __device__ __forceinline__ VT fr2(double2 v);
 template <> __device__ __forceinline__ double2 fr2<double2>(double2 v) { return v; }
 template <> __device__ __forceinline__ float2 fr2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
 
-// partial[b][i][r] (i <= ncols: column ncols holds |w_r|^2)
-template <typename VT, int NB>
+// 16-byte packets of a block vector: two c64 values (adjacent right-hand sides of one row) when
+// NB is even, else one value.
+template <typename VT, int NB> struct Pack {
+    static constexpr int E = 1;
+    using T = VT;
+    static __device__ __forceinline__ void get(const T& p, double2* v) { v[0] = to2(p); }
+    static __device__ __forceinline__ T put(const double2* v) { return fr2<VT>(v[0]); }
+};
+template <int NB> struct PackF2 {
+    static constexpr int E = 2;
+    using T = float4;
+    static __device__ __forceinline__ void get(const float4& p, double2* v) {
+        v[0] = make_double2(p.x, p.y);
+        v[1] = make_double2(p.z, p.w);
+    }
+    static __device__ __forceinline__ float4 put(const double2* v) {
+        return make_float4((float)v[0].x, (float)v[0].y, (float)v[1].x, (float)v[1].y);
+    }
+};
+template <> struct Pack<float2, 2> : PackF2<2> {};
+template <> struct Pack<float2, 4> : PackF2<4> {};
+template <> struct Pack<float2, 8> : PackF2<8> {};
+template <> struct Pack<float2, 16> : PackF2<16> {};
+template <> struct Pack<float2, 32> : PackF2<32> {};
+
+// partial[b][i][r] (i <= ncols: column ncols holds |w_r|^2).  Grid: x = row blocks, y = groups
+// of 8 columns; warp w of group g owns column 8g + w over the block's rows, reading 16-byte
+// packets (lanes: NB / E packets per row, 32 E / NB rows at a time), so every lane keeps E
+// accumulators and the unrolled row loop keeps 8 loads of V in flight.  Warp 0 of group 0 also
+// sums |w|^2.
+template <typename VT, typename WT, int NB>
 __global__ void __launch_bounds__(kT)
-k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ W, double2* partial,
+k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W, double2* partial,
         const int* active_any) {
     if (active_any && *active_any == 0) return;
-    constexpr int RS = 32 / NB;                 // row subsets per warp
+    using P = Pack<VT, NB>;
+    constexpr int E = P::E;
+    constexpr int PR = NB / E;                  // packets per row
+    constexpr int RS = 32 / PR;                 // rows per warp pass
     __shared__ double2 ws[kRowsTile * NB];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int r = lane % NB, rs = lane / NB;
-    double2 acc[kColsPerWarp];
+    const int rp = lane % PR, rs = lane / PR;
+    const int i = blockIdx.y * 8 + wid;
+    const bool norm = blockIdx.y == 0 && wid == 0;
+    double ax[E], ay[E], wn2[E];
 #pragma unroll
-    for (int k = 0; k < kColsPerWarp; ++k) acc[k] = make_double2(0.0, 0.0);
-    double wn2 = 0.0;
+    for (int q = 0; q < E; ++q) { ax[q] = 0.0; ay[q] = 0.0; wn2[q] = 0.0; }
     int64_t per = (N + gridDim.x - 1) / gridDim.x;
     int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(N, r0 + per);
+    const typename P::T* colbase = reinterpret_cast<const typename P::T*>(V + (int64_t)(i < ncols ? i : 0) * N * NB);
     for (int64_t t0 = r0; t0 < r1; t0 += kRowsTile) {
         const int rows = (int)((r1 - t0) < kRowsTile ? (r1 - t0) : kRowsTile);
         for (int e = threadIdx.x; e < kRowsTile * NB; e += kT) {
             int t = e / NB;
-            double2 v = (t < rows) ? to2(W[(t0 + t) * NB + (e % NB)]) : make_double2(0.0, 0.0);
-            ws[e] = v;
+            ws[e] = (t < rows) ? to2(W[(t0 + t) * NB + (e % NB)]) : make_double2(0.0, 0.0);
         }
         __syncthreads();
-        if (wid == 0) {
+        if (norm) {
             for (int t = rs; t < rows; t += RS) {
-                double2 v = ws[t * NB + r];
-                wn2 += v.x * v.x + v.y * v.y;
+#pragma unroll
+                for (int q = 0; q < E; ++q) {
+                    double2 v = ws[t * NB + rp * E + q];
+                    wn2[q] += v.x * v.x + v.y * v.y;
+                }
             }
         }
+        if (i < ncols) {
+            const typename P::T* col = colbase + t0 * PR;
+#pragma unroll 8
+            for (int t = rs; t < rows; t += RS) {
+                double2 v[E];
+                P::get(col[t * PR + rp], v);
 #pragma unroll
-        for (int k = 0; k < kColsPerWarp; ++k) {
-            int i = wid + 8 * k;
-            if (i < ncols) {
-                const VT* col = V + (int64_t)i * N * NB + t0 * NB;
-                for (int t = rs; t < rows; t += RS) {
-                    double2 v = to2(col[t * NB + r]);
-                    double2 w = ws[t * NB + r];
-                    acc[k].x += v.x * w.x + v.y * w.y;
-                    acc[k].y += v.x * w.y - v.y * w.x;
+                for (int q = 0; q < E; ++q) {
+                    double2 w = ws[t * NB + rp * E + q];
+                    ax[q] += v[q].x * w.x + v[q].y * w.y;
+                    ay[q] += v[q].x * w.y - v[q].y * w.x;
                 }
             }
         }
@@ -90,22 +129,21 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ W
     }
     double2* out = partial + (int64_t)blockIdx.x * (kMaxCols + 1) * NB;
 #pragma unroll
-    for (int k = 0; k < kColsPerWarp; ++k) {
-        int i = wid + 8 * k;
-        double sx = acc[k].x, sy = acc[k].y;
+    for (int q = 0; q < E; ++q) {
 #pragma unroll
-        for (int o = NB; o < 32; o <<= 1) {
-            sx += __shfl_xor_sync(0xffffffffu, sx, o);
-            sy += __shfl_xor_sync(0xffffffffu, sy, o);
+        for (int o = PR; o < 32; o <<= 1) {
+            ax[q] += __shfl_xor_sync(0xffffffffu, ax[q], o);
+            ay[q] += __shfl_xor_sync(0xffffffffu, ay[q], o);
+            wn2[q] += __shfl_xor_sync(0xffffffffu, wn2[q], o);
         }
-        if (i < ncols && rs == 0) out[i * NB + r] = make_double2(sx, sy);
-    }
-    if (wid == 0) {
-#pragma unroll
-        for (int o = NB; o < 32; o <<= 1) wn2 += __shfl_xor_sync(0xffffffffu, wn2, o);
-        if (rs == 0) out[ncols * NB + r] = make_double2(wn2, 0.0);
+        if (rs == 0) {
+            if (i < ncols) out[i * NB + rp * E + q] = make_double2(ax[q], ay[q]);
+            if (norm) out[ncols * NB + rp * E + q] = make_double2(wn2[q], 0.0);
+        }
     }
 }
+
+inline dim3 bproj_grid(int rowblocks, int ncols) { return dim3(rowblocks, (unsigned)std::max(1, (ncols + 7) / 8)); }
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
@@ -133,38 +171,62 @@ __global__ void k_breduce(const double2* partial, int grid, int ncols1, double2*
 
 inline int breduce_grid(int ncols1, int nb) { return (ncols1 * nb + 7) / 8; }
 
-// W[n][r] -= sum_i coef[i][r] V_i[n][r] for active r; per-block |W_r|^2 partials
+// W[n][r] -= sum_i coef[i][r] V_i[n][r] for active r; per-block |W_r|^2 partials.  A thread
+// owns one 16-byte packet (E right-hand sides of a row) per grid-stride step; the unrolled
+// column loop keeps 8 packet loads in flight.
 template <typename VT, int NB>
 __global__ void __launch_bounds__(kT)
 k_bupdate(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restrict__ coef, VT* __restrict__ W,
           double* npartial /* [grid][NB] */, const int* active /* [NB] or null */, const int* active_any) {
     if (active_any && *active_any == 0) return;
+    using P = Pack<VT, NB>;
+    using PT = typename P::T;
+    constexpr int E = P::E;
     extern __shared__ double2 c[];   // [ncols * NB]
     __shared__ double nrm[32];
     for (int e = threadIdx.x; e < ncols * NB; e += kT) c[e] = coef[e];
     if (threadIdx.x < 32) nrm[threadIdx.x] = 0.0;
     __syncthreads();
-    const int r = threadIdx.x % NB;
-    const bool on = !active || active[r];
-    double wn2 = 0.0;
-    const int64_t total = N * NB;
+    const int r0 = (threadIdx.x * E) % NB;     // fixed: the grid stride is a multiple of NB / E packets
+    bool on[E];
+    bool anyon = false;
+#pragma unroll
+    for (int q = 0; q < E; ++q) { on[q] = !active || active[r0 + q]; anyon = anyon || on[q]; }
+    double wn2[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) wn2[q] = 0.0;
+    const int64_t total = N * NB / E;           // packets per column
+    const PT* Vp = reinterpret_cast<const PT*>(V);
+    PT* Wp = reinterpret_cast<PT*>(W);
     for (int64_t e = (int64_t)blockIdx.x * kT + threadIdx.x; e < total; e += (int64_t)gridDim.x * kT) {
-        double2 acc = to2(W[e]);
-        if (on) {
-            const int64_t n = e / NB;
+        double2 acc[E], orig[E];
+        P::get(Wp[e], orig);
+#pragma unroll
+        for (int q = 0; q < E; ++q) acc[q] = orig[q];
+        if (anyon) {
+#pragma unroll 8
             for (int i = 0; i < ncols; ++i) {
-                double2 cf = c[i * NB + r];
-                double2 v = to2(V[(int64_t)i * N * NB + n * NB + r]);
-                acc.x -= cf.x * v.x - cf.y * v.y;
-                acc.y -= cf.x * v.y + cf.y * v.x;
+                double2 v[E];
+                P::get(Vp[(int64_t)i * total + e], v);
+#pragma unroll
+                for (int q = 0; q < E; ++q) {
+                    const double2 cf = c[i * NB + r0 + q];
+                    acc[q].x -= cf.x * v[q].x - cf.y * v[q].y;
+                    acc[q].y -= cf.x * v[q].y + cf.y * v[q].x;
+                }
             }
-            VT st = fr2<VT>(acc);
-            W[e] = st;
-            acc = to2(st);
+#pragma unroll
+            for (int q = 0; q < E; ++q)
+                if (!on[q]) acc[q] = orig[q];
+            const PT st = P::put(acc);
+            Wp[e] = st;
+            P::get(st, acc);
         }
-        wn2 += acc.x * acc.x + acc.y * acc.y;
+#pragma unroll
+        for (int q = 0; q < E; ++q) wn2[q] += acc[q].x * acc[q].x + acc[q].y * acc[q].y;
     }
-    atomicAdd(&nrm[r], wn2);
+#pragma unroll
+    for (int q = 0; q < E; ++q) atomicAdd(&nrm[r0 + q], wn2[q]);
     __syncthreads();
     if (threadIdx.x < NB) npartial[(int64_t)blockIdx.x * NB + threadIdx.x] = nrm[threadIdx.x];
 }
@@ -237,71 +299,62 @@ __global__ void k_brandom(VT* v, int64_t total, uint64_t seed) {
     }
 }
 
-// out[i][n][r] = sum_a U[i][a][r] V[a][n][r]  (U: [nout][m][NB], r fastest so a warp's coefficient
-// loads are coalesced), optionally out[nout] = V[copy_col].  A tile of TR rows x (m+1) columns is
-// staged in shared memory; each thread owns RPT rows of one right-hand side and accumulates OC
-// outputs at a time in registers.  In place (out == V) is safe: a tile is read whole before any
-// of its rows is written.
-template <typename VIN, typename VOUT, int NB, int RPT>
+// out[i][n][r] = sum_a U[i][a][r] V[a][n][r]  (U: [nout][m][NB] real, r fastest so a warp's
+// coefficient loads are coalesced), optionally out[nout] = V[copy_col].  Each thread owns RPT rows
+// of one right-hand side and accumulates OC outputs at a time in registers of type ACC, streaming
+// V straight from HBM (the unrolled a-loop keeps several loads in flight).  out must not overlap V.
+template <typename VIN, typename VOUT, typename ACC, int NB, int RPT, int OC>
 __global__ void __launch_bounds__(kT)
-k_bcombine(const VIN* V, int64_t N, int m, const double* __restrict__ U, int nout, VOUT* out, int copy_col) {
-    constexpr int TPR = kT / NB;        // row slots per pass
-    constexpr int TR = TPR * RPT;       // rows per tile
-    constexpr int OC = 8;               // outputs per register chunk
-    extern __shared__ unsigned char smem_raw[];
-    VIN* tile = reinterpret_cast<VIN*>(smem_raw);   // [(m + 1)][TR][NB]
-    const int ncopy = copy_col >= 0 ? 1 : 0;
-    const int r = threadIdx.x % NB, tl = threadIdx.x / NB;
-    for (int64_t t0 = (int64_t)blockIdx.x * TR; t0 < N; t0 += (int64_t)gridDim.x * TR) {
-        const int rows = (int)((N - t0) < TR ? (N - t0) : TR);
-        for (int e = threadIdx.x; e < (m + ncopy) * TR * NB; e += kT) {
-            int a = e / (TR * NB), rem = e % (TR * NB);
-            int t = rem / NB;
-            int col = a < m ? a : copy_col;
-            VIN z;
-            z.x = 0;
-            z.y = 0;
-            tile[e] = (t < rows) ? V[(int64_t)col * N * NB + (t0 + t) * NB + (rem % NB)] : z;
+k_bcombine(const VIN* __restrict__ V, int64_t N, int m, const double* __restrict__ U, int nout,
+           VOUT* __restrict__ out, int copy_col) {
+    constexpr int TPR = kT / NB;        // row slots per block pass
+    const int r = threadIdx.x % NB, slot = threadIdx.x / NB;
+    const int64_t stride = N * NB;
+    for (int64_t t0 = (int64_t)blockIdx.x * TPR * RPT; t0 < N; t0 += (int64_t)gridDim.x * TPR * RPT) {
+        int64_t off[RPT];
+        bool ok[RPT];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            const int64_t row = t0 + slot + (int64_t)j * TPR;
+            ok[j] = row < N;
+            off[j] = (ok[j] ? row : 0) * NB + r;
         }
-        __syncthreads();
         for (int c0 = 0; c0 < nout; c0 += OC) {
-            double ax[RPT][OC], ay[RPT][OC];
+            ACC ax[RPT][OC], ay[RPT][OC];
 #pragma unroll
             for (int j = 0; j < RPT; ++j)
 #pragma unroll
-                for (int k = 0; k < OC; ++k) { ax[j][k] = 0.0; ay[j][k] = 0.0; }
+                for (int k = 0; k < OC; ++k) { ax[j][k] = 0; ay[j][k] = 0; }
+#pragma unroll 2
             for (int a = 0; a < m; ++a) {
-                double u[OC];
+                ACC u[OC];
 #pragma unroll
                 for (int k = 0; k < OC; ++k)
-                    u[k] = (c0 + k < nout) ? __ldg(U + ((int64_t)(c0 + k) * m + a) * NB + r) : 0.0;
+                    u[k] = (c0 + k < nout) ? (ACC)__ldg(U + ((int64_t)(c0 + k) * m + a) * NB + r) : (ACC)0;
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
-                    double2 v = to2(tile[(a * TR + tl + j * TPR) * NB + r]);
+                    const VIN v = V[(int64_t)a * stride + off[j]];
 #pragma unroll
                     for (int k = 0; k < OC; ++k) {
-                        ax[j][k] += u[k] * v.x;
-                        ay[j][k] += u[k] * v.y;
+                        ax[j][k] += u[k] * (ACC)v.x;
+                        ay[j][k] += u[k] * (ACC)v.y;
                     }
                 }
             }
 #pragma unroll
             for (int j = 0; j < RPT; ++j) {
-                const int t = tl + j * TPR;
-                if (t < rows) {
+                if (!ok[j]) continue;
 #pragma unroll
-                    for (int k = 0; k < OC; ++k)
-                        if (c0 + k < nout)
-                            out[(int64_t)(c0 + k) * N * NB + (t0 + t) * NB + r] =
-                                fr2<VOUT>(make_double2(ax[j][k], ay[j][k]));
-                }
+                for (int k = 0; k < OC; ++k)
+                    if (c0 + k < nout)
+                        out[(int64_t)(c0 + k) * stride + off[j]] = fr2<VOUT>(make_double2((double)ax[j][k], (double)ay[j][k]));
             }
         }
-        if (ncopy) {
-            for (int e = threadIdx.x; e < rows * NB; e += kT)
-                out[(int64_t)nout * N * NB + t0 * NB + e] = fr2<VOUT>(to2(tile[(m * TR) * NB + e]));
+        if (copy_col >= 0) {
+#pragma unroll
+            for (int j = 0; j < RPT; ++j)
+                if (ok[j]) out[(int64_t)nout * stride + off[j]] = fr2<VOUT>(to2(V[(int64_t)copy_col * stride + off[j]]));
         }
-        __syncthreads();
     }
 }
 
@@ -358,7 +411,7 @@ struct BlockLanczos {
     int m;
     cudaStream_t st;
     int grid, ugrid;
-    DevBuf<VT> V;
+    DevBuf<VT> V, V2;
     DevBuf<double2> partial, coefA, coefB;
     DevBuf<double> npart, after, scal, alpha, beta, Ud;
     DevBuf<int> flag, any;
@@ -389,16 +442,28 @@ struct BlockLanczos {
     VT* col(int i) { return V.p + (size_t)i * N * NB; }
 
     void proj(int ncols, const VT* w, double2* out, const int* act) {
-        k_bproj<VT, NB><<<grid, kT, 0, st>>>(V.p, N, ncols, w, partial.p, act);
+        k_bproj<VT, VT, NB><<<bproj_grid(grid, ncols), kT, 0, st>>>(V.p, N, ncols, w, partial.p, act);
         k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(partial.p, grid, ncols + 1, out, act);
         launches += 2;
     }
     void update(int ncols, const double2* coef, VT* w, const int* active, const int* act) {
         size_t smem = (size_t)ncols * NB * sizeof(double2);
         auto k = k_bupdate<VT, NB>;
-        if (smem > 48 * 1024) MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        // process-wide kernel attribute: always the largest size, so concurrent callers never lower it
+        constexpr size_t smem_max = (size_t)kMaxCols * NB * sizeof(double2);
+        if (smem_max > 48 * 1024)
+            MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
         k<<<ugrid, kT, smem, st>>>(V.p, N, ncols, coef, w, npart.p, active, act);
         ++launches;
+    }
+    // column k0 made orthogonal to columns [0, k0) (two classical Gram-Schmidt passes), then normalised
+    void orth_start(int k0) {
+        VT* v = col(k0);
+        for (int pass = 0; pass < 2 && k0 > 0; ++pass) {
+            proj(k0, v, coefA.p, nullptr);
+            update(k0, coefA.p, v, nullptr, nullptr);
+        }
+        normalize(v);
     }
     void normalize(VT* v) {
         proj(0, v, coefA.p, nullptr);
@@ -423,28 +488,24 @@ struct BlockLanczos {
     template <typename VOUT>
     void combine(const std::vector<double>& Uh, int nout, VOUT* out, int copy_col, int mm) {
         MOMED_CUDA_TRY(cudaMemcpyAsync(Ud.p, Uh.data(), Uh.size() * 8, cudaMemcpyHostToDevice, st));
-        constexpr int TPR = kT / NB;
-        const size_t per_row = (size_t)(mm + 1) * NB * sizeof(VT);
-        const size_t limit = 200 * 1024;
-        if (per_row * TPR * 2 <= limit) {
-            constexpr int TR = TPR * 2;
-            size_t smem = per_row * TR;
-            auto k = k_bcombine<VT, VOUT, NB, 2>;
-            MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms()));
-            k<<<g, kT, smem, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
-        } else {
-            constexpr int TR = TPR;
-            size_t smem = per_row * TR;
-            MOMED_REQUIRE(smem <= 227 * 1024, MOMED_EINVAL, "krylovdim too large for the batched restart tile");
-            auto k = k_bcombine<VT, VOUT, NB, 1>;
-            MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms()));
-            k<<<g, kT, smem, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
-        }
+        // FP32 accumulation when FP32 vectors are recombined into FP32 vectors; FP64 otherwise
+        constexpr bool f32 = std::is_same<VT, float2>::value && std::is_same<VOUT, float2>::value;
+        using ACC = typename std::conditional<f32, float, double>::type;
+        constexpr int RPT = f32 ? 4 : 2;
+        constexpr int TR = (kT / NB) * RPT;
+        auto k = k_bcombine<VT, VOUT, ACC, NB, RPT, 8>;
+        int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms() * 8));
+        k<<<g, kT, 0, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
         MOMED_CUDA_TRY(cudaGetLastError());
         MOMED_CUDA_TRY(cudaStreamSynchronize(st));
         ++launches;
+    }
+    // restart: the kept combinations (and column m) go to V2, which then becomes the basis
+    void recombine(const std::vector<double>& Uh, int keep) {
+        V2.resize((size_t)(m + 1) * N * NB);
+        combine<VT>(Uh, keep, V2.p, m, m);
+        std::swap(V.p, V2.p);
+        std::swap(V.n, V2.n);
     }
 
     struct Out {
@@ -555,7 +616,7 @@ struct BlockLanczos {
                 double bl = hb[(size_t)r * m + m - 1];
                 for (int i = 0; i < keep; ++i) arrow[r][i] = bl * U[r][(size_t)(m - 1) * m + i];
             }
-            combine<VT>(Uh, keep, V.p, m, m);
+            recombine(Uh, keep);
             k = keep;
             ++restarts;
         }
@@ -618,6 +679,67 @@ __global__ void k_bresid(const double2* __restrict__ W, const double2* __restric
         __syncthreads();
         if (threadIdx.x < NB) part[((int64_t)blockIdx.x * k + i) * NB + threadIdx.x] = acc[threadIdx.x];
         __syncthreads();
+    }
+}
+
+// out[n][r] = sum_{i<k} wt[r][i] (W[i][n][r] - th[r][i] X[i][n][r])  (start of the refinement)
+template <typename VT, int NB>
+__global__ void k_bresid_sum(const double2* __restrict__ W, const double2* __restrict__ X, int64_t N, int k,
+                             const double* __restrict__ th, const double* __restrict__ wt, VT* __restrict__ out) {
+    const int64_t total = N * NB;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e % NB);
+        double sx = 0.0, sy = 0.0;
+        for (int i = 0; i < k; ++i) {
+            const double c = wt[r * k + i];
+            if (c == 0.0) continue;
+            const double t = th[r * k + i];
+            const double2 w = W[(int64_t)i * total + e], x = X[(int64_t)i * total + e];
+            sx += c * (w.x - t * x.x);
+            sy += c * (w.y - t * x.y);
+        }
+        out[e] = fr2<VT>(make_double2(sx, sy));
+    }
+}
+
+// out[e] = (VT) X[e] over a flat range
+template <typename VT>
+__global__ void k_bto(const double2* __restrict__ X, int64_t total, VT* __restrict__ out) {
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+        out[e] = fr2<VT>(X[e]);
+}
+
+// out[i][n][r] = sum_{a<kx} Y[i][a][r] X[a][n][r] + sum_{j<p} Y[i][kx+j][r] Q[j][n][r]
+// (Y complex, [(i * (kx + p) + a) * NB + r]; FP64 anchors X, FP32 extension Q; FP64 out)
+template <int NB>
+__global__ void __launch_bounds__(kT)
+k_bcombine_xq(const double2* __restrict__ X, int kx, const float2* __restrict__ Q, int p, int64_t N,
+              const double2* __restrict__ Y, int nout, double2* __restrict__ out) {
+    constexpr int OC = 8;
+    const int d = kx + p;
+    const int64_t total = N * NB;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e % NB);
+        for (int c0 = 0; c0 < nout; c0 += OC) {
+            double ax[OC], ay[OC];
+#pragma unroll
+            for (int k = 0; k < OC; ++k) { ax[k] = 0.0; ay[k] = 0.0; }
+#pragma unroll 2
+            for (int a = 0; a < d; ++a) {
+                const double2 v = a < kx ? X[(int64_t)a * total + e] : to2(Q[(int64_t)(a - kx) * total + e]);
+#pragma unroll
+                for (int k = 0; k < OC; ++k) {
+                    if (c0 + k < nout) {
+                        const double2 y = __ldg(Y + ((int64_t)(c0 + k) * d + a) * NB + r);
+                        ax[k] += y.x * v.x - y.y * v.y;
+                        ay[k] += y.x * v.y + y.y * v.x;
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < OC; ++k)
+                if (c0 + k < nout) out[(int64_t)(c0 + k) * total + e] = make_double2(ax[k], ay[k]);
+        }
     }
 }
 
@@ -693,7 +815,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
         for (int pass = 0; pass < 2; ++pass) {
             for (int i = 0; i < k1; ++i) {
                 const double2* rhs = (pass == 0 ? Wb.p : Xb.p) + (size_t)i * stride;
-                k_bproj<double2, NB><<<grid, kT, 0, st>>>(Xb.p, N, k1, rhs, part.p, nullptr);
+                k_bproj<double2, double2, NB><<<bproj_grid(grid, k1), kT, 0, st>>>(Xb.p, N, k1, rhs, part.p, nullptr);
                 k_breduce<NB><<<breduce_grid(k1 + 1, NB), 256, 0, st>>>(part.p, grid, k1 + 1, red.p, nullptr);
                 note_launches(2);
                 MOMED_CUDA_TRY(cudaMemcpyAsync(hr.data(), red.p, hr.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
@@ -787,6 +909,185 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
         }
         okv[q] = ok ? 1 : 0;
         convv[q] = conv;
+    }
+    // Mixed precision, parameters that missed the target: anchored refinement.  The FP64 Ritz
+    // vectors X (with W = H X from the FP64 map) anchor a subspace that an FP32 Lanczos extends,
+    // starting from their residuals.  Rayleigh-Ritz on [X, Q] takes X^H H X, X^H X, X^H H Q =
+    // W^H Q and X^H Q from FP64 data and only Q^H H Q from the FP32 recurrence; an error e there
+    // moves an eigenvalue by about |y_Q|^2 e, where y_Q (the correction's weight) is of the size
+    // of the residual over the gap.  W is recomputed with the FP64 map each cycle, so the
+    // residuals and the acceptance test are exact.  Parameters still failing after the cycles
+    // go on to the FP64 block Lanczos below.
+    if (mixed && m - k1 >= 4) {
+        auto failing = [&]() {
+            int c = 0;
+            for (int q = 0; q < nu; ++q) c += (!okv[q] && !broken[q]) ? 1 : 0;
+            return c;
+        };
+        if (failing() > 0) {
+            const int p = m - k1, d = k1 + p;
+            BlockLanczos<float2, NB> LR(h, m, uv);
+            DevBuf<double> thd, wtd;
+            thd.resize((size_t)NB * k1);
+            wtd.resize((size_t)NB * k1);
+            DevBuf<double2> red, Yd;
+            red.resize((size_t)(kMaxCols + 1) * NB);
+            Yd.resize((size_t)k1 * d * NB);
+            std::vector<int> failed(NB, 0);
+            for (int cyc = 0; cyc < kRefineCycles && failing() > 0; ++cyc) {
+                // anchors and start vector (weighted residuals of the pairs not yet accepted)
+                k_bto<float2><<<eg, 256, 0, st>>>(Xb.p, (int64_t)k1 * stride, LR.col(0));
+                std::vector<double> thh((size_t)NB * k1, 0.0), wth((size_t)NB * k1, 0.0);
+                for (int q = 0; q < nu; ++q) {
+                    for (int i = 0; i < k1; ++i) thh[(size_t)q * k1 + i] = th[q][i];
+                    int used = 0;
+                    for (int i = convv[q]; i < nev; ++i)
+                        if (rs[q][i] > 0.0) { wth[(size_t)q * k1 + i] = std::sqrt(i + 1.0) / rs[q][i]; ++used; }
+                    if (!used)
+                        for (int i = 0; i < nev; ++i)
+                            if (rs[q][i] > 0.0) wth[(size_t)q * k1 + i] = std::sqrt(i + 1.0) / rs[q][i];
+                }
+                MOMED_CUDA_TRY(cudaMemcpyAsync(thd.p, thh.data(), thh.size() * 8, cudaMemcpyHostToDevice, st));
+                MOMED_CUDA_TRY(cudaMemcpyAsync(wtd.p, wth.data(), wth.size() * 8, cudaMemcpyHostToDevice, st));
+                k_bresid_sum<float2, NB><<<eg, 256, 0, st>>>(Wb.p, Xb.p, N, k1, thd.p, wtd.p, LR.col(k1));
+                note_launches(2);
+                MOMED_CUDA_TRY(cudaGetLastError());
+                LR.orth_start(k1);
+                for (int j = k1; j < m; ++j) LR.step(j);
+                matvecs += (int64_t)p * nu;
+                std::vector<double> ha((size_t)NB * m), hb((size_t)NB * m);
+                MOMED_CUDA_TRY(cudaMemcpyAsync(ha.data(), LR.alpha.p, ha.size() * 8, cudaMemcpyDeviceToHost, st));
+                MOMED_CUDA_TRY(cudaMemcpyAsync(hb.data(), LR.beta.p, hb.size() * 8, cudaMemcpyDeviceToHost, st));
+                // FP64 Gram blocks: b_a^H H b_i and b_a^H b_i for the anchors i against [X, Q]
+                std::vector<std::vector<std::complex<double>>> G(NB, std::vector<std::complex<double>>((size_t)d * d)),
+                    S(NB, std::vector<std::complex<double>>((size_t)d * d));
+                std::vector<double2> hr((size_t)(kMaxCols + 1) * NB);
+                auto gram = [&](const void* cols, bool fp32, int ncols, const double2* rhs) {
+                    if (fp32)
+                        k_bproj<float2, double2, NB><<<bproj_grid(LR.grid, ncols), kT, 0, st>>>(
+                            reinterpret_cast<const float2*>(cols), N, ncols, rhs, LR.partial.p, nullptr);
+                    else
+                        k_bproj<double2, double2, NB><<<bproj_grid(LR.grid, ncols), kT, 0, st>>>(
+                            reinterpret_cast<const double2*>(cols), N, ncols, rhs, LR.partial.p, nullptr);
+                    k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(LR.partial.p, LR.grid, ncols + 1, red.p,
+                                                                             nullptr);
+                    note_launches(2);
+                    MOMED_CUDA_TRY(cudaMemcpyAsync(hr.data(), red.p, (size_t)(ncols + 1) * NB * sizeof(double2),
+                                                   cudaMemcpyDeviceToHost, st));
+                    MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+                };
+                for (int i = 0; i < k1; ++i) {
+                    for (int pass = 0; pass < 2; ++pass) {
+                        const double2* rhs = (pass == 0 ? Wb.p : Xb.p) + (size_t)i * stride;
+                        auto& M = pass == 0 ? G : S;
+                        gram(Xb.p, false, k1, rhs);              // x_a^H rhs
+                        for (int q = 0; q < nu; ++q)
+                            for (int a = 0; a < k1; ++a)
+                                M[q][(size_t)i * d + a] = std::complex<double>(hr[a * NB + q].x, hr[a * NB + q].y);
+                        gram(LR.col(k1), true, p, rhs);          // q_j^H rhs
+                        for (int q = 0; q < nu; ++q)
+                            for (int j = 0; j < p; ++j) {
+                                std::complex<double> v(hr[j * NB + q].x, hr[j * NB + q].y);
+                                M[q][(size_t)i * d + k1 + j] = v;
+                                M[q][(size_t)(k1 + j) * d + i] = std::conj(v);
+                            }
+                    }
+                }
+                std::vector<double2> Yh((size_t)k1 * d * NB, make_double2(0.0, 0.0));
+                std::vector<std::vector<double>> tq(NB);
+                std::vector<int> ok_rr(NB, 0);
+                {
+                    std::vector<std::future<void>> fs;
+                    for (int q = 0; q < nu; ++q) {
+                        if (broken[q] || failed[q]) continue;
+                        fs.push_back(std::async(std::launch::async, [&, q]() {
+                            double tmax = 0.0;
+                            for (int i = 0; i < k1; ++i) tmax = std::max(tmax, std::fabs(th[q][i]));
+                            for (int j = 0; j < p; ++j) {
+                                const double a = ha[(size_t)q * m + k1 + j];
+                                G[q][(size_t)(k1 + j) * d + k1 + j] = a;
+                                S[q][(size_t)(k1 + j) * d + k1 + j] = 1.0;
+                                tmax = std::max(tmax, std::fabs(a));
+                                if (j + 1 < p) {
+                                    const double b = hb[(size_t)q * m + k1 + j];
+                                    G[q][(size_t)(k1 + j) * d + k1 + j + 1] = b;
+                                    G[q][(size_t)(k1 + j + 1) * d + k1 + j] = b;
+                                }
+                            }
+                            for (int j = 0; j + 1 < p; ++j)
+                                if (hb[(size_t)q * m + k1 + j] <= 1e-12 * std::max(tmax, 1.0)) return;   // invariant
+                            std::vector<double> t;
+                            std::vector<std::complex<double>> Y;
+                            if (!gen_herm_eig(d, G[q], S[q], t, Y)) return;
+                            for (int i = 0; i < k1; ++i)
+                                for (int a = 0; a < d; ++a) {
+                                    const auto y = Y[(size_t)i * d + a];
+                                    Yh[((size_t)i * d + a) * NB + q] = make_double2(y.real(), y.imag());
+                                }
+                            tq[q] = t;
+                            ok_rr[q] = 1;
+                        }));
+                    }
+                    for (auto& f : fs) f.get();
+                }
+                for (int q = 0; q < NB; ++q) {
+                    if (ok_rr[q]) continue;
+                    if (q < nu && !okv[q]) failed[q] = 1;     // left to the FP64 block Lanczos
+                    for (int i = 0; i < k1; ++i) Yh[((size_t)i * d + i) * NB + q] = make_double2(1.0, 0.0);
+                }
+                MOMED_CUDA_TRY(cudaMemcpyAsync(Yd.p, Yh.data(), Yh.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
+                k_bcombine_xq<NB><<<eg, kT, 0, st>>>(Xb.p, k1, LR.col(k1), p, N, Yd.p, k1, Sb.p);
+                note_launches(1);
+                MOMED_CUDA_TRY(cudaGetLastError());
+                std::swap(Xb.p, Sb.p);
+                for (int i = 0; i < k1; ++i)
+                    BlockMv<double2>::run(h, Xb.p + (size_t)i * stride, Wb.p + (size_t)i * stride, ud64.p, NB);
+                matvecs += (int64_t)k1 * nu;
+                matvecs64 += (int64_t)k1 * nu;
+                for (int q = 0; q < nu; ++q)
+                    if (ok_rr[q])
+                        for (int i = 0; i < k1; ++i) th[q][i] = tq[q][i];
+                // exact FP64 residuals and acceptance
+                const int rg = std::max(1, std::min<int>((int)((stride + 255) / 256), 512));
+                DevBuf<double> part;
+                part.resize((size_t)rg * k1 * NB);
+                std::vector<double> thn((size_t)NB * k1, 0.0);
+                for (int q = 0; q < nu; ++q)
+                    for (int i = 0; i < k1; ++i) thn[(size_t)q * k1 + i] = th[q][i];
+                MOMED_CUDA_TRY(cudaMemcpyAsync(thd.p, thn.data(), thn.size() * 8, cudaMemcpyHostToDevice, st));
+                k_bresid<NB><<<rg, 256, 0, st>>>(Wb.p, Xb.p, N, k1, thd.p, part.p);
+                note_launches(1);
+                MOMED_CUDA_TRY(cudaGetLastError());
+                std::vector<double> hp((size_t)rg * k1 * NB);
+                MOMED_CUDA_TRY(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 8, cudaMemcpyDeviceToHost, st));
+                MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+                for (int q = 0; q < nu; ++q) {
+                    for (int i = 0; i < k1; ++i) {
+                        double s2 = 0.0;
+                        for (int b = 0; b < rg; ++b) s2 += hp[((size_t)b * k1 + i) * NB + q];
+                        rs[q][i] = std::sqrt(s2);
+                    }
+                    if (okv[q] || broken[q] || !ok_rr[q]) continue;
+                    const std::vector<double>& t = tq[q];
+                    int conv = 0;
+                    bool ok = true;
+                    for (int i = 0; i < nev; ++i) {
+                        double gap = 1e300;
+                        for (int j = 0; j < d; ++j)
+                            if (j != i && std::fabs(t[j] - t[i]) > 1e-9 * std::max(1.0, std::fabs(t[i])))
+                                gap = std::min(gap, std::fabs(t[j] - t[i]));
+                        const double est = rs[q][i] * rs[q][i] / std::max(gap, 1e-300);
+                        const bool good = rs[q][i] <= tol || est <= kEigTarget * std::max(1.0, std::fabs(t[i]));
+                        if (good && conv == i) ++conv;
+                        ok = ok && good;
+                    }
+                    convv[q] = conv;
+                    okv[q] = ok ? 1 : 0;
+                }
+                note_launches(LR.launches);
+                LR.launches = 0;
+            }
+        }
     }
     // Parameters that missed the target are finished together: a lockstep FP64 block Lanczos
     // warm-started, per parameter, from the sum of its refined Ritz vectors.

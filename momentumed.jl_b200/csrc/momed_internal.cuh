@@ -18,11 +18,19 @@ struct Error {
     std::string msg;
 };
 
+inline std::string base_name(const char* path) {
+    std::string s(path);
+    size_t k = s.find_last_of('/');
+    return k == std::string::npos ? s : s.substr(k + 1);
+}
+
 #define MOMED_CUDA_TRY(expr)                                                                 \
     do {                                                                                     \
         cudaError_t _e = (expr);                                                             \
         if (_e != cudaSuccess) {                                                             \
-            throw ::momed::Error{MOMED_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e)}; \
+            throw ::momed::Error{MOMED_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(_e) +  \
+                                                  " (" + ::momed::base_name(__FILE__) + ":" +           \
+                                                  std::to_string(__LINE__) + ")"};                    \
         }                                                                                    \
     } while (0)
 

@@ -38,6 +38,8 @@ __device__ __forceinline__ void block_rows(int64_t N, int64_t& r0, int64_t& r1) 
     r1 = min(N, r0 + per);
 }
 
+// Grid: x = row blocks, y = groups of 8 columns; warp w of group g owns column 8g + w (one
+// accumulator per lane, 8 loads of V in flight per warp); group 0 also sums |w|^2.
 template <typename VT>
 __global__ void __launch_bounds__(kVecThreads)
 k_proj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ w, double2* partial,
@@ -46,12 +48,11 @@ k_proj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ w,
     __shared__ double2 ws[kVecThreads];
     __shared__ double red[kVecThreads / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    double2 acc[kColsPerWarp];
-#pragma unroll
-    for (int k = 0; k < kColsPerWarp; ++k) acc[k] = make_double2(0.0, 0.0);
-    double wn2 = 0.0;
+    const int i = blockIdx.y * 8 + wid;
+    double ax = 0.0, ay = 0.0, wn2 = 0.0;
     int64_t r0, r1;
     block_rows(N, r0, r1);
+    const VT* colbase = V + (int64_t)(i < ncols ? i : 0) * N;
     for (int64_t t0 = r0; t0 < r1; t0 += kVecThreads) {
         int64_t n = t0 + threadIdx.x;
         double2 wv = (n < r1) ? to_d2(w[n]) : make_double2(0.0, 0.0);
@@ -59,27 +60,22 @@ k_proj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ w,
         wn2 += wv.x * wv.x + wv.y * wv.y;
         __syncthreads();
         const int rows = (int)((r1 - t0) < (int64_t)kVecThreads ? (r1 - t0) : (int64_t)kVecThreads);
-#pragma unroll
-        for (int k = 0; k < kColsPerWarp; ++k) {
-            int i = wid + 8 * k;
-            if (i < ncols) {
-                const VT* col = V + (int64_t)i * N + t0;
-                for (int r = lane; r < rows; r += 32) {
-                    double2 p = cmul_conj(to_d2(col[r]), ws[r]);
-                    acc[k].x += p.x;
-                    acc[k].y += p.y;
-                }
+        if (i < ncols) {
+            const VT* col = colbase + t0;
+#pragma unroll 8
+            for (int r = lane; r < rows; r += 32) {
+                double2 p = cmul_conj(to_d2(col[r]), ws[r]);
+                ax += p.x;
+                ay += p.y;
             }
         }
         __syncthreads();
     }
     double2* out = partial + (int64_t)blockIdx.x * (kMaxCols + 1);
-#pragma unroll
-    for (int k = 0; k < kColsPerWarp; ++k) {
-        int i = wid + 8 * k;
-        double sx = warp_sum(acc[k].x), sy = warp_sum(acc[k].y);
-        if (i < ncols && lane == 0) out[i] = make_double2(sx, sy);
-    }
+    ax = warp_sum(ax);
+    ay = warp_sum(ay);
+    if (i < ncols && lane == 0) out[i] = make_double2(ax, ay);
+    if (blockIdx.y != 0) return;
     wn2 = warp_sum(wn2);
     if (lane == 0) red[wid] = wn2;
     __syncthreads();
@@ -122,6 +118,7 @@ k_update(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restri
     double wn2 = 0.0;
     for (int64_t n = r0 + threadIdx.x; n < r1; n += kVecThreads) {
         double2 acc = to_d2(w[n]);
+#pragma unroll 8
         for (int i = 0; i < ncols; ++i) {
             double2 p = cmul(c[i], to_d2(V[(int64_t)i * N + n]));
             acc.x -= p.x;
@@ -199,6 +196,7 @@ k_combine(const VIN* V, int64_t N, int m, const double* __restrict__ U, int nout
     const int ncopy = copy_col >= 0 ? 1 : 0;
     for (int64_t t0 = (int64_t)blockIdx.x * TR; t0 < N; t0 += (int64_t)gridDim.x * TR) {
         const int rows = (int)((N - t0) < (int64_t)TR ? (N - t0) : (int64_t)TR);
+#pragma unroll 4
         for (int e = threadIdx.x; e < (m + ncopy) * TR; e += blockDim.x) {
             int a = e / TR, r = e % TR;
             int col = (a < m) ? a : copy_col;
@@ -304,7 +302,8 @@ template <typename VT>
 void vec_proj(const VT* V, int64_t N, int ncols, const VT* w, double2* partial, int grid, const int* active,
               cudaStream_t st) {
     MOMED_REQUIRE(ncols <= kMaxCols, MOMED_EINVAL, "krylovdim too large");
-    k_proj<VT><<<grid, kVecThreads, 0, st>>>(V, N, ncols, w, partial, active);
+    k_proj<VT><<<dim3(grid, (unsigned)std::max(1, (ncols + 7) / 8)), kVecThreads, 0, st>>>(V, N, ncols, w, partial,
+                                                                                            active);
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }
@@ -347,19 +346,24 @@ void vec_random(VT* v, int64_t N, uint64_t seed, cudaStream_t st) {
 template <typename VIN, typename VOUT>
 void vec_combine(const VIN* V, int64_t N, int m, const double* U, int nout, VOUT* out, int64_t out_ld, int copy_col,
                  cudaStream_t st) {
+    // The shared-memory limit is a process-wide attribute of the kernel: it is always set to the
+    // largest tile the kernel can get, so callers on other threads never lower it under a launch.
     const int ncopy = copy_col >= 0 ? 1 : 0;
+    MOMED_REQUIRE(m + ncopy <= kMaxCols + 1, MOMED_EINVAL, "krylovdim too large");
     if (m + ncopy <= 100) {
         constexpr int TR = 64;
         size_t smem = (size_t)(m + ncopy) * TR * sizeof(double2);
         auto k = k_combine<VIN, VOUT, TR>;
-        MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)(100 * TR * sizeof(double2))));
         int grid = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sm_count() * 2));
         k<<<grid, kVecThreads, smem, st>>>(V, N, m, U, nout, out, out_ld, copy_col);
     } else {
         constexpr int TR = 32;
         size_t smem = (size_t)(m + ncopy) * TR * sizeof(double2);
         auto k = k_combine<VIN, VOUT, TR>;
-        MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)((kMaxCols + 1) * TR * sizeof(double2))));
         int grid = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sm_count() * 2));
         k<<<grid, kVecThreads, smem, st>>>(V, N, m, U, nout, out, out_ld, copy_col);
     }

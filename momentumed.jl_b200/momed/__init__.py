@@ -6,7 +6,7 @@ ED_scatterlist_onebody/twobody, Scatter, MBOperator, HilbertSubspace,
 MBS64Vector, EDsolve) and every compute step runs in libmomed_b200.so (CUDA,
 sm_100a) through its C ABI.  There is no CPU fallback.
 """
-from ._lib import Handle, MomedError, NotConverged, version
+from ._lib import Handle, MomedError, NotConverged, Server, version
 from .core import (MBS64, HilbertSubspace, MBOperator, MBS64Vector, Scatter, ScatterList, hermitian_complete,
                    index_fit, make_mask64, occ_list, parity_mask, scat_occ_number, sort_merge_scatlist)
 from .methods import (DEFAULT_GPU, GPU_AVAILABLE, EDsolve, LinearMap, activate_b200, activate_gpu_device,
@@ -16,7 +16,7 @@ from .preparation import (ED_momentum_subspaces, ED_scatterlist_onebody, ED_scat
                           group_momentum_pairs, momentum_residue)
 
 __all__ = [
-    "Handle", "MomedError", "NotConverged", "version",
+    "Handle", "MomedError", "NotConverged", "Server", "version",
     "MBS64", "HilbertSubspace", "MBOperator", "MBS64Vector", "Scatter", "ScatterList", "hermitian_complete",
     "index_fit", "make_mask64", "occ_list", "parity_mask", "scat_occ_number", "sort_merge_scatlist",
     "DEFAULT_GPU", "GPU_AVAILABLE", "EDsolve", "LinearMap", "activate_b200", "activate_gpu_device",

@@ -337,14 +337,25 @@ class Handle:
                                    "seconds": info.seconds}
 
     def batch_solve(self, u: np.ndarray, nev: int, krylovdim: int = 30, tol: float = 1e-12, maxiter: int = 100,
-                    seed: int = 0, precision: int = PREC_MIXED, want_vectors: bool = False):
+                    seed: int = 0, precision: int = PREC_MIXED, want_vectors: bool = False,
+                    out_vecs: np.ndarray | None = None):
+        """out_vecs: optional caller-owned C-contiguous complex128 array of shape (len(u), nev, n)
+        (pinned host memory makes the copy-out fast); used instead of a fresh array."""
         u = np.ascontiguousarray(u, np.float64)
         n = self.n
         nev_eff = min(nev, n)
         opts = SolveOpts(nev, krylovdim, maxiter, precision, tol, seed, int(want_vectors), 0)
         vals = np.zeros((len(u), nev_eff))
         resid = np.zeros((len(u), nev_eff))
-        vecs = np.zeros((len(u), nev_eff, n), np.complex128) if want_vectors else None
+        vecs = None
+        if want_vectors:
+            if out_vecs is not None:
+                if (out_vecs.dtype != np.complex128 or out_vecs.shape != (len(u), nev_eff, n)
+                        or not out_vecs.flags.c_contiguous):
+                    raise ValueError(f"out_vecs must be C-contiguous complex128 of shape {(len(u), nev_eff, n)}")
+                vecs = out_vecs
+            else:
+                vecs = np.zeros((len(u), nev_eff, n), np.complex128)
         info = Info()
         rc = lib().momed_batch_solve(self._h, C.byref(opts), _p(u), len(u), _p(vals), _p(resid), _p(vecs),
                                      C.byref(info))

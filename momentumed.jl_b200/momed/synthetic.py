@@ -117,6 +117,23 @@ WORKLOADS = {
     "two_comp_4x6": dict(a=4, b=6, N_each=(4, 4), nev=8, seed=3, Nc_conserve=2),
 }
 
+# Meshes of the serving stream (Poisson arrivals at 50 req/s, seed 4): mesh -> (electrons, recipe seed)
+SERVE_MESHES = {"3x5": (5, 0), "3x9": (9, 2), "3x10": (10, 1), "4x9": (12, 4)}
+
+
+def serve_requests(n: int, meshes, sector_counts, rate: float = 50.0, seed: int = 4):
+    """The serving stream: n requests with Poisson arrivals at `rate` per second.  Each picks a
+    mesh uniformly from `meshes`, a uniform sector of it (`sector_counts[mesh]` sectors),
+    U0 ~ U(0.5, 2), nev in 1..20 and tolerance 1e-10.  Returns dicts sorted by arrival (s)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    out = []
+    for i in range(n):
+        mesh = meshes[int(rng.integers(len(meshes)))]
+        out.append(dict(arrival=float(t[i]), mesh=mesh, sector=int(rng.integers(sector_counts[mesh])),
+                        u=float(rng.uniform(0.5, 2.0)), nev=int(rng.integers(1, 21)), tol=1e-10))
+    return out
+
 
 def u_grid(n: int = 32, lo: float = 0.5, hi: float = 2.0) -> np.ndarray:
     """Interaction strengths U0 of the sweep, evenly spaced over [lo, hi]."""

@@ -155,3 +155,20 @@ def test_no_device_fails_loudly():
         pytest.skip("a GPU is present")
     with pytest.raises(momed.MomedError):
         momed.Handle(0)
+
+
+def test_serving_stream_is_seeded_poisson():
+    """The serving stream: seeded, arrivals increasing at about 50/s, fields in their ranges."""
+    from momed.synthetic import SERVE_MESHES, serve_requests
+    counts = {"3x5": 15, "3x9": 27, "3x10": 30, "4x9": 36}
+    meshes = list(SERVE_MESHES)
+    a = serve_requests(2000, meshes, counts)
+    b = serve_requests(2000, meshes, counts)
+    assert a == b
+    t = np.array([r["arrival"] for r in a])
+    assert np.all(np.diff(t) > 0)
+    assert abs(len(t) / t[-1] - 50.0) < 5.0
+    assert {r["mesh"] for r in a} == set(meshes)
+    assert all(0 <= r["sector"] < counts[r["mesh"]] for r in a)
+    assert all(1 <= r["nev"] <= 20 and 0.5 <= r["u"] <= 2.0 and r["tol"] == 1e-10 for r in a)
+    assert serve_requests(5, meshes, counts, seed=5) != a[:5]
