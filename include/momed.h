@@ -140,7 +140,8 @@ MOMED_API int  momed_eigsolve(momed_handle* h, const momed_solve_opts* opts, con
 
 /* Batched solve of H(u) = A + u B (momed_set_scatter_pair) for nu values of u at once on the
  * working basis: block matvec over all u, one Lanczos per u.  vals [nu][nev], resid [nu][nev];
- * vecs [nu][nev][N] c128 host (may be NULL).  Mixed precision is opts->precision. */
+ * vecs [nu][nev][N] c128 host (may be NULL).  Mixed precision is opts->precision.  With a
+ * single operator (momed_set_scatter) every u solves H = A. */
 MOMED_API int  momed_batch_solve(momed_handle* h, const momed_solve_opts* opts, const double* u, int32_t nu,
                        double* vals, double* resid, double* vecs, momed_info* info);
 

@@ -5,7 +5,9 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+#include <vector>
 
 #include "index.cuh"
 
@@ -204,6 +206,8 @@ void ensure_ready(momed_handle* h) {
     }
 }
 
+thread_local cudaStream_t g_alloc_stream = nullptr;
+
 }  // namespace momed
 
 namespace {
@@ -211,6 +215,7 @@ namespace {
 template <typename F>
 int guarded(momed_handle* h, F&& f) {
     try {
+        AllocScope scope(h ? h->stream : g_alloc_stream);
         if (h) {
             cudaError_t e = cudaSetDevice(h->device);
             if (e != cudaSuccess) throw Error{MOMED_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e)};
@@ -228,6 +233,20 @@ int guarded(momed_handle* h, F&& f) {
 }
 
 thread_local std::string g_create_error;
+
+// The default memory pool of each device keeps freed blocks for reuse instead of returning them
+// at every synchronisation (set once per device; process-local, gone at exit).
+void keep_pool_memory(int device) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (std::find(done.begin(), done.end(), device) != done.end()) return;
+    cudaMemPool_t pool;
+    MOMED_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, device));
+    uint64_t thr = UINT64_MAX;
+    MOMED_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    done.push_back(device);
+}
 
 __global__ void k_or_basis(const uint64_t* b, int64_t n, unsigned long long* out) {
     uint64_t acc = 0;
@@ -268,8 +287,10 @@ int momed_create(int device, momed_handle** out) {
     momed_handle* h = new momed_handle();
     h->device = device;
     int rc = guarded(h, [&]() {
+        keep_pool_memory(device);
         MOMED_CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
         h->own_stream = true;
+        g_alloc_stream = h->stream;   // this call's scope (set before the stream existed)
         MOMED_CUDA_TRY(cudaEventCreate(&h->ev0));
         MOMED_CUDA_TRY(cudaEventCreate(&h->ev1));
         std::vector<uint32_t> b(33 * 33, 0);
@@ -306,9 +327,18 @@ int momed_destroy(momed_handle* h) {
     for (cudaEvent_t e : h->prof_ev) cudaEventDestroy(e);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
-    cudaStream_t st = h->own_stream ? h->stream : nullptr;
-    delete h;   // releases every DevBuf
-    if (st) cudaStreamDestroy(st);
+    cudaStream_t hs = h->stream;
+    const bool own = h->own_stream;
+    {
+        AllocScope scope(hs);
+        delete h;   // releases every DevBuf, ordered on the handle's stream
+    }
+    cudaStreamSynchronize(hs);
+    if (own && hs) cudaStreamDestroy(hs);
+    cudaMemPool_t pool;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+        cudaMemPoolTrimTo(pool, 0);   // return blocks no other handle is using
     return MOMED_OK;
 }
 

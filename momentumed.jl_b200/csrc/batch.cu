@@ -143,6 +143,14 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W
     }
 }
 
+// Row blocks of k_bproj for ncols columns: about 6 blocks per SM over all column groups, between
+// 1 and 4 per SM, never more than the row tiles; maxrb (the partial buffer's capacity) caps it.
+inline int bproj_rowblocks(int64_t N, int ncols, int sm, int maxrb) {
+    const int groups = std::max(1, (ncols + 7) / 8);
+    int rb = std::max(sm, std::min(4 * sm, 6 * sm / groups));
+    rb = (int)std::min<int64_t>(rb, (N + kRowsTile - 1) / kRowsTile);
+    return std::max(1, std::min(rb, maxrb));
+}
 inline dim3 bproj_grid(int rowblocks, int ncols) { return dim3(rowblocks, (unsigned)std::max(1, (ncols + 7) / 8)); }
 
 __device__ __forceinline__ double wsum(double v) {
@@ -419,7 +427,7 @@ struct BlockLanczos {
     int64_t launches = 0;
 
     BlockLanczos(momed_handle* hh, int mm, const std::vector<double>& u) : h(hh), N(hh->n), m(mm), st(hh->stream) {
-        grid = std::max(1, std::min<int>((int)((N + kRowsTile - 1) / kRowsTile), sms() * 2));
+        grid = std::max(1, std::min<int>((int)((N + kRowsTile - 1) / kRowsTile), sms() * 4));   // max row blocks
         ugrid = std::max(1, std::min<int>((int)((N * NB + kT - 1) / kT), sms() * 8));
         V.resize((size_t)(m + 1) * N * NB);
         partial.resize((size_t)grid * (kMaxCols + 1) * NB);
@@ -442,8 +450,9 @@ struct BlockLanczos {
     VT* col(int i) { return V.p + (size_t)i * N * NB; }
 
     void proj(int ncols, const VT* w, double2* out, const int* act) {
-        k_bproj<VT, VT, NB><<<bproj_grid(grid, ncols), kT, 0, st>>>(V.p, N, ncols, w, partial.p, act);
-        k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(partial.p, grid, ncols + 1, out, act);
+        const int rb = bproj_rowblocks(N, ncols, sms(), grid);
+        k_bproj<VT, VT, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(V.p, N, ncols, w, partial.p, act);
+        k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(partial.p, rb, ncols + 1, out, act);
         launches += 2;
     }
     void update(int ncols, const double2* coef, VT* w, const int* active, const int* act) {
@@ -963,13 +972,14 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                     S(NB, std::vector<std::complex<double>>((size_t)d * d));
                 std::vector<double2> hr((size_t)(kMaxCols + 1) * NB);
                 auto gram = [&](const void* cols, bool fp32, int ncols, const double2* rhs) {
+                    const int rb = bproj_rowblocks(N, ncols, sms(), LR.grid);
                     if (fp32)
-                        k_bproj<float2, double2, NB><<<bproj_grid(LR.grid, ncols), kT, 0, st>>>(
+                        k_bproj<float2, double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
                             reinterpret_cast<const float2*>(cols), N, ncols, rhs, LR.partial.p, nullptr);
                     else
-                        k_bproj<double2, double2, NB><<<bproj_grid(LR.grid, ncols), kT, 0, st>>>(
+                        k_bproj<double2, double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
                             reinterpret_cast<const double2*>(cols), N, ncols, rhs, LR.partial.p, nullptr);
-                    k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(LR.partial.p, LR.grid, ncols + 1, red.p,
+                    k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(LR.partial.p, rb, ncols + 1, red.p,
                                                                              nullptr);
                     note_launches(2);
                     MOMED_CUDA_TRY(cudaMemcpyAsync(hr.data(), red.p, (size_t)(ncols + 1) * NB * sizeof(double2),
@@ -1206,7 +1216,7 @@ using namespace momed;
 int momed_batch_solve_impl(momed_handle* h, const momed_solve_opts* o, const double* u, int32_t nu, double* vals,
                            double* resid, double* vecs, momed_info* info) {
     ensure_ready(h);
-    MOMED_REQUIRE(h->op.has_b, MOMED_ESTATE, "batched solves need an operator pair (momed_set_scatter_pair)");
+    // without a second operator (momed_set_scatter) every parameter solves H = A
     MOMED_REQUIRE(nu >= 1 && nu <= 32, MOMED_EINVAL, "nu must be 1..32 per call");
     int nb = 1;
     while (nb < nu) nb <<= 1;

@@ -40,7 +40,20 @@ inline std::string base_name(const char* path) {
     } while (0)
 
 // ---------------------------------------------------------------- device buffer
-// Owning device allocation (cudaMalloc / cudaFree); moves only.
+// Stream on which the calling thread's DevBuf allocations and frees are ordered: the handle's
+// stream for the duration of an API call (AllocScope).  Allocation is stream-ordered
+// (cudaMallocAsync / cudaFreeAsync from the device's default memory pool), so freeing a solve's
+// buffers does not synchronise the device and solves on other streams keep running.
+extern thread_local cudaStream_t g_alloc_stream;
+struct AllocScope {
+    cudaStream_t prev;
+    explicit AllocScope(cudaStream_t s) : prev(g_alloc_stream) { g_alloc_stream = s; }
+    ~AllocScope() { g_alloc_stream = prev; }
+    AllocScope(const AllocScope&) = delete;
+    AllocScope& operator=(const AllocScope&) = delete;
+};
+
+// Owning device allocation, ordered on g_alloc_stream; moves only.
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
@@ -55,7 +68,7 @@ struct DevBuf {
     }
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) cudaFreeAsync(p, g_alloc_stream);
         p = nullptr;
         n = 0;
     }
@@ -63,10 +76,11 @@ struct DevBuf {
         if (count <= n && p) return;
         release();
         if (count == 0) return;
-        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), g_alloc_stream);
         if (e != cudaSuccess) {
             p = nullptr;
-            throw Error{MOMED_ENOMEM, std::string("cudaMalloc of ") + std::to_string(count * sizeof(T)) +
+            cudaGetLastError();
+            throw Error{MOMED_ENOMEM, std::string("device allocation of ") + std::to_string(count * sizeof(T)) +
                                           " bytes failed: " + cudaGetErrorString(e)};
         }
         n = count;

@@ -62,7 +62,7 @@ struct momed_server {
     std::condition_variable cv_work, cv_done;
     std::deque<std::shared_ptr<Request>> queue;
     std::unordered_map<int64_t, std::shared_ptr<Request>> all;
-    std::vector<HostOperator> ops;
+    std::vector<std::shared_ptr<const HostOperator>> ops;   // read by workers under mu
     std::vector<std::thread> workers;
     std::vector<momed_handle*> handles;
     int64_t next_id = 1;
@@ -79,20 +79,31 @@ int64_t estimate_bytes(int64_t N, const momed_solve_opts& o) {
     if (m > N) m = N;
     int64_t nev = o.nev;
     const bool mixed = o.precision == MOMED_PREC_MIXED;
-    int64_t s = mixed ? 8 : 16;
     int64_t k1 = nev + (mixed ? 4 : 0);
     int64_t b = 8 * N;                                // basis
-    b += (m + 1) * N * s;                             // Krylov basis
-    b += (mixed ? 3 * k1 : 0) * N * 16;               // refinement X, W, scratch
-    b += 2 * std::max<int64_t>(nev, 1) * N * 16;      // output vectors + residual workspace
+    if (mixed) {
+        // batched solver with one right-hand side: the FP32 Krylov basis and its restart copy,
+        // Ritz vectors X, W = H X and scratch, the FP64 block Lanczos fallback (basis + restart
+        // copy), its vectors and the returned vectors
+        b += 2 * (m + 1) * N * 16;
+        b += 3 * k1 * N * 16;
+        b += 2 * std::max<int64_t>(k1, nev) * N * 16;
+    } else {
+        b += 2 * (m + 1) * N * 16;                    // Krylov basis and restart scratch
+        b += 2 * std::max<int64_t>(nev, 1) * N * 16;  // output vectors + residual workspace
+    }
     b += 16ll << 20;                                  // index tables, term lists, partial sums
     return b;
 }
 
 void worker_loop(momed_server* S, int slot) {
     momed_handle* h = S->handles[slot];
+    cudaSetDevice(S->device);
+    AllocScope scope(h->stream);       // this slot's buffers are ordered on its own stream
+    int32_t cur_op = -1;               // operator resident on this slot's handle
     for (;;) {
         std::shared_ptr<Request> r;
+        std::shared_ptr<const HostOperator> opp;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             // FIFO admission: the head request starts when it fits the free budget
@@ -104,6 +115,7 @@ void worker_loop(momed_server* S, int slot) {
             if (S->stopping) return;
             r = S->queue.front();
             S->queue.pop_front();
+            if (r->op >= 0 && r->op < (int32_t)S->ops.size()) opp = S->ops[r->op];
             S->used += r->bytes;
             r->status = 1;
             r->start = clock_t_::now();
@@ -111,8 +123,8 @@ void worker_loop(momed_server* S, int slot) {
         int rc = MOMED_OK;
         std::string err;
         try {
-            cudaSetDevice(S->device);
-            const HostOperator& op = S->ops[r->op];
+            MOMED_REQUIRE(opp != nullptr, MOMED_EINVAL, "unknown operator id");
+            const HostOperator& op = *opp;
             const int64_t N = (int64_t)r->basis.size();
             h->basis.resize(std::max<int64_t>(N, 1));
             MOMED_CUDA_TRY(cudaMemcpyAsync(h->basis.p, r->basis.data(), N * 8, cudaMemcpyHostToDevice, h->stream));
@@ -121,8 +133,12 @@ void worker_loop(momed_server* S, int slot) {
             h->op_validated = false;
             h->basis_or = 0;
             for (uint64_t v : r->basis) h->basis_or |= v;
-            upload_operator(h, op.amp_a.data(), op.has_b ? op.amp_b.data() : nullptr, op.in.data(), op.out.data(),
-                            op.parity.empty() ? nullptr : op.parity.data(), (int64_t)op.in.size());
+            if (cur_op != r->op) {
+                cur_op = -1;
+                upload_operator(h, op.amp_a.data(), op.has_b ? op.amp_b.data() : nullptr, op.in.data(),
+                                op.out.data(), op.parity.empty() ? nullptr : op.parity.data(), (int64_t)op.in.size());
+                cur_op = r->op;
+            }
             double u = r->u;
             float uf = (float)u;
             MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
@@ -133,7 +149,13 @@ void worker_loop(momed_server* S, int slot) {
             r->resid.assign(nev, 0.0);
             momed_solve_opts o = r->opts;
             o.want_vectors = 0;
-            rc = momed_eigsolve_impl(h, &o, nullptr, r->vals.data(), r->resid.data(), nullptr, &r->info);
+            if (o.precision == MOMED_PREC_MIXED) {
+                // mixed precision: the batched solver with one right-hand side (FP32 Lanczos, FP64
+                // Rayleigh-Ritz, anchored refinement); H(u) = A + u B, or A when B is absent
+                rc = momed_batch_solve_impl(h, &o, &u, 1, r->vals.data(), r->resid.data(), nullptr, &r->info);
+            } else {
+                rc = momed_eigsolve_impl(h, &o, nullptr, r->vals.data(), r->resid.data(), nullptr, &r->info);
+            }
             if (rc == MOMED_ENOTCONV) rc = MOMED_OK;   // results written; info.converged tells
         } catch (const Error& e) {
             rc = e.code;
@@ -198,7 +220,7 @@ MOMED_API int momed_serve_register_operator(momed_server* S, const double* amp_a
     if (parity) op.parity.assign(parity, parity + nscat);
     else op.parity.clear();
     std::lock_guard<std::mutex> lk(S->mu);
-    S->ops.push_back(std::move(op));
+    S->ops.push_back(std::make_shared<const HostOperator>(std::move(op)));
     *op_id = (int32_t)S->ops.size() - 1;
     return MOMED_OK;
 }

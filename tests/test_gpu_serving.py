@@ -122,3 +122,45 @@ def test_unknown_operator_and_bad_request(workload):
     with pytest.raises(momed.MomedError):
         srv.submit(op, b35[0], 1.0, 0)          # nev < 1
     srv.stop()
+
+
+def test_mixed_precision_requests(workload):
+    """Mixed-precision requests (batched solver with one right-hand side): the same result alone
+    and in a mix with FP64 and other mixed requests, and within 1e-10 of the FP64 solver."""
+    p35, p38, b35, b38 = workload
+    srv = _lib.Server(0, slots=4)
+    op35 = srv.register_operator(*p35)
+    op38 = srv.register_operator(*p38)
+    rid = srv.submit(op38, b38[1], 0.8, 6, tol=1e-10, seed=3, precision=_lib.PREC_MIXED)
+    alone, _, info, _, _ = wait_all(srv, [rid], {rid: 6})[rid]
+    assert info["converged"] >= 6
+    rids, nev = [], {}
+    for k in range(8):
+        if k == 3:
+            r = srv.submit(op38, b38[1], 0.8, 6, tol=1e-10, seed=3, precision=_lib.PREC_MIXED)
+            target, n = r, 6
+        else:
+            n = 1 + k
+            prec = _lib.PREC_MIXED if k % 2 else _lib.PREC_FP64
+            r = srv.submit(op35, b35[k], 1.0 + 0.1 * k, n, tol=1e-10, seed=k, precision=prec)
+        nev[r] = n
+        rids.append(r)
+    res = wait_all(srv, rids, nev)
+    assert np.max(np.abs(res[target][0] - alone) / np.abs(alone)) < 1e-12
+    assert srv.stats()["failed"] == 0
+    srv.stop()
+    h = momed.Handle(0)
+    h.set_scatter_pair(*p38)
+    h.set_basis(b38[1])
+    h.set_param(0.8)
+    v, _, _, _ = h.eigsolve(6, tol=1e-12, seed=1, want_vectors=False)
+    h.set_scatter_pair(*p35)
+    for r, k in zip(rids, range(8)):
+        if k == 3:
+            continue
+        h.set_basis(b35[k])
+        h.set_param(1.0 + 0.1 * k)
+        ref, _, _, _ = h.eigsolve(nev[r], tol=1e-12, seed=1, want_vectors=False)
+        assert np.max(np.abs(res[r][0] - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-10
+    h.close()
+    assert np.max(np.abs(v - alone) / np.abs(v)) < 1e-10
