@@ -5,13 +5,18 @@
 // takes requests in arrival order as soon as (a) a slot is free and (b) the request's HBM
 // estimate fits the server's budget; every admitted solve keeps its Krylov basis and
 // recurrence coefficients in HBM for its whole life, and the slots' kernels overlap on the
-// device.  A request larger than the whole budget fails at once with MOMED_ENOMEM; a request
+// device.  Continuous batching: a worker that takes the head request also takes every queued
+// request on the same operator, sector basis and precision (up to 32, as long as the group
+// fits the budget) and solves them as one batched solve, one right-hand side per request's
+// parameter u; the block map then evaluates each candidate term once for the whole group.  A
+// request alone runs the FP64 single-vector solver, the fastest form for one right-hand side.  A request larger than the whole budget fails at once with MOMED_ENOMEM; a request
 // can be cancelled while queued; every wait the API offers is bounded and returns
 // MOMED_ETIMEOUT when it runs out.
 //
 // A solve is deterministic (seeded start vector, fixed reduction order), so a request's
 // result is the same alone and in any mix.
 #include <chrono>
+#include <cstring>
 #include <condition_variable>
 #include <deque>
 #include <memory>
@@ -41,6 +46,7 @@ struct Request {
     int64_t id = 0;
     int32_t op = 0;
     std::vector<uint64_t> basis;
+    uint64_t bhash = 0;          // hash of the basis, to find requests on the same sector
     double u = 1.0;
     momed_solve_opts opts{};
     int64_t bytes = 0;
@@ -74,17 +80,21 @@ struct momed_server {
 namespace {
 
 // HBM a solve needs: basis, index tables (bounded), Krylov basis, Ritz/refinement buffers.
-int64_t estimate_bytes(int64_t N, const momed_solve_opts& o) {
+// nb: right-hand sides of a batched solve (a power of two), 0 for the single-vector solver.
+int64_t estimate_bytes(int64_t N, const momed_solve_opts& o, int64_t nb = 0) {
     int64_t m = o.krylovdim > 0 ? o.krylovdim : 30;
     if (m > N) m = N;
     int64_t nev = o.nev;
-    const bool mixed = o.precision == MOMED_PREC_MIXED;
-    int64_t k1 = nev + (mixed ? 4 : 0);
     int64_t b = 8 * N;                                // basis
-    if (mixed) {
-        // batched solver with one right-hand side: the FP32 Krylov basis and its restart copy,
-        // Ritz vectors X, W = H X and scratch, the FP64 block Lanczos fallback (basis + restart
-        // copy), its vectors and the returned vectors
+    if (nb > 0) {
+        // batched solver: the Krylov basis and its restart copy (FP64 fallback at worst), Ritz
+        // vectors X, W = H X and scratch, the fallback's vectors and the returned vectors
+        const int64_t k1 = nev + 4;
+        b += 2 * (m + 1) * N * nb * 16;
+        b += 3 * k1 * N * nb * 16;
+        b += 2 * std::max<int64_t>(k1, nev) * N * nb * 16;
+    } else if (o.precision == MOMED_PREC_MIXED) {
+        const int64_t k1 = nev + 4;                   // single vector: FP32 basis, FP64 finish
         b += 2 * (m + 1) * N * 16;
         b += 3 * k1 * N * 16;
         b += 2 * std::max<int64_t>(k1, nev) * N * 16;
@@ -96,14 +106,35 @@ int64_t estimate_bytes(int64_t N, const momed_solve_opts& o) {
     return b;
 }
 
+// Group parameters of a batched solve: nev, krylovdim and maxiter the largest, tol the smallest.
+momed_solve_opts group_opts(const std::vector<std::shared_ptr<Request>>& g) {
+    momed_solve_opts o = g[0]->opts;
+    for (const auto& q : g) {
+        o.nev = std::max(o.nev, q->opts.nev);
+        o.krylovdim = std::max(o.krylovdim, q->opts.krylovdim);
+        o.maxiter = std::max(o.maxiter, q->opts.maxiter);
+        if (q->opts.tol > 0 && (o.tol <= 0 || q->opts.tol < o.tol)) o.tol = q->opts.tol;
+    }
+    o.want_vectors = 0;
+    o.vecs_on_device = 0;
+    return o;
+}
+
+int64_t pow2_at_least(int64_t n) {
+    int64_t p = 1;
+    while (p < n) p <<= 1;
+    return p;
+}
+
 void worker_loop(momed_server* S, int slot) {
     momed_handle* h = S->handles[slot];
     cudaSetDevice(S->device);
     AllocScope scope(h->stream);       // this slot's buffers are ordered on its own stream
     int32_t cur_op = -1;               // operator resident on this slot's handle
     for (;;) {
-        std::shared_ptr<Request> r;
+        std::vector<std::shared_ptr<Request>> grp;
         std::shared_ptr<const HostOperator> opp;
+        int64_t gbytes = 0;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             // FIFO admission: the head request starts when it fits the free budget
@@ -113,15 +144,44 @@ void worker_loop(momed_server* S, int slot) {
                 return !S->queue.empty() && S->used + S->queue.front()->bytes <= S->budget;
             });
             if (S->stopping) return;
-            r = S->queue.front();
+            auto r = S->queue.front();
             S->queue.pop_front();
+            grp.push_back(r);
+            gbytes = r->bytes;
             if (r->op >= 0 && r->op < (int32_t)S->ops.size()) opp = S->ops[r->op];
-            S->used += r->bytes;
-            r->status = 1;
-            r->start = clock_t_::now();
+            // continuous batching: queued requests on the same operator, sector and precision
+            const int64_t N = (int64_t)r->basis.size();
+            for (auto it = S->queue.begin(); it != S->queue.end() && grp.size() < 32;) {
+                const auto& q = *it;
+                const bool same = q->status == 0 && q->op == r->op && q->opts.precision == r->opts.precision &&
+                                  q->bhash == r->bhash && (int64_t)q->basis.size() == N &&
+                                  std::memcmp(q->basis.data(), r->basis.data(), (size_t)N * 8) == 0;
+                if (!same) {
+                    ++it;
+                    continue;
+                }
+                grp.push_back(q);
+                const int64_t need = estimate_bytes(N, group_opts(grp), pow2_at_least((int64_t)grp.size()));
+                if (S->used + need > S->budget) {
+                    grp.pop_back();
+                    break;
+                }
+                gbytes = need;
+                it = S->queue.erase(it);
+            }
+            S->used += gbytes;
+            const auto now = clock_t_::now();
+            for (auto& q : grp) {
+                q->status = 1;
+                q->start = now;
+            }
         }
         int rc = MOMED_OK;
         std::string err;
+        std::vector<double> gvals, gres;
+        momed_info ginfo{};
+        const auto& r = grp[0];
+        const int nu = (int)grp.size();
         try {
             MOMED_REQUIRE(opp != nullptr, MOMED_EINVAL, "unknown operator id");
             const HostOperator& op = *opp;
@@ -139,24 +199,33 @@ void worker_loop(momed_server* S, int slot) {
                                 op.out.data(), op.parity.empty() ? nullptr : op.parity.data(), (int64_t)op.in.size());
                 cur_op = r->op;
             }
-            double u = r->u;
-            float uf = (float)u;
-            MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
-            MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(uf), cudaMemcpyHostToDevice, h->stream));
-            MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
-            int nev = (int)std::min<int64_t>(r->opts.nev, N);
-            r->vals.assign(nev, 0.0);
-            r->resid.assign(nev, 0.0);
-            momed_solve_opts o = r->opts;
-            o.want_vectors = 0;
-            if (o.precision == MOMED_PREC_MIXED) {
-                // mixed precision: the batched solver with one right-hand side (FP32 Lanczos, FP64
-                // Rayleigh-Ritz, anchored refinement); H(u) = A + u B, or A when B is absent
-                rc = momed_batch_solve_impl(h, &o, &u, 1, r->vals.data(), r->resid.data(), nullptr, &r->info);
+            momed_solve_opts o = group_opts(grp);
+            const int nev = (int)std::min<int64_t>(o.nev, N);
+            gvals.assign((size_t)nu * nev, 0.0);
+            gres.assign((size_t)nu * nev, 0.0);
+            if (nu == 1) {
+                // one right-hand side: the FP64 single-vector solver (a mixed request gets FP64
+                // arithmetic throughout, which is faster here and at least as accurate)
+                double u = r->u;
+                float uf = (float)u;
+                MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
+                MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(uf), cudaMemcpyHostToDevice, h->stream));
+                MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+                o.precision = MOMED_PREC_FP64;
+                rc = momed_eigsolve_impl(h, &o, nullptr, gvals.data(), gres.data(), nullptr, &ginfo);
             } else {
-                rc = momed_eigsolve_impl(h, &o, nullptr, r->vals.data(), r->resid.data(), nullptr, &r->info);
+                std::vector<double> us(nu);
+                for (int i = 0; i < nu; ++i) us[i] = grp[i]->u;
+                rc = momed_batch_solve_impl(h, &o, us.data(), nu, gvals.data(), gres.data(), nullptr, &ginfo);
             }
             if (rc == MOMED_ENOTCONV) rc = MOMED_OK;   // results written; info.converged tells
+            for (int i = 0; i < nu; ++i) {
+                const int ni = (int)std::min<int64_t>(grp[i]->opts.nev, N);
+                grp[i]->vals.assign(gvals.begin() + (size_t)i * nev, gvals.begin() + (size_t)i * nev + ni);
+                grp[i]->resid.assign(gres.begin() + (size_t)i * nev, gres.begin() + (size_t)i * nev + ni);
+                grp[i]->info = ginfo;
+                grp[i]->info.converged = std::min<int32_t>(ginfo.converged, ni);
+            }
         } catch (const Error& e) {
             rc = e.code;
             err = e.msg;
@@ -166,12 +235,15 @@ void worker_loop(momed_server* S, int slot) {
         }
         {
             std::lock_guard<std::mutex> lk(S->mu);
-            r->done = clock_t_::now();
-            r->rc = rc;
-            r->err = err;
-            r->status = rc == MOMED_OK ? 2 : 3;
-            S->used -= r->bytes;
-            if (rc == MOMED_OK) ++S->completed; else ++S->failed;
+            const auto now = clock_t_::now();
+            for (auto& q : grp) {
+                q->done = now;
+                q->rc = rc;
+                q->err = err;
+                q->status = rc == MOMED_OK ? 2 : 3;
+                if (rc == MOMED_OK) ++S->completed; else ++S->failed;
+            }
+            S->used -= gbytes;
         }
         S->cv_done.notify_all();
         S->cv_work.notify_all();
@@ -234,6 +306,11 @@ MOMED_API int momed_serve_submit(momed_server* S, int32_t op_id, const uint64_t*
     r->u = u;
     r->opts = *opts;
     r->bytes = estimate_bytes(n, *opts);
+    uint64_t hsh = 0x9E3779B97F4A7C15ull ^ (uint64_t)n;
+    for (int64_t i = 0; i < n; ++i) {
+        hsh ^= basis[i] + 0x9E3779B97F4A7C15ull + (hsh << 6) + (hsh >> 2);
+    }
+    r->bhash = hsh;
     r->arrival = clock_t_::now();
     std::lock_guard<std::mutex> lk(S->mu);
     if (op_id < 0 || op_id >= (int32_t)S->ops.size()) {

@@ -164,3 +164,30 @@ def test_mixed_precision_requests(workload):
         assert np.max(np.abs(res[r][0] - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-10
     h.close()
     assert np.max(np.abs(v - alone) / np.abs(v)) < 1e-10
+
+
+def test_queued_requests_on_one_sector_are_batched(workload):
+    """Requests queued behind a running one that share its operator, sector and precision are
+    solved together (continuous batching): they finish as one group, each with its own u, and
+    every result matches the one-at-a-time FP64 solver within 1e-10."""
+    p35, p38, b35, b38 = workload
+    srv = _lib.Server(0, slots=1)
+    op35 = srv.register_operator(*p35)
+    op38 = srv.register_operator(*p38)
+    blocker = srv.submit(op38, b38[0], 1.0, 6, tol=1e-10)           # keeps the only slot busy
+    us = [0.6, 0.9, 1.2, 1.5]
+    rids = [srv.submit(op35, b35[2], u, 3, tol=1e-10, precision=_lib.PREC_MIXED) for u in us]
+    nev = {r: 3 for r in rids}
+    nev[blocker] = 6
+    res = wait_all(srv, [blocker] + rids, nev)
+    srv.stop()
+    infos = [res[r][2] for r in rids]
+    assert len({(i["matvecs"], i["seconds"]) for i in infos}) == 1      # one group, one solve
+    h = momed.Handle(0)
+    h.set_scatter_pair(*p35)
+    h.set_basis(b35[2])
+    for r, u in zip(rids, us):
+        h.set_param(u)
+        ref, _, _, _ = h.eigsolve(3, tol=1e-12, seed=1, want_vectors=False)
+        assert np.max(np.abs(res[r][0] - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-10
+    h.close()
