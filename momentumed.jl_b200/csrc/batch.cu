@@ -32,7 +32,8 @@ bool gen_herm_eig(int k, const std::vector<std::complex<double>>& G, const std::
 namespace {
 
 constexpr int kT = 256;
-constexpr int kRowsTile = 64;   // rows of W staged per tile in k_bproj
+constexpr int kTileElems = 2048;   // values of W (rows x right-hand sides) staged per tile in k_bproj
+template <int NB> constexpr int rows_tile() { return kTileElems / NB; }
 // Accepted eigenvalue error estimate (relative, r^2/gap) of the mixed-precision batch: 10x
 // below the 1e-10 target.
 constexpr double kEigTarget = 1e-11;
@@ -84,7 +85,8 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W
     constexpr int E = P::E;
     constexpr int PR = NB / E;                  // packets per row
     constexpr int RS = 32 / PR;                 // rows per warp pass
-    __shared__ double2 ws[kRowsTile * NB];
+    constexpr int TR = rows_tile<NB>();
+    __shared__ double2 ws[kTileElems];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int rp = lane % PR, rs = lane / PR;
     const int i = blockIdx.y * 8 + wid;
@@ -95,9 +97,9 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W
     int64_t per = (N + gridDim.x - 1) / gridDim.x;
     int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(N, r0 + per);
     const typename P::T* colbase = reinterpret_cast<const typename P::T*>(V + (int64_t)(i < ncols ? i : 0) * N * NB);
-    for (int64_t t0 = r0; t0 < r1; t0 += kRowsTile) {
-        const int rows = (int)((r1 - t0) < kRowsTile ? (r1 - t0) : kRowsTile);
-        for (int e = threadIdx.x; e < kRowsTile * NB; e += kT) {
+    for (int64_t t0 = r0; t0 < r1; t0 += TR) {
+        const int rows = (int)((r1 - t0) < TR ? (r1 - t0) : TR);
+        for (int e = threadIdx.x; e < kTileElems; e += kT) {
             int t = e / NB;
             ws[e] = (t < rows) ? to2(W[(t0 + t) * NB + (e % NB)]) : make_double2(0.0, 0.0);
         }
@@ -145,10 +147,10 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W
 
 // Row blocks of k_bproj for ncols columns: about 6 blocks per SM over all column groups, between
 // 1 and 4 per SM, never more than the row tiles; maxrb (the partial buffer's capacity) caps it.
-inline int bproj_rowblocks(int64_t N, int ncols, int sm, int maxrb) {
+inline int bproj_rowblocks(int64_t N, int ncols, int sm, int maxrb, int tile_rows) {
     const int groups = std::max(1, (ncols + 7) / 8);
     int rb = std::max(sm, std::min(4 * sm, 6 * sm / groups));
-    rb = (int)std::min<int64_t>(rb, (N + kRowsTile - 1) / kRowsTile);
+    rb = (int)std::min<int64_t>(rb, (N + tile_rows - 1) / tile_rows);
     return std::max(1, std::min(rb, maxrb));
 }
 inline dim3 bproj_grid(int rowblocks, int ncols) { return dim3(rowblocks, (unsigned)std::max(1, (ncols + 7) / 8)); }
@@ -427,7 +429,7 @@ struct BlockLanczos {
     int64_t launches = 0;
 
     BlockLanczos(momed_handle* hh, int mm, const std::vector<double>& u) : h(hh), N(hh->n), m(mm), st(hh->stream) {
-        grid = std::max(1, std::min<int>((int)((N + kRowsTile - 1) / kRowsTile), sms() * 4));   // max row blocks
+        grid = std::max(1, std::min<int>((int)((N + rows_tile<NB>() - 1) / rows_tile<NB>()), sms() * 4));   // max row blocks
         ugrid = std::max(1, std::min<int>((int)((N * NB + kT - 1) / kT), sms() * 8));
         V.resize((size_t)(m + 1) * N * NB);
         partial.resize((size_t)grid * (kMaxCols + 1) * NB);
@@ -450,7 +452,7 @@ struct BlockLanczos {
     VT* col(int i) { return V.p + (size_t)i * N * NB; }
 
     void proj(int ncols, const VT* w, double2* out, const int* act) {
-        const int rb = bproj_rowblocks(N, ncols, sms(), grid);
+        const int rb = bproj_rowblocks(N, ncols, sms(), grid, rows_tile<NB>());
         k_bproj<VT, VT, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(V.p, N, ncols, w, partial.p, act);
         k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(partial.p, rb, ncols + 1, out, act);
         launches += 2;
@@ -718,14 +720,16 @@ __global__ void k_bto(const double2* __restrict__ X, int64_t total, VT* __restri
         out[e] = fr2<VT>(X[e]);
 }
 
-// out[i][n][r] = sum_{a<kx} Y[i][a][r] X[a][n][r] + sum_{j<p} Y[i][kx+j][r] Q[j][n][r]
-// (Y complex, [(i * (kx + p) + a) * NB + r]; FP64 anchors X, FP32 extension Q; FP64 out)
+// out[i][n][r] = sum_{a<kx} Y[i][a][r] X[a][n][r] + sum_{b<kz} Y[i][kx+b][r] Z[b][n][r]
+//               + sum_{j<p} Y[i][kx+kz+j][r] Q[j][n][r]
+// (Y complex, [(i * (kx + kz + p) + a) * NB + r]; FP64 sources X and Z, FP32 source Q; FP64 out)
 template <int NB>
 __global__ void __launch_bounds__(kT)
-k_bcombine_xq(const double2* __restrict__ X, int kx, const float2* __restrict__ Q, int p, int64_t N,
-              const double2* __restrict__ Y, int nout, double2* __restrict__ out) {
+k_bcombine_xq(const double2* __restrict__ X, int kx, const double2* __restrict__ Z, int kz,
+              const float2* __restrict__ Q, int p, int64_t N, const double2* __restrict__ Y, int nout,
+              double2* __restrict__ out) {
     constexpr int OC = 8;
-    const int d = kx + p;
+    const int d = kx + kz + p;
     const int64_t total = N * NB;
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
         const int r = (int)(e % NB);
@@ -735,7 +739,9 @@ k_bcombine_xq(const double2* __restrict__ X, int kx, const float2* __restrict__ 
             for (int k = 0; k < OC; ++k) { ax[k] = 0.0; ay[k] = 0.0; }
 #pragma unroll 2
             for (int a = 0; a < d; ++a) {
-                const double2 v = a < kx ? X[(int64_t)a * total + e] : to2(Q[(int64_t)(a - kx) * total + e]);
+                const double2 v = a < kx        ? X[(int64_t)a * total + e]
+                                  : a < kx + kz ? Z[(int64_t)(a - kx) * total + e]
+                                                : to2(Q[(int64_t)(a - kx - kz) * total + e]);
 #pragma unroll
                 for (int k = 0; k < OC; ++k) {
                     if (c0 + k < nout) {
@@ -814,7 +820,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
     const int eg = std::max(1, std::min<int>((int)((stride + 255) / 256), sms() * 8));
     if (mixed) {
         // Gram matrices G_r = X_r^H W_r and S_r = X_r^H X_r, all r at once
-        const int grid = std::max(1, std::min<int>((int)((N + kRowsTile - 1) / kRowsTile), sms() * 2));
+        const int grid = std::max(1, std::min<int>((int)((N + rows_tile<NB>() - 1) / rows_tile<NB>()), sms() * 2));
         DevBuf<double2> part, red;
         part.resize((size_t)grid * (kMaxCols + 1) * NB);
         red.resize((size_t)(kMaxCols + 1) * NB);
@@ -935,15 +941,61 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
         };
         if (failing() > 0) {
             const int p = m - k1, d = k1 + p;
+            const int d2 = 2 * k1 + p + 1;     // sources of W': W, X, Q and the next Lanczos vector
             BlockLanczos<float2, NB> LR(h, m, uv);
             DevBuf<double> thd, wtd;
             thd.resize((size_t)NB * k1);
             wtd.resize((size_t)NB * k1);
-            DevBuf<double2> red, Yd;
+            DevBuf<double2> red, Yd, Y2d, W2;
             red.resize((size_t)(kMaxCols + 1) * NB);
             Yd.resize((size_t)k1 * d * NB);
+            Y2d.resize((size_t)k1 * d2 * NB);
+            W2.resize((size_t)k1 * stride);
             std::vector<int> failed(NB, 0);
+            std::vector<std::vector<double>> last_t(NB);   // full Ritz spectrum of the last cycle
+            const int rg = std::max(1, std::min<int>((int)((stride + 255) / 256), 512));
+            DevBuf<double> part;
+            part.resize((size_t)rg * k1 * NB);
+            // residual norms ||W_i - th_i X_i|| of every (i, q) into rs
+            auto residuals = [&]() {
+                std::vector<double> thn((size_t)NB * k1, 0.0);
+                for (int q = 0; q < nu; ++q)
+                    for (int i = 0; i < k1; ++i) thn[(size_t)q * k1 + i] = th[q][i];
+                MOMED_CUDA_TRY(cudaMemcpyAsync(thd.p, thn.data(), thn.size() * 8, cudaMemcpyHostToDevice, st));
+                k_bresid<NB><<<rg, 256, 0, st>>>(Wb.p, Xb.p, N, k1, thd.p, part.p);
+                note_launches(1);
+                MOMED_CUDA_TRY(cudaGetLastError());
+                std::vector<double> hp((size_t)rg * k1 * NB);
+                MOMED_CUDA_TRY(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 8, cudaMemcpyDeviceToHost, st));
+                MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+                for (int q = 0; q < nu; ++q)
+                    for (int i = 0; i < k1; ++i) {
+                        double s2 = 0.0;
+                        for (int b = 0; b < rg; ++b) s2 += hp[((size_t)b * k1 + i) * NB + q];
+                        rs[q][i] = std::sqrt(s2);
+                    }
+            };
+            // acceptance of parameter q from its Ritz spectrum t and rs; margin < 1 asks for more
+            auto accept = [&](int q, const std::vector<double>& t, double margin) {
+                int conv = 0;
+                bool ok = true;
+                for (int i = 0; i < nev; ++i) {
+                    double gap = 1e300;
+                    for (int j = 0; j < (int)t.size(); ++j)
+                        if (j != i && std::fabs(t[j] - t[i]) > 1e-9 * std::max(1.0, std::fabs(t[i])))
+                            gap = std::min(gap, std::fabs(t[j] - t[i]));
+                    const double est = rs[q][i] * rs[q][i] / std::max(gap, 1e-300);
+                    const bool good = rs[q][i] <= margin * tol ||
+                                      est <= margin * kEigTarget * std::max(1.0, std::fabs(t[i]));
+                    if (good && conv == i) ++conv;
+                    ok = ok && good;
+                }
+                convv[q] = conv;
+                okv[q] = ok ? 1 : 0;
+            };
+            int cycles = 0;
             for (int cyc = 0; cyc < kRefineCycles && failing() > 0; ++cyc) {
+                ++cycles;
                 // anchors and start vector (weighted residuals of the pairs not yet accepted)
                 k_bto<float2><<<eg, 256, 0, st>>>(Xb.p, (int64_t)k1 * stride, LR.col(0));
                 std::vector<double> thh((size_t)NB * k1, 0.0), wth((size_t)NB * k1, 0.0);
@@ -972,7 +1024,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                     S(NB, std::vector<std::complex<double>>((size_t)d * d));
                 std::vector<double2> hr((size_t)(kMaxCols + 1) * NB);
                 auto gram = [&](const void* cols, bool fp32, int ncols, const double2* rhs) {
-                    const int rb = bproj_rowblocks(N, ncols, sms(), LR.grid);
+                    const int rb = bproj_rowblocks(N, ncols, sms(), LR.grid, rows_tile<NB>());
                     if (fp32)
                         k_bproj<float2, double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
                             reinterpret_cast<const float2*>(cols), N, ncols, rhs, LR.partial.p, nullptr);
@@ -1004,6 +1056,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                     }
                 }
                 std::vector<double2> Yh((size_t)k1 * d * NB, make_double2(0.0, 0.0));
+                std::vector<double2> Y2h((size_t)k1 * d2 * NB, make_double2(0.0, 0.0));
                 std::vector<std::vector<double>> tq(NB);
                 std::vector<int> ok_rr(NB, 0);
                 {
@@ -1034,6 +1087,28 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                                     const auto y = Y[(size_t)i * d + a];
                                     Yh[((size_t)i * d + a) * NB + q] = make_double2(y.real(), y.imag());
                                 }
+                            // W' = H X' = W Y_X + X (C Y_Q) + Q (T Y_Q) + q_p beta_last (Y_Q)_last, with
+                            // C = X^H H Q exact (from W) and T the FP32 recurrence
+                            auto put2 = [&](int i, int a, std::complex<double> v) {
+                                Y2h[((size_t)i * d2 + a) * NB + q] = make_double2(v.real(), v.imag());
+                            };
+                            const double blast = hb[(size_t)q * m + m - 1];
+                            for (int i = 0; i < k1; ++i) {
+                                const std::complex<double>* yq = &Y[(size_t)i * d + k1];
+                                for (int a = 0; a < k1; ++a) put2(i, a, Y[(size_t)i * d + a]);
+                                for (int b = 0; b < k1; ++b) {
+                                    std::complex<double> c = 0.0;
+                                    for (int j = 0; j < p; ++j) c += G[q][(size_t)(k1 + j) * d + b] * yq[j];
+                                    put2(i, k1 + b, c);
+                                }
+                                for (int l = 0; l < p; ++l) {
+                                    std::complex<double> c = ha[(size_t)q * m + k1 + l] * yq[l];
+                                    if (l > 0) c += hb[(size_t)q * m + k1 + l - 1] * yq[l - 1];
+                                    if (l + 1 < p) c += hb[(size_t)q * m + k1 + l] * yq[l + 1];
+                                    put2(i, 2 * k1 + l, c);
+                                }
+                                put2(i, 2 * k1 + p, blast * yq[p - 1]);
+                            }
                             tq[q] = t;
                             ok_rr[q] = 1;
                         }));
@@ -1043,59 +1118,43 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                 for (int q = 0; q < NB; ++q) {
                     if (ok_rr[q]) continue;
                     if (q < nu && !okv[q]) failed[q] = 1;     // left to the FP64 block Lanczos
-                    for (int i = 0; i < k1; ++i) Yh[((size_t)i * d + i) * NB + q] = make_double2(1.0, 0.0);
+                    for (int i = 0; i < k1; ++i) {
+                        Yh[((size_t)i * d + i) * NB + q] = make_double2(1.0, 0.0);
+                        Y2h[((size_t)i * d2 + i) * NB + q] = make_double2(1.0, 0.0);
+                    }
                 }
                 MOMED_CUDA_TRY(cudaMemcpyAsync(Yd.p, Yh.data(), Yh.size() * sizeof(double2), cudaMemcpyHostToDevice, st));
-                k_bcombine_xq<NB><<<eg, kT, 0, st>>>(Xb.p, k1, LR.col(k1), p, N, Yd.p, k1, Sb.p);
-                note_launches(1);
+                MOMED_CUDA_TRY(cudaMemcpyAsync(Y2d.p, Y2h.data(), Y2h.size() * sizeof(double2), cudaMemcpyHostToDevice,
+                                               st));
+                // X' = [X Q] Y and W' from the Lanczos relation (both read the old X and W)
+                k_bcombine_xq<NB><<<eg, kT, 0, st>>>(Xb.p, k1, nullptr, 0, LR.col(k1), p, N, Yd.p, k1, Sb.p);
+                k_bcombine_xq<NB><<<eg, kT, 0, st>>>(Wb.p, k1, Xb.p, k1, LR.col(k1), p + 1, N, Y2d.p, k1, W2.p);
+                note_launches(2);
                 MOMED_CUDA_TRY(cudaGetLastError());
                 std::swap(Xb.p, Sb.p);
+                std::swap(Wb.p, W2.p);
+                for (int q = 0; q < nu; ++q)
+                    if (ok_rr[q]) {
+                        for (int i = 0; i < k1; ++i) th[q][i] = tq[q][i];
+                        last_t[q] = tq[q];
+                    }
+                // residuals from W' (accurate to the FP32 error times |y_Q|) and acceptance with
+                // a margin; the exact FP64 check follows the loop
+                residuals();
+                for (int q = 0; q < nu; ++q)
+                    if (!okv[q] && !broken[q] && ok_rr[q]) accept(q, tq[q], 0.5);
+                note_launches(LR.launches);
+                LR.launches = 0;
+            }
+            if (cycles > 0) {
+                // exact W = H X with the FP64 map, exact residuals, final acceptance
                 for (int i = 0; i < k1; ++i)
                     BlockMv<double2>::run(h, Xb.p + (size_t)i * stride, Wb.p + (size_t)i * stride, ud64.p, NB);
                 matvecs += (int64_t)k1 * nu;
                 matvecs64 += (int64_t)k1 * nu;
+                residuals();
                 for (int q = 0; q < nu; ++q)
-                    if (ok_rr[q])
-                        for (int i = 0; i < k1; ++i) th[q][i] = tq[q][i];
-                // exact FP64 residuals and acceptance
-                const int rg = std::max(1, std::min<int>((int)((stride + 255) / 256), 512));
-                DevBuf<double> part;
-                part.resize((size_t)rg * k1 * NB);
-                std::vector<double> thn((size_t)NB * k1, 0.0);
-                for (int q = 0; q < nu; ++q)
-                    for (int i = 0; i < k1; ++i) thn[(size_t)q * k1 + i] = th[q][i];
-                MOMED_CUDA_TRY(cudaMemcpyAsync(thd.p, thn.data(), thn.size() * 8, cudaMemcpyHostToDevice, st));
-                k_bresid<NB><<<rg, 256, 0, st>>>(Wb.p, Xb.p, N, k1, thd.p, part.p);
-                note_launches(1);
-                MOMED_CUDA_TRY(cudaGetLastError());
-                std::vector<double> hp((size_t)rg * k1 * NB);
-                MOMED_CUDA_TRY(cudaMemcpyAsync(hp.data(), part.p, hp.size() * 8, cudaMemcpyDeviceToHost, st));
-                MOMED_CUDA_TRY(cudaStreamSynchronize(st));
-                for (int q = 0; q < nu; ++q) {
-                    for (int i = 0; i < k1; ++i) {
-                        double s2 = 0.0;
-                        for (int b = 0; b < rg; ++b) s2 += hp[((size_t)b * k1 + i) * NB + q];
-                        rs[q][i] = std::sqrt(s2);
-                    }
-                    if (okv[q] || broken[q] || !ok_rr[q]) continue;
-                    const std::vector<double>& t = tq[q];
-                    int conv = 0;
-                    bool ok = true;
-                    for (int i = 0; i < nev; ++i) {
-                        double gap = 1e300;
-                        for (int j = 0; j < d; ++j)
-                            if (j != i && std::fabs(t[j] - t[i]) > 1e-9 * std::max(1.0, std::fabs(t[i])))
-                                gap = std::min(gap, std::fabs(t[j] - t[i]));
-                        const double est = rs[q][i] * rs[q][i] / std::max(gap, 1e-300);
-                        const bool good = rs[q][i] <= tol || est <= kEigTarget * std::max(1.0, std::fabs(t[i]));
-                        if (good && conv == i) ++conv;
-                        ok = ok && good;
-                    }
-                    convv[q] = conv;
-                    okv[q] = ok ? 1 : 0;
-                }
-                note_launches(LR.launches);
-                LR.launches = 0;
+                    if (!broken[q] && !last_t[q].empty()) accept(q, last_t[q], 1.0);
             }
         }
     }

@@ -75,9 +75,15 @@ struct momed_server {
     bool stopping = false;
     std::string last_error;
     int64_t completed = 0, failed = 0;
+    int large_running = 0;   // groups of at least kLargeRows states on the device
 };
 
 namespace {
+
+// A solve of at least this many states keeps the GPU (and its L2, which holds the map's input
+// vector and index tables) busy on its own; two at once only evict each other's working sets.
+// Such requests run one at a time; smaller ones still overlap with them and with each other.
+constexpr int64_t kLargeRows = 1 << 17;
 
 // HBM a solve needs: basis, index tables (bounded), Krylov basis, Ritz/refinement buffers.
 // nb: right-hand sides of a batched solve (a power of two), 0 for the single-vector solver.
@@ -137,15 +143,25 @@ void worker_loop(momed_server* S, int slot) {
         int64_t gbytes = 0;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            // FIFO admission: the head request starts when it fits the free budget
-            S->cv_work.wait(lk, [&] {
-                if (S->stopping) return true;
+            // admission in arrival order: the first queued request that fits the free budget and,
+            // if it is large, finds no other large group running (a request waiting for memory
+            // holds back the ones behind it)
+            std::deque<std::shared_ptr<Request>>::iterator pick;
+            auto find = [&]() {
                 while (!S->queue.empty() && S->queue.front()->status == 4) S->queue.pop_front();
-                return !S->queue.empty() && S->used + S->queue.front()->bytes <= S->budget;
-            });
+                for (auto it = S->queue.begin(); it != S->queue.end(); ++it) {
+                    if ((*it)->status == 4) continue;
+                    if ((int64_t)(*it)->basis.size() >= kLargeRows && S->large_running > 0) continue;
+                    if (S->used + (*it)->bytes > S->budget) return false;
+                    pick = it;
+                    return true;
+                }
+                return false;
+            };
+            S->cv_work.wait(lk, [&] { return S->stopping || find(); });
             if (S->stopping) return;
-            auto r = S->queue.front();
-            S->queue.pop_front();
+            auto r = *pick;
+            S->queue.erase(pick);
             grp.push_back(r);
             gbytes = r->bytes;
             if (r->op >= 0 && r->op < (int32_t)S->ops.size()) opp = S->ops[r->op];
@@ -170,6 +186,7 @@ void worker_loop(momed_server* S, int slot) {
                 it = S->queue.erase(it);
             }
             S->used += gbytes;
+            if (N >= kLargeRows) ++S->large_running;
             const auto now = clock_t_::now();
             for (auto& q : grp) {
                 q->status = 1;
@@ -244,6 +261,7 @@ void worker_loop(momed_server* S, int slot) {
                 if (rc == MOMED_OK) ++S->completed; else ++S->failed;
             }
             S->used -= gbytes;
+            if ((int64_t)r->basis.size() >= kLargeRows) --S->large_running;
         }
         S->cv_done.notify_all();
         S->cv_work.notify_all();

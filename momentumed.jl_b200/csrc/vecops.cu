@@ -45,7 +45,8 @@ __global__ void __launch_bounds__(kVecThreads)
 k_proj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ w, double2* partial,
        const int* active) {
     if (active && *active == 0) return;
-    __shared__ double2 ws[kVecThreads];
+    constexpr int TR = 2048;                     // rows of w staged per tile
+    __shared__ double2 ws[TR];
     __shared__ double red[kVecThreads / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int i = blockIdx.y * 8 + wid;
@@ -53,13 +54,16 @@ k_proj(const VT* __restrict__ V, int64_t N, int ncols, const VT* __restrict__ w,
     int64_t r0, r1;
     block_rows(N, r0, r1);
     const VT* colbase = V + (int64_t)(i < ncols ? i : 0) * N;
-    for (int64_t t0 = r0; t0 < r1; t0 += kVecThreads) {
-        int64_t n = t0 + threadIdx.x;
-        double2 wv = (n < r1) ? to_d2(w[n]) : make_double2(0.0, 0.0);
-        ws[threadIdx.x] = wv;
-        wn2 += wv.x * wv.x + wv.y * wv.y;
+    for (int64_t t0 = r0; t0 < r1; t0 += TR) {
+#pragma unroll
+        for (int e = threadIdx.x; e < TR; e += kVecThreads) {
+            int64_t n = t0 + e;
+            double2 wv = (n < r1) ? to_d2(w[n]) : make_double2(0.0, 0.0);
+            ws[e] = wv;
+            wn2 += wv.x * wv.x + wv.y * wv.y;
+        }
         __syncthreads();
-        const int rows = (int)((r1 - t0) < (int64_t)kVecThreads ? (r1 - t0) : (int64_t)kVecThreads);
+        const int rows = (int)((r1 - t0) < (int64_t)TR ? (r1 - t0) : (int64_t)TR);
         if (i < ncols) {
             const VT* col = colbase + t0;
 #pragma unroll 8
