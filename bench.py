@@ -306,7 +306,7 @@ def serve_bench(args, device: int):
                 time.sleep(r["arrival"] - now)
             ids.append(srv.submit(op_id[r["mesh"]], sectors[r["mesh"]][r["sector"]], r["u"], r["nev"], tol=r["tol"],
                                   krylovdim=serve_krylovdim(r["nev"]), maxiter=300, precision=_lib.PREC_MIXED))
-        vals, lat, conv, groups = [], [], [], set()
+        vals, lat, conv, groups = [], [], [], {}
         for rid, r in zip(ids, reqs):
             while True:
                 st, v, res, info, q, l = srv.poll(rid, r["nev"], wait_ms=1000)
@@ -315,12 +315,18 @@ def serve_bench(args, device: int):
             vals.append(v)
             lat.append(l)
             conv.append(info["converged"] >= r["nev"])
-            groups.add((r["mesh"], r["sector"], info["matvecs"], info["seconds"]))
+            g = groups.setdefault((r["mesh"], r["sector"], info["matvecs"], info["seconds"]), [])
+            g.append(r["nev"])
         span = time.perf_counter() - t0
         srv.stop()
-        return vals, lat, conv, span, len(groups)
+        return vals, lat, conv, span, groups
 
-    s_vals, s_lat, s_conv, s_span, n_solves = run_server()
+    s_vals, s_lat, s_conv, s_span, groups = run_server()
+    n_solves = len(groups)
+    slow = sorted(groups.items(), key=lambda kv: -kv[0][3])[:6]
+    gsizes = {}
+    for k, v in groups.items():
+        gsizes[len(v)] = gsizes.get(len(v), 0) + 1
     errs = [float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0))) for a, b in zip(s_vals, plain_vals)]
     n = len(reqs)
     sizes = {m: [len(x) for x in sectors[m]] for m in meshes}
@@ -330,7 +336,9 @@ def serve_bench(args, device: int):
         "meshes_states_per_sector": {m: [min(v), max(v)] for m, v in sizes.items()},
         "served": {"solves_per_s": n / s_span, "latency_ms_p50": 1e3 * pct(s_lat, 50),
                    "latency_ms_p99": 1e3 * pct(s_lat, 99), "slots": args.serve_slots,
-                   "device_solves": n_solves,
+                   "device_solves": n_solves, "group_sizes": {str(k): v for k, v in sorted(gsizes.items())},
+                   "slowest_solves": [{"mesh": k[0], "nev": v, "device_s": round(k[3], 3), "matvecs": k[2]}
+                                      for k, v in slow],
                    "precision": "mixed requests: batched mixed solver for groups on one sector, FP64 "
                                 "single-vector solver for a request alone",
                    "all_converged": bool(all(s_conv)), "max_rel_eig_err_vs_plain_fp64": max(errs)},

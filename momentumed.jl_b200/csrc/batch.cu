@@ -73,9 +73,10 @@ template <> struct Pack<float2, 32> : PackF2<32> {};
 
 // partial[b][i][r] (i <= ncols: column ncols holds |w_r|^2).  Grid: x = row blocks, y = groups
 // of 8 columns; warp w of group g owns column 8g + w over the block's rows, reading 16-byte
-// packets (lanes: NB / E packets per row, 32 E / NB rows at a time), so every lane keeps E
-// accumulators and the unrolled row loop keeps 8 loads of V in flight.  Warp 0 of group 0 also
-// sums |w|^2.
+// packets of V (lanes: NB / E packets per row, 32 E / NB rows at a time) and the matching values
+// of W straight from global memory (the block's 8 warps read the same rows of W, which L1
+// serves), so there is no shared-memory staging and no barrier; the unrolled row loop keeps 8
+// loads of V in flight per warp.  Warp 0 of group 0 also sums |w|^2.
 template <typename VT, typename WT, int NB>
 __global__ void __launch_bounds__(kT)
 k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W, double2* partial,
@@ -85,49 +86,39 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W
     constexpr int E = P::E;
     constexpr int PR = NB / E;                  // packets per row
     constexpr int RS = 32 / PR;                 // rows per warp pass
-    constexpr int TR = rows_tile<NB>();
-    __shared__ double2 ws[kTileElems];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int rp = lane % PR, rs = lane / PR;
     const int i = blockIdx.y * 8 + wid;
     const bool norm = blockIdx.y == 0 && wid == 0;
+    if (i >= ncols && !norm) return;            // warp-uniform: this warp has no column
     double ax[E], ay[E], wn2[E];
 #pragma unroll
     for (int q = 0; q < E; ++q) { ax[q] = 0.0; ay[q] = 0.0; wn2[q] = 0.0; }
     int64_t per = (N + gridDim.x - 1) / gridDim.x;
     int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(N, r0 + per);
-    const typename P::T* colbase = reinterpret_cast<const typename P::T*>(V + (int64_t)(i < ncols ? i : 0) * N * NB);
-    for (int64_t t0 = r0; t0 < r1; t0 += TR) {
-        const int rows = (int)((r1 - t0) < TR ? (r1 - t0) : TR);
-        for (int e = threadIdx.x; e < kTileElems; e += kT) {
-            int t = e / NB;
-            ws[e] = (t < rows) ? to2(W[(t0 + t) * NB + (e % NB)]) : make_double2(0.0, 0.0);
-        }
-        __syncthreads();
-        if (norm) {
-            for (int t = rs; t < rows; t += RS) {
-#pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    double2 v = ws[t * NB + rp * E + q];
-                    wn2[q] += v.x * v.x + v.y * v.y;
-                }
-            }
-        }
-        if (i < ncols) {
-            const typename P::T* col = colbase + t0 * PR;
+    const typename P::T* col = reinterpret_cast<const typename P::T*>(V + (int64_t)(i < ncols ? i : 0) * N * NB);
+    const WT* wr = W + rp * E;
+    if (i < ncols) {
 #pragma unroll 8
-            for (int t = rs; t < rows; t += RS) {
-                double2 v[E];
-                P::get(col[t * PR + rp], v);
+        for (int64_t t = r0 + rs; t < r1; t += RS) {
+            double2 v[E];
+            P::get(col[t * PR + rp], v);
 #pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    double2 w = ws[t * NB + rp * E + q];
-                    ax[q] += v[q].x * w.x + v[q].y * w.y;
-                    ay[q] += v[q].x * w.y - v[q].y * w.x;
-                }
+            for (int q = 0; q < E; ++q) {
+                const double2 w = to2(__ldg(wr + t * NB + q));
+                ax[q] += v[q].x * w.x + v[q].y * w.y;
+                ay[q] += v[q].x * w.y - v[q].y * w.x;
+                if (norm) wn2[q] += w.x * w.x + w.y * w.y;
             }
         }
-        __syncthreads();
+    } else {
+        for (int64_t t = r0 + rs; t < r1; t += RS) {
+#pragma unroll
+            for (int q = 0; q < E; ++q) {
+                const double2 w = to2(__ldg(wr + t * NB + q));
+                wn2[q] += w.x * w.x + w.y * w.y;
+            }
+        }
     }
     double2* out = partial + (int64_t)blockIdx.x * (kMaxCols + 1) * NB;
 #pragma unroll

@@ -15,6 +15,7 @@
 //
 // A solve is deterministic (seeded start vector, fixed reduction order), so a request's
 // result is the same alone and in any mix.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <condition_variable>
@@ -84,6 +85,10 @@ namespace {
 // vector and index tables) busy on its own; two at once only evict each other's working sets.
 // Such requests run one at a time; smaller ones still overlap with them and with each other.
 constexpr int64_t kLargeRows = 1 << 17;
+// Smallest group that the batched solver serves faster per request than the single-vector solver.
+constexpr int kMinGroup = 3;
+// Largest nev for which a group takes the mixed-precision batched solver.
+constexpr int kMaxMixedNev = 8;
 
 // HBM a solve needs: basis, index tables (bounded), Krylov basis, Ritz/refinement buffers.
 // nb: right-hand sides of a batched solve (a power of two), 0 for the single-vector solver.
@@ -165,25 +170,31 @@ void worker_loop(momed_server* S, int slot) {
             grp.push_back(r);
             gbytes = r->bytes;
             if (r->op >= 0 && r->op < (int32_t)S->ops.size()) opp = S->ops[r->op];
-            // continuous batching: queued requests on the same operator, sector and precision
+            // continuous batching: queued requests on the same operator, sector and precision join
+            // the head when the group reaches kMinGroup (smaller groups cost as much per solve as
+            // the single-vector solver)
             const int64_t N = (int64_t)r->basis.size();
-            for (auto it = S->queue.begin(); it != S->queue.end() && grp.size() < 32;) {
+            for (auto it = S->queue.begin(); it != S->queue.end() && grp.size() < 32; ++it) {
                 const auto& q = *it;
                 const bool same = q->status == 0 && q->op == r->op && q->opts.precision == r->opts.precision &&
                                   q->bhash == r->bhash && (int64_t)q->basis.size() == N &&
                                   std::memcmp(q->basis.data(), r->basis.data(), (size_t)N * 8) == 0;
-                if (!same) {
-                    ++it;
-                    continue;
-                }
+                if (!same) continue;
                 grp.push_back(q);
                 const int64_t need = estimate_bytes(N, group_opts(grp), pow2_at_least((int64_t)grp.size()));
                 if (S->used + need > S->budget) {
                     grp.pop_back();
                     break;
                 }
-                gbytes = need;
-                it = S->queue.erase(it);
+            }
+            if ((int)grp.size() >= kMinGroup) {
+                gbytes = estimate_bytes(N, group_opts(grp), pow2_at_least((int64_t)grp.size()));
+                auto taken = [&](const std::shared_ptr<Request>& q) {
+                    return std::find(grp.begin() + 1, grp.end(), q) != grp.end();
+                };
+                S->queue.erase(std::remove_if(S->queue.begin(), S->queue.end(), taken), S->queue.end());
+            } else {
+                grp.resize(1);
             }
             S->used += gbytes;
             if (N >= kLargeRows) ++S->large_running;
@@ -233,6 +244,9 @@ void worker_loop(momed_server* S, int slot) {
             } else {
                 std::vector<double> us(nu);
                 for (int i = 0; i < nu; ++i) us[i] = grp[i]->u;
+                // many eigenpairs per parameter: the FP64 block Lanczos converges in fewer steps
+                // than the mixed-precision refinement
+                if (o.nev > kMaxMixedNev) o.precision = MOMED_PREC_FP64;
                 rc = momed_batch_solve_impl(h, &o, us.data(), nu, gvals.data(), gres.data(), nullptr, &ginfo);
             }
             if (rc == MOMED_ENOTCONV) rc = MOMED_OK;   // results written; info.converged tells
