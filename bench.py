@@ -137,7 +137,14 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- distributed
-def dist_setup(args):
+_DIST_DEVICE = "cuda"
+
+
+def dist_setup(args, backend: str = "nccl"):
+    """One process per GPU (RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* from the launcher).  The
+    ranks only exchange timings and counts (replicas: no data-path collective); `backend`
+    "gloo" runs the same plumbing on CPU."""
+    global _DIST_DEVICE
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -146,10 +153,20 @@ def dist_setup(args):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+            _DIST_DEVICE = "cuda"
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            _DIST_DEVICE = "cpu"
     return rank, world, local
+
+
+def sector_order(rank: int, world: int, nsec: int, count: int):
+    """The sectors rank `rank` solves, in order: every world-th sector starting at rank, cycling."""
+    return [(rank + world * i) % nsec for i in range(count)]
 
 
 def all_max(x: float, world: int) -> float:
@@ -157,7 +174,7 @@ def all_max(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_DIST_DEVICE)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -167,7 +184,7 @@ def all_sum(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=_DIST_DEVICE)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
@@ -381,7 +398,7 @@ def run_plain_workload(args, rank, world, local):
     h.set_scatter_pair(*pair)
     h.set_param(1.0)
     W, K = max(args.warmup, 0), max(args.steps, 1)
-    order = [(rank + world * i) % len(sectors) for i in range(W + K)]
+    order = sector_order(rank, world, len(sectors), W + K)
 
     def solve(sidx, prec):
         h.select_sector(sidx, len(sectors[sidx][1]))
@@ -533,7 +550,7 @@ def main():
     nsec = len(sectors)
     h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
     W, K = max(args.warmup, 0), max(args.steps, 1)
-    order = [(rank + world * i) % nsec for i in range(W + K)]
+    order = sector_order(rank, world, nsec, W + K)
 
     def step_device(sidx):
         h.select_sector(sidx, len(sectors[sidx][1]))
