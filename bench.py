@@ -49,6 +49,9 @@ KRYLOV = 30
 # of `bench.py --profile-only` (dram__bytes_read.sum + dram__bytes_write.sum = 46.5 + 28.8 MB): the
 # x block and the term tables stay in L2, so the per-hit gathers of the algorithmic count hit L2.
 MV_DRAM_BYTES = 75.3e6
+METRIC = "batched solves/s, p50/p99 latency vs plain GPU Lanczos at <=1e-10 eig error"
+WORKLOAD = (f"3x9 mesh Ne=9, one sector (~174k states) x {NU} U0 in [0.5,2] per step, nev={NEV}, "
+            f"krylovdim={KRYLOV}, tol 1e-12")
 
 
 def parse():
@@ -236,12 +239,12 @@ def run_reference(args, rank, world):
             break
     value = len(times) / sum(times)
     line = {
-        "impl": "reference", "metric": "batched solves/s at <=1e-10 eigenvalue error", "value": value,
+        "impl": "reference", "metric": METRIC, "value": value,
         "unit": "solves/s", "n_gpus": 0, "steps": len(times), "warmup": 0,
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": f"3x9 mesh Ne=9 sectors (~174k states) x U0 in [0.5,2]; nev={NEV}; one "
-                               "(sector, U0) solve per step", "solver": "reference CPU map + FP64 Lanczos"},
+        "config": {"workload": WORKLOAD, "solver": "reference CPU map + FP64 Lanczos (oracle restatement), "
+                                                   "one (sector, U0) solve per step"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "port",
                          "sample": f"{len(times)} full (sector, U0) solves, {len(sectors[0][1])}-state sector"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -692,12 +695,11 @@ def main():
                 pass
         lat = sorted(step_ms)
         line = {
-            "metric": "batched solves/s, p50/p99 latency vs plain GPU Lanczos at <=1e-10 eig error",
+            "metric": METRIC,
             "value": value, "unit": "solves/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": elapsed_max * 1e3 / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64 matvec / f64 recurrences + f64 Rayleigh-Ritz", "data": "synthetic",
-            "config": {"workload": f"3x9 mesh Ne=9, one sector (~174k states) x {NU} U0 in [0.5,2] per step, "
-                                   f"nev={NEV}, krylovdim={KRYLOV}, tol 1e-12",
+            "config": {"workload": WORKLOAD,
                        "global_batch": NU * world, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (Krylov basis ~1.4 GB per step)"},
             "latency_ms": {"per_batch_p50": float(np.percentile(lat, 50)),
