@@ -49,33 +49,19 @@ __device__ __forceinline__ int64_t search_basis(const uint64_t* __restrict__ b, 
     return (__ldg(b + base) == v) ? base : -1;
 }
 
-template <bool LDG>
-__device__ __forceinline__ uint32_t table_load(const uint32_t* p) {
-    if (LDG) return __ldg(p);
-    return *p;
-}
-
-// base_hi / base_lo / binom are the caller's (shared-memory) copies of the tables; offh / rankl
-// are the two index tables, in global memory (LDG) or staged in shared memory by the caller.
-template <bool LDG>
-__device__ __forceinline__ int64_t lookup_index_tab(const IndexView& iv, uint64_t t, const uint32_t* base_hi,
-                                                    const uint32_t* base_lo, const uint32_t* binom,
-                                                    const uint32_t* offh, const uint32_t* rankl) {
+// base_hi / base_lo / binom are the caller's (shared-memory) copies of the tables
+__device__ __forceinline__ int64_t lookup_index(const IndexView& iv, uint64_t t, const uint32_t* base_hi,
+                                                const uint32_t* base_lo, const uint32_t* binom) {
     if (iv.mode == INDEX_SEARCH) return search_basis(iv.basis, iv.n, t);
     uint32_t sh = part_slot(t, iv.hi, base_hi, binom);
     uint32_t sl = part_slot(t, iv.lo, base_lo, binom);
-    if (iv.mode == INDEX_RANKED) return (int64_t)table_load<LDG>(offh + sh) + (int64_t)table_load<LDG>(rankl + sl);
+    if (iv.mode == INDEX_RANKED) return (int64_t)__ldg(iv.off_hi + sh) + (int64_t)__ldg(iv.rank_lo + sl);
     if (sh == kInvalid || sl == kInvalid || sh >= iv.hi.size || sl >= iv.lo.size) return -1;
-    uint32_t o = table_load<LDG>(offh + sh), r = table_load<LDG>(rankl + sl);
+    uint32_t o = __ldg(iv.off_hi + sh), r = __ldg(iv.rank_lo + sl);
     if (o == kInvalid || r == kInvalid) return -1;
     int64_t j = (int64_t)o + (int64_t)r;
     if (j >= iv.n || __ldg(iv.basis + j) != t) return -1;
     return j;
-}
-
-__device__ __forceinline__ int64_t lookup_index(const IndexView& iv, uint64_t t, const uint32_t* base_hi,
-                                                const uint32_t* base_lo, const uint32_t* binom) {
-    return lookup_index_tab<true>(iv, t, base_hi, base_lo, binom, iv.off_hi, iv.rank_lo);
 }
 
 }  // namespace momed

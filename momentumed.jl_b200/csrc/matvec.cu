@@ -161,11 +161,9 @@ __device__ __forceinline__ int stage_batch(int g, const OpView& ov, WarpScratch&
 }
 
 // Evaluate the term at flattened position f of the staged batch: returns j (or -1) and the sign.
-// offh / rankl: the index tables (global memory with LDG, or the caller's shared-memory copy).
-template <bool LDG>
-__device__ __forceinline__ int64_t eval_term_tab(int f, int& gi, uint64_t s, int64_t row, const OpView& ov,
-                                                 const IndexView& iv, const WarpScratch& ws, const SharedTables& sh,
-                                                 int& t, bool& neg, const uint32_t* offh, const uint32_t* rankl) {
+__device__ __forceinline__ int64_t eval_term(int f, int& gi, uint64_t s, int64_t row, const OpView& ov,
+                                             const IndexView& iv, const WarpScratch& ws, const SharedTables& sh,
+                                             int& t, bool& neg) {
     while (ws.pref[gi + 1] <= f) ++gi;
     t = ws.start[gi] + (f - ws.pref[gi]);
     uint64_t om = ws.out[gi];
@@ -175,29 +173,23 @@ __device__ __forceinline__ int64_t eval_term_tab(int f, int& gi, uint64_t s, int
     if ((mid & tin) != 0) return -1;
     if (tin == om) return row;                                    // diagonal term
     neg = (__popcll(mid & __ldg(ov.t_pm + t)) & 1) != 0;
-    return lookup_index_tab<LDG>(iv, mid | tin, sh.base_hi, sh.base_lo, sh.binom, offh, rankl);
+    return lookup_index(iv, mid | tin, sh.base_hi, sh.base_lo, sh.binom);
 }
 
-__device__ __forceinline__ int64_t eval_term(int f, int& gi, uint64_t s, int64_t row, const OpView& ov,
-                                             const IndexView& iv, const WarpScratch& ws, const SharedTables& sh,
-                                             int& t, bool& neg) {
-    return eval_term_tab<true>(f, gi, s, row, ov, iv, ws, sh, t, neg, iv.off_hi, iv.rank_lo);
-}
-
-// Rows of the single-vector map for one block of WARPS warps (TAB: the index tables are the
-// block's shared-memory copy at offh / rankl; otherwise they are read from global memory).
-template <typename R, bool HAS_B, int WARPS, bool TAB>
-__device__ __forceinline__ void matvec_rows(const IndexView& iv, const OpView& ov,
-                                            const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-                                            const R* __restrict__ u_ptr, int64_t rows, const SharedTables& sh,
-                                            WarpScratch* s_ws, const uint32_t* offh, const uint32_t* rankl) {
+template <typename R, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+         const R* __restrict__ u_ptr, int64_t rows) {
     using C2 = typename Cx<R>::T;
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    stage_tables(sh, iv);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     WarpScratch& ws = s_ws[wid];
     const R u = HAS_B ? *u_ptr : R(0);
     const C2* __restrict__ A = amp_a<R>(ov);
     const C2* __restrict__ B = amp_b<R>(ov);
-    for (int64_t row = (int64_t)blockIdx.x * WARPS + wid; row < rows; row += (int64_t)gridDim.x * WARPS) {
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
         const uint64_t s = __ldg(iv.basis + row);
         R ar = 0, ai = 0;
         for_each_group_batch(s, ov, [&](int g) {
@@ -208,7 +200,7 @@ __device__ __forceinline__ void matvec_rows(const IndexView& iv, const OpView& o
                 if (f < total) {
                     int t;
                     bool neg;
-                    int64_t j = eval_term_tab<!TAB>(f, gi, s, row, ov, iv, ws, sh, t, neg, offh, rankl);
+                    int64_t j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
                     if (j >= 0) {
                         C2 a = load_amp(A, t);
                         if (HAS_B) {
@@ -237,35 +229,6 @@ __device__ __forceinline__ void matvec_rows(const IndexView& iv, const OpView& o
             y[row] = out;
         }
     }
-}
-
-template <typename R, bool HAS_B>
-__global__ void __launch_bounds__(kWarps * 32)
-k_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-         const R* __restrict__ u_ptr, int64_t rows) {
-    __shared__ SharedTables sh;
-    __shared__ WarpScratch s_ws[kWarps];
-    stage_tables(sh, iv);
-    matvec_rows<R, HAS_B, kWarps, false>(iv, ov, x, y, u_ptr, rows, sh, s_ws, iv.off_hi, iv.rank_lo);
-}
-
-// The same map with both index tables copied into shared memory once per block (when they fit,
-// kTabEntries): every hit's two table reads become shared-memory reads instead of random L1
-// gathers.  1024-thread blocks, two per SM, keep as many warps resident as k_matvec.
-constexpr int kTabWarps = 32;
-constexpr int kTabEntries = 23 * 1024;
-template <typename R, bool HAS_B>
-__global__ void __launch_bounds__(kTabWarps * 32, 2)
-k_matvec_st(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-            const R* __restrict__ u_ptr, int64_t rows) {
-    extern __shared__ uint32_t s_tab[];          // [hi.size] off_hi, then [lo.size] rank_lo
-    __shared__ SharedTables sh;
-    __shared__ WarpScratch s_ws[kTabWarps];
-    const uint32_t nh = iv.hi.size, nl = iv.lo.size;
-    for (uint32_t i = threadIdx.x; i < nh; i += blockDim.x) s_tab[i] = __ldg(iv.off_hi + i);
-    for (uint32_t i = threadIdx.x; i < nl; i += blockDim.x) s_tab[nh + i] = __ldg(iv.rank_lo + i);
-    stage_tables(sh, iv);                        // ends with __syncthreads
-    matvec_rows<R, HAS_B, kTabWarps, true>(iv, ov, x, y, u_ptr, rows, sh, s_ws, s_tab, s_tab + nh);
 }
 
 // Counts hits (targets found) and misses (targets outside the basis) without touching x.
@@ -613,49 +576,15 @@ int persistent_grid(K kernel, int64_t rows) {
 
 }  // namespace
 
-// Launches k_matvec_st when the index tables fit in shared memory; false otherwise.
-template <typename R>
-static bool launch_tab_matvec(const IndexView& iv, const OpView& ov, const typename Cx<R>::T* x,
-                              typename Cx<R>::T* y, const R* u, bool hb, int64_t rows, cudaStream_t st) {
-    if (iv.mode == INDEX_SEARCH) return false;
-    const size_t entries = (size_t)iv.hi.size + (size_t)iv.lo.size;
-    if (entries == 0 || entries > (size_t)kTabEntries) return false;
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    const int64_t need = (rows + kTabWarps - 1) / kTabWarps;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * 2));
-    const size_t smem = entries * sizeof(uint32_t);
-    // process-wide kernel attribute: always the largest size, so concurrent callers never lower it
-    const int smem_max = kTabEntries * (int)sizeof(uint32_t);
-    if (hb) {
-        auto k = k_matvec_st<R, true>;
-        MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
-        k<<<grid, kTabWarps * 32, smem, st>>>(iv, ov, x, y, u, rows);
-    } else {
-        auto k = k_matvec_st<R, false>;
-        MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
-        k<<<grid, kTabWarps * 32, smem, st>>>(iv, ov, x, y, nullptr, rows);
-    }
-    return true;
-}
-
 void launch_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y, const double* u_scale,
                         int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
-    const bool hb = u_scale && ov.t_ampb;
-    if (!launch_tab_matvec<double>(iv, ov, x, y, hb ? u_scale : nullptr, hb, rows, st)) {
-        if (hb) {
-            auto k = k_matvec<double, true>;
-            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u_scale, rows);
-        } else {
-            auto k = k_matvec<double, false>;
-            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
-        }
+    if (u_scale && ov.t_ampb) {
+        auto k = k_matvec<double, true>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u_scale, rows);
+    } else {
+        auto k = k_matvec<double, false>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
     }
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
@@ -664,15 +593,12 @@ void launch_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x,
 void launch_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y, const float* u_scale,
                        int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
-    const bool hb = u_scale && ov.t_ampb32;
-    if (!launch_tab_matvec<float>(iv, ov, x, y, hb ? u_scale : nullptr, hb, rows, st)) {
-        if (hb) {
-            auto k = k_matvec<float, true>;
-            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u_scale, rows);
-        } else {
-            auto k = k_matvec<float, false>;
-            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
-        }
+    if (u_scale && ov.t_ampb32) {
+        auto k = k_matvec<float, true>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u_scale, rows);
+    } else {
+        auto k = k_matvec<float, false>;
+        k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
     }
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
