@@ -50,7 +50,10 @@ KRYLOV = 30
 # x block and the term tables stay in L2, so the per-hit gathers of the algorithmic count hit L2.
 MV_DRAM_BYTES = 75.3e6
 METRIC = "batched solves/s, p50/p99 latency vs plain GPU Lanczos at <=1e-10 eig error"
-WORKLOAD = (f"3x9 mesh Ne=9, one sector (~174k states) x {NU} U0 in [0.5,2] per step, nev={NEV}, "
+
+
+def workload_name() -> str:
+    return (f"3x9 mesh Ne=9, one sector (~174k states) x {NU} U0 in [0.5,2] per step, nev={NEV}, "
             f"krylovdim={KRYLOV}, tol 1e-12")
 
 
@@ -62,6 +65,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--plain", type=int, default=4, help="U0 values solved one at a time for the plain comparison")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    ap.add_argument("--krylovdim", type=int, default=0, help="Krylov dimension of the batched solver (default 30)")
     ap.add_argument("--profile-only", action="store_true", help="one short run for ncu (no timing output)")
     ap.add_argument("--workload", default="batch_3x9",
                     choices=["batch_3x9", "plain_3x5", "plain_3x10", "two_comp_4x6"],
@@ -243,7 +247,7 @@ def run_reference(args, rank, world):
         "unit": "solves/s", "n_gpus": 0, "steps": len(times), "warmup": 0,
         "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "solver": "reference CPU map + FP64 Lanczos (oracle restatement), "
+        "config": {"workload": workload_name(), "solver": "reference CPU map + FP64 Lanczos (oracle restatement), "
                                                    "one (sector, U0) solve per step"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "port",
                          "sample": f"{len(times)} full (sector, U0) solves, {len(sectors[0][1])}-state sector"},
@@ -524,7 +528,10 @@ def block_bytes(N: int, nnz: int, nscat: int, nb: int, s: int) -> float:
 
 
 def main():
+    global KRYLOV
     args = parse()
+    if args.krylovdim > 0:
+        KRYLOV = args.krylovdim
     rank, world, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -699,7 +706,7 @@ def main():
             "value": value, "unit": "solves/s", "n_gpus": world, "steps": K, "warmup": W,
             "ms_per_step": elapsed_max * 1e3 / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64 matvec / f64 recurrences + f64 Rayleigh-Ritz", "data": "synthetic",
-            "config": {"workload": WORKLOAD,
+            "config": {"workload": workload_name(),
                        "global_batch": NU * world, "parallelism": f"replicas x{world}",
                        "l2": "inputs larger than L2 (Krylov basis ~1.4 GB per step)"},
             "latency_ms": {"per_batch_p50": float(np.percentile(lat, 50)),

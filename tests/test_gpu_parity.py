@@ -193,6 +193,42 @@ def test_matvec_3x10_sector_properties(h):
     assert st["index_mode"] == 0 and st["nnz"] > 300 * len(basis)
 
 
+def sector_count(a, b, ne, K):
+    """States of ne electrons on the a x b mesh with total momentum K (mod (a, b)), by a DP over
+    orbitals (no enumeration)."""
+    dp = np.zeros((ne + 1, a, b), np.int64)
+    dp[0, 0, 0] = 1
+    for i in range(a * b):
+        kx, ky = i % a, i // a
+        dp[1:] = dp[1:] + np.roll(np.roll(dp[:-1], kx, axis=1), ky, axis=2)
+    return int(dp[ne, K[0] % a, K[1] % b])
+
+
+def test_matvec_4x9_ne12_largest_sector(h):
+    """The largest configured size: a 4x9 Ne=12 sector (~34.8M states, 36-bit states, from a
+    1.25G-rank enumeration).  Size against a DP count, sorted and unique, momentum of sampled
+    states, Hermiticity and sampled rows of the c128 map against the oracle."""
+    para, op, full, ofull = operator_lists(4, 9, 4)
+    got = h.enumerate_basis(O.mesh_klist(4, 9), (4, 9), 1, 1, (12,), momentum_list=[(1, 2)])
+    k, basis = got[0]
+    assert tuple(k) == (1, 2)
+    assert len(basis) == sector_count(4, 9, 12, (1, 2)) > 34_000_000
+    assert np.all(basis[1:] > basis[:-1])
+    rng = np.random.default_rng(11)
+    for st in basis[rng.choice(len(basis), 2000, replace=False)]:
+        occ = [i for i in range(36) if (int(st) >> i) & 1]
+        assert len(occ) == 12
+        assert (sum(i % 4 for i in occ) % 4, sum(i // 4 for i in occ) % 9) == (1, 2)
+    load(h, basis, full)
+    x = rng.normal(size=len(basis)) + 1j * rng.normal(size=len(basis))
+    z = rng.normal(size=len(basis)) + 1j * rng.normal(size=len(basis))
+    hx, hz = h.matvec(x), h.matvec(z)
+    assert abs(np.vdot(z, hx) - np.vdot(hz, x)) < 1e-10 * abs(np.vdot(z, hx))
+    rows = rng.choice(len(basis), 2000, replace=False)
+    assert rel(hx[rows], O.matvec_rows(basis, ofull, x, rows)) < 1e-13
+    assert h.stats()["nnz"] > 500 * len(basis)
+
+
 # ------------------------------------------------------------------------------ Lanczos
 def check_eigs(vals, vecs, H, tol_rel=1e-10, overlap_tol=1e-9):
     w, U = np.linalg.eigh(H)
