@@ -33,7 +33,7 @@ namespace {
 
 constexpr int kT = 256;
 constexpr int kTileElems = 2048;   // values of W (rows x right-hand sides) staged per tile in k_bproj
-template <int NB> constexpr int rows_tile() { return kTileElems / NB; }
+template <int NB> __host__ __device__ constexpr int rows_tile() { return kTileElems / NB; }
 // Accepted eigenvalue error estimate (relative, r^2/gap) of the mixed-precision batch: 10x
 // below the 1e-10 target.
 constexpr double kEigTarget = 1e-11;
@@ -230,6 +230,121 @@ k_bupdate(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restr
     for (int q = 0; q < E; ++q) atomicAdd(&nrm[r0 + q], wn2[q]);
     __syncthreads();
     if (threadIdx.x < NB) npartial[(int64_t)blockIdx.x * NB + threadIdx.x] = nrm[threadIdx.x];
+}
+
+// Fused first update and second projection of a Lanczos step (up to kFuseCols columns):
+//   w' = w - V c (stored, rounded to VT), npartial[b][r] = block's |w'_r|^2,
+//   partial[b][i][r] = block's sum of conj(V_i) w'  (i < ncols; column ncols holds |w'|^2).
+// A block walks its rows in tiles: the threads update a tile (one 16-byte packet of W each, as in
+// k_bupdate) and keep w' in shared memory; then warp w projects columns w, w + 8, ... over the
+// tile (as in k_bproj), re-reading V from L2 instead of making another pass over HBM.
+constexpr int kFuseCols = 32;
+template <typename VT, int NB>
+__global__ void __launch_bounds__(kT)
+k_bupdproj(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restrict__ coef, VT* __restrict__ W,
+           double2* partial, double* npartial) {
+    using P = Pack<VT, NB>;
+    using PT = typename P::T;
+    constexpr int E = P::E;
+    constexpr int PR = NB / E;                  // packets per row
+    constexpr int RS = 32 / PR;                 // rows per warp pass (projection)
+    constexpr int TE = 16384 / (int)sizeof(VT);  // values of w' per tile (16 KB, kept in VT)
+    constexpr int TR = TE / NB;                 // rows per tile
+    constexpr int MAXC = kFuseCols / 8;         // columns per warp
+    __shared__ double2 c[kFuseCols * NB];
+    __shared__ VT wt[TE];
+    __shared__ double nrm[32];
+    for (int e = threadIdx.x; e < ncols * NB; e += kT) c[e] = coef[e];
+    if (threadIdx.x < 32) nrm[threadIdx.x] = 0.0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int rp = lane % PR, rs = lane / PR;
+    const int pr0 = (threadIdx.x % PR) * E;     // right-hand sides of this thread's packets (phase A)
+    const int64_t total = N * NB / E;
+    const PT* Vp = reinterpret_cast<const PT*>(V);
+    PT* Wp = reinterpret_cast<PT*>(W);
+    double wn2[E];
+    double ax[MAXC][E], ay[MAXC][E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) wn2[q] = 0.0;
+#pragma unroll
+    for (int k = 0; k < MAXC; ++k)
+#pragma unroll
+        for (int q = 0; q < E; ++q) { ax[k][q] = 0.0; ay[k][q] = 0.0; }
+    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(N, r0 + per);
+    for (int64_t t0 = r0; t0 < r1; t0 += TR) {
+        const int rows = (int)((r1 - t0) < TR ? (r1 - t0) : TR);
+        // phase A: w' = w - V c for the tile
+        for (int pk = threadIdx.x; pk < rows * PR; pk += kT) {
+            const int64_t e = t0 * PR + pk;
+            double2 acc[E];
+            P::get(Wp[e], acc);
+#pragma unroll 8
+            for (int i = 0; i < ncols; ++i) {
+                double2 v[E];
+                P::get(Vp[(int64_t)i * total + e], v);
+#pragma unroll
+                for (int q = 0; q < E; ++q) {
+                    const double2 cf = c[i * NB + pr0 + q];
+                    acc[q].x -= cf.x * v[q].x - cf.y * v[q].y;
+                    acc[q].y -= cf.x * v[q].y + cf.y * v[q].x;
+                }
+            }
+            const PT st = P::put(acc);
+            Wp[e] = st;
+            P::get(st, acc);
+            const int t = pk / PR;
+#pragma unroll
+            for (int q = 0; q < E; ++q) {
+                wn2[q] += acc[q].x * acc[q].x + acc[q].y * acc[q].y;
+                wt[t * NB + pr0 + q] = fr2<VT>(acc[q]);
+            }
+        }
+        __syncthreads();
+        // phase B: warp wid projects columns wid, wid + 8, ... over the tile
+#pragma unroll
+        for (int k = 0; k < MAXC; ++k) {
+            const int i = wid + 8 * k;
+            if (i < ncols) {
+                const PT* col = Vp + (int64_t)i * total + t0 * PR;
+#pragma unroll 4
+                for (int t = rs; t < rows; t += RS) {
+                    double2 v[E];
+                    P::get(col[t * PR + rp], v);
+#pragma unroll
+                    for (int q = 0; q < E; ++q) {
+                        const double2 w = to2(wt[t * NB + rp * E + q]);
+                        ax[k][q] += v[q].x * w.x + v[q].y * w.y;
+                        ay[k][q] += v[q].x * w.y - v[q].y * w.x;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < E; ++q) atomicAdd(&nrm[pr0 + q], wn2[q]);
+    double2* out = partial + (int64_t)blockIdx.x * (kMaxCols + 1) * NB;
+#pragma unroll
+    for (int k = 0; k < MAXC; ++k) {
+        const int i = wid + 8 * k;
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            double sx = ax[k][q], sy = ay[k][q];
+#pragma unroll
+            for (int o = PR; o < 32; o <<= 1) {
+                sx += __shfl_xor_sync(0xffffffffu, sx, o);
+                sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            }
+            if (i < ncols && rs == 0) out[i * NB + rp * E + q] = make_double2(sx, sy);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < NB) {
+        npartial[(int64_t)blockIdx.x * NB + threadIdx.x] = nrm[threadIdx.x];
+        out[ncols * NB + threadIdx.x] = make_double2(nrm[threadIdx.x], 0.0);
+    }
 }
 
 // launched with NB warps: warp r reduces the norm partials of right-hand side r
@@ -478,14 +593,25 @@ struct BlockLanczos {
         BlockMv<VT>::run(h, col(j), w, ud.p, NB);   // counted by its launcher
         const int nc = j + 1;
         proj(nc, w, coefA.p, nullptr);
-        update(nc, coefA.p, w, nullptr, nullptr);
-        k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p);
-        proj(nc, w, coefB.p, any.p);
+        if (nc <= kFuseCols) {
+            // first update fused with the second projection (computed for every right-hand side,
+            // used where the DGKS test asks for the second pass)
+            const int fg = std::min(grid, ugrid);
+            k_bupdproj<VT, NB><<<fg, kT, 0, st>>>(V.p, N, nc, coefA.p, w, partial.p, npart.p);
+            k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, fg, flag.p, any.p, after.p);
+            k_breduce<NB><<<breduce_grid(nc + 1, NB), 256, 0, st>>>(partial.p, fg, nc + 1, coefB.p, nullptr);
+            launches += 3;
+        } else {
+            update(nc, coefA.p, w, nullptr, nullptr);
+            k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p);
+            proj(nc, w, coefB.p, any.p);
+            ++launches;
+        }
         update(nc, coefB.p, w, flag.p, any.p);
         k_bfinalize<NB><<<1, NB * 32, 0, st>>>(coefA.p, coefB.p, nc, npart.p, ugrid, flag.p, any.p, after.p, scal.p,
                                           alpha.p, beta.p, j, m);
         k_bscale<VT, NB><<<ugrid, kT, 0, st>>>(w, N, scal.p);
-        launches += 3;
+        launches += 2;
     }
     template <typename VOUT>
     void combine(const std::vector<double>& Uh, int nout, VOUT* out, int copy_col, int mm) {
@@ -713,41 +839,61 @@ __global__ void k_bto(const double2* __restrict__ X, int64_t total, VT* __restri
 
 // out[i][n][r] = sum_{a<kx} Y[i][a][r] X[a][n][r] + sum_{b<kz} Y[i][kx+b][r] Z[b][n][r]
 //               + sum_{j<p} Y[i][kx+kz+j][r] Q[j][n][r]
-// (Y complex, [(i * (kx + kz + p) + a) * NB + r]; FP64 sources X and Z, FP32 source Q; FP64 out)
+// (Y complex, [(i * (kx + kz + p) + a) * NB + r]; FP64 sources X and Z, FP32 source Q; FP64 out).
+// A thread owns RPT rows of one right-hand side, so each coefficient load serves RPT rows.
 template <int NB>
-__global__ void __launch_bounds__(kT)
+__global__ void __launch_bounds__(kT, 2)
 k_bcombine_xq(const double2* __restrict__ X, int kx, const double2* __restrict__ Z, int kz,
               const float2* __restrict__ Q, int p, int64_t N, const double2* __restrict__ Y, int nout,
               double2* __restrict__ out) {
-    constexpr int OC = 8;
+    constexpr int OC = 8, RPT = 2;
+    constexpr int TPR = kT / NB;        // row slots per block pass
     const int d = kx + kz + p;
-    const int64_t total = N * NB;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-        const int r = (int)(e % NB);
+    const int64_t stride = N * NB;
+    const int r = threadIdx.x % NB, slot = threadIdx.x / NB;
+    for (int64_t t0 = (int64_t)blockIdx.x * TPR * RPT; t0 < N; t0 += (int64_t)gridDim.x * TPR * RPT) {
+        int64_t off[RPT];
+        bool ok[RPT];
+#pragma unroll
+        for (int j = 0; j < RPT; ++j) {
+            const int64_t row = t0 + slot + (int64_t)j * TPR;
+            ok[j] = row < N;
+            off[j] = (ok[j] ? row : 0) * NB + r;
+        }
         for (int c0 = 0; c0 < nout; c0 += OC) {
-            double ax[OC], ay[OC];
+            double ax[RPT][OC], ay[RPT][OC];
 #pragma unroll
-            for (int k = 0; k < OC; ++k) { ax[k] = 0.0; ay[k] = 0.0; }
-#pragma unroll 2
+            for (int j = 0; j < RPT; ++j)
+#pragma unroll
+                for (int k = 0; k < OC; ++k) { ax[j][k] = 0.0; ay[j][k] = 0.0; }
             for (int a = 0; a < d; ++a) {
-                const double2 v = a < kx        ? X[(int64_t)a * total + e]
-                                  : a < kx + kz ? Z[(int64_t)(a - kx) * total + e]
-                                                : to2(Q[(int64_t)(a - kx - kz) * total + e]);
+                double2 y[OC];
 #pragma unroll
-                for (int k = 0; k < OC; ++k) {
-                    if (c0 + k < nout) {
-                        const double2 y = __ldg(Y + ((int64_t)(c0 + k) * d + a) * NB + r);
-                        ax[k] += y.x * v.x - y.y * v.y;
-                        ay[k] += y.x * v.y + y.y * v.x;
+                for (int k = 0; k < OC; ++k)
+                    y[k] = (c0 + k < nout) ? __ldg(Y + ((int64_t)(c0 + k) * d + a) * NB + r) : make_double2(0.0, 0.0);
+#pragma unroll
+                for (int j = 0; j < RPT; ++j) {
+                    const double2 v = a < kx        ? X[(int64_t)a * stride + off[j]]
+                                      : a < kx + kz ? Z[(int64_t)(a - kx) * stride + off[j]]
+                                                    : to2(Q[(int64_t)(a - kx - kz) * stride + off[j]]);
+#pragma unroll
+                    for (int k = 0; k < OC; ++k) {
+                        ax[j][k] += y[k].x * v.x - y[k].y * v.y;
+                        ay[j][k] += y[k].x * v.y + y[k].y * v.x;
                     }
                 }
             }
 #pragma unroll
-            for (int k = 0; k < OC; ++k)
-                if (c0 + k < nout) out[(int64_t)(c0 + k) * total + e] = make_double2(ax[k], ay[k]);
+            for (int j = 0; j < RPT; ++j) {
+                if (!ok[j]) continue;
+#pragma unroll
+                for (int k = 0; k < OC; ++k)
+                    if (c0 + k < nout) out[(int64_t)(c0 + k) * stride + off[j]] = make_double2(ax[j][k], ay[j][k]);
+            }
         }
     }
 }
+
 
 template <int NB>
 int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32_t nu, double* vals, double* resid,
@@ -1118,8 +1264,9 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                 MOMED_CUDA_TRY(cudaMemcpyAsync(Y2d.p, Y2h.data(), Y2h.size() * sizeof(double2), cudaMemcpyHostToDevice,
                                                st));
                 // X' = [X Q] Y and W' from the Lanczos relation (both read the old X and W)
-                k_bcombine_xq<NB><<<eg, kT, 0, st>>>(Xb.p, k1, nullptr, 0, LR.col(k1), p, N, Yd.p, k1, Sb.p);
-                k_bcombine_xq<NB><<<eg, kT, 0, st>>>(Wb.p, k1, Xb.p, k1, LR.col(k1), p + 1, N, Y2d.p, k1, W2.p);
+                const int xg = std::max(1, std::min<int>((int)((N + 2 * (kT / NB) - 1) / (2 * (kT / NB))), sms() * 8));
+                k_bcombine_xq<NB><<<xg, kT, 0, st>>>(Xb.p, k1, nullptr, 0, LR.col(k1), p, N, Yd.p, k1, Sb.p);
+                k_bcombine_xq<NB><<<xg, kT, 0, st>>>(Wb.p, k1, Xb.p, k1, LR.col(k1), p + 1, N, Y2d.p, k1, W2.p);
                 note_launches(2);
                 MOMED_CUDA_TRY(cudaGetLastError());
                 std::swap(Xb.p, Sb.p);
