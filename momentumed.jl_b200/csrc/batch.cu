@@ -232,121 +232,6 @@ k_bupdate(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restr
     if (threadIdx.x < NB) npartial[(int64_t)blockIdx.x * NB + threadIdx.x] = nrm[threadIdx.x];
 }
 
-// Fused first update and second projection of a Lanczos step (up to kFuseCols columns):
-//   w' = w - V c (stored, rounded to VT), npartial[b][r] = block's |w'_r|^2,
-//   partial[b][i][r] = block's sum of conj(V_i) w'  (i < ncols; column ncols holds |w'|^2).
-// A block walks its rows in tiles: the threads update a tile (one 16-byte packet of W each, as in
-// k_bupdate) and keep w' in shared memory; then warp w projects columns w, w + 8, ... over the
-// tile (as in k_bproj), re-reading V from L2 instead of making another pass over HBM.
-constexpr int kFuseCols = 32;
-template <typename VT, int NB>
-__global__ void __launch_bounds__(kT)
-k_bupdproj(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restrict__ coef, VT* __restrict__ W,
-           double2* partial, double* npartial) {
-    using P = Pack<VT, NB>;
-    using PT = typename P::T;
-    constexpr int E = P::E;
-    constexpr int PR = NB / E;                  // packets per row
-    constexpr int RS = 32 / PR;                 // rows per warp pass (projection)
-    constexpr int TE = 16384 / (int)sizeof(VT);  // values of w' per tile (16 KB, kept in VT)
-    constexpr int TR = TE / NB;                 // rows per tile
-    constexpr int MAXC = kFuseCols / 8;         // columns per warp
-    __shared__ double2 c[kFuseCols * NB];
-    __shared__ VT wt[TE];
-    __shared__ double nrm[32];
-    for (int e = threadIdx.x; e < ncols * NB; e += kT) c[e] = coef[e];
-    if (threadIdx.x < 32) nrm[threadIdx.x] = 0.0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int rp = lane % PR, rs = lane / PR;
-    const int pr0 = (threadIdx.x % PR) * E;     // right-hand sides of this thread's packets (phase A)
-    const int64_t total = N * NB / E;
-    const PT* Vp = reinterpret_cast<const PT*>(V);
-    PT* Wp = reinterpret_cast<PT*>(W);
-    double wn2[E];
-    double ax[MAXC][E], ay[MAXC][E];
-#pragma unroll
-    for (int q = 0; q < E; ++q) wn2[q] = 0.0;
-#pragma unroll
-    for (int k = 0; k < MAXC; ++k)
-#pragma unroll
-        for (int q = 0; q < E; ++q) { ax[k][q] = 0.0; ay[k][q] = 0.0; }
-    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
-    const int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(N, r0 + per);
-    for (int64_t t0 = r0; t0 < r1; t0 += TR) {
-        const int rows = (int)((r1 - t0) < TR ? (r1 - t0) : TR);
-        // phase A: w' = w - V c for the tile
-        for (int pk = threadIdx.x; pk < rows * PR; pk += kT) {
-            const int64_t e = t0 * PR + pk;
-            double2 acc[E];
-            P::get(Wp[e], acc);
-#pragma unroll 8
-            for (int i = 0; i < ncols; ++i) {
-                double2 v[E];
-                P::get(Vp[(int64_t)i * total + e], v);
-#pragma unroll
-                for (int q = 0; q < E; ++q) {
-                    const double2 cf = c[i * NB + pr0 + q];
-                    acc[q].x -= cf.x * v[q].x - cf.y * v[q].y;
-                    acc[q].y -= cf.x * v[q].y + cf.y * v[q].x;
-                }
-            }
-            const PT st = P::put(acc);
-            Wp[e] = st;
-            P::get(st, acc);
-            const int t = pk / PR;
-#pragma unroll
-            for (int q = 0; q < E; ++q) {
-                wn2[q] += acc[q].x * acc[q].x + acc[q].y * acc[q].y;
-                wt[t * NB + pr0 + q] = fr2<VT>(acc[q]);
-            }
-        }
-        __syncthreads();
-        // phase B: warp wid projects columns wid, wid + 8, ... over the tile
-#pragma unroll
-        for (int k = 0; k < MAXC; ++k) {
-            const int i = wid + 8 * k;
-            if (i < ncols) {
-                const PT* col = Vp + (int64_t)i * total + t0 * PR;
-#pragma unroll 4
-                for (int t = rs; t < rows; t += RS) {
-                    double2 v[E];
-                    P::get(col[t * PR + rp], v);
-#pragma unroll
-                    for (int q = 0; q < E; ++q) {
-                        const double2 w = to2(wt[t * NB + rp * E + q]);
-                        ax[k][q] += v[q].x * w.x + v[q].y * w.y;
-                        ay[k][q] += v[q].x * w.y - v[q].y * w.x;
-                    }
-                }
-            }
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int q = 0; q < E; ++q) atomicAdd(&nrm[pr0 + q], wn2[q]);
-    double2* out = partial + (int64_t)blockIdx.x * (kMaxCols + 1) * NB;
-#pragma unroll
-    for (int k = 0; k < MAXC; ++k) {
-        const int i = wid + 8 * k;
-#pragma unroll
-        for (int q = 0; q < E; ++q) {
-            double sx = ax[k][q], sy = ay[k][q];
-#pragma unroll
-            for (int o = PR; o < 32; o <<= 1) {
-                sx += __shfl_xor_sync(0xffffffffu, sx, o);
-                sy += __shfl_xor_sync(0xffffffffu, sy, o);
-            }
-            if (i < ncols && rs == 0) out[i * NB + rp * E + q] = make_double2(sx, sy);
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x < NB) {
-        npartial[(int64_t)blockIdx.x * NB + threadIdx.x] = nrm[threadIdx.x];
-        out[ncols * NB + threadIdx.x] = make_double2(nrm[threadIdx.x], 0.0);
-    }
-}
-
 // launched with NB warps: warp r reduces the norm partials of right-hand side r
 template <int NB>
 __global__ void k_bdecide(const double2* coefA, int ncols, const double* npartial, int grid, int* flag, int* any,
@@ -593,20 +478,10 @@ struct BlockLanczos {
         BlockMv<VT>::run(h, col(j), w, ud.p, NB);   // counted by its launcher
         const int nc = j + 1;
         proj(nc, w, coefA.p, nullptr);
-        if (nc <= kFuseCols) {
-            // first update fused with the second projection (computed for every right-hand side,
-            // used where the DGKS test asks for the second pass)
-            const int fg = std::min(grid, ugrid);
-            k_bupdproj<VT, NB><<<fg, kT, 0, st>>>(V.p, N, nc, coefA.p, w, partial.p, npart.p);
-            k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, fg, flag.p, any.p, after.p);
-            k_breduce<NB><<<breduce_grid(nc + 1, NB), 256, 0, st>>>(partial.p, fg, nc + 1, coefB.p, nullptr);
-            launches += 3;
-        } else {
-            update(nc, coefA.p, w, nullptr, nullptr);
-            k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p);
-            proj(nc, w, coefB.p, any.p);
-            ++launches;
-        }
+        update(nc, coefA.p, w, nullptr, nullptr);
+        k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p);
+        ++launches;
+        proj(nc, w, coefB.p, any.p);
         update(nc, coefB.p, w, flag.p, any.p);
         k_bfinalize<NB><<<1, NB * 32, 0, st>>>(coefA.p, coefB.p, nc, npart.p, ugrid, flag.p, any.p, after.p, scal.p,
                                           alpha.p, beta.p, j, m);
