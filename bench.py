@@ -720,7 +720,7 @@ def main():
             "speedup_vs_plain": (value / world) / plain["solves_per_s"] if plain else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": MV_DRAM_BYTES, "peak_source": peak_src,
-                         "kernel": "block matvec c64 x32 (k_block_matvec32<float>)",
+                         "kernel": "block matvec c64 x32 (k_block_matvec_v<float, 32>)",
                          "launches": n_mv, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "cpu_baseline": cpu,

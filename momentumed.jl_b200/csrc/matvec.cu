@@ -44,12 +44,6 @@ struct WarpScratch {
     int32_t pref[33];
 };
 
-template <typename R> struct HitScratch {
-    uint32_t j[32];
-    typename Cx<R>::T a[32];
-    typename Cx<R>::T b[32];
-};
-
 __device__ __forceinline__ double2 load_amp(const double2* p, int t) { return __ldg(p + t); }
 __device__ __forceinline__ float2 load_amp(const float2* p, int t) { return __ldg(p + t); }
 
@@ -278,133 +272,23 @@ k_count(IndexView iv, OpView ov, unsigned long long* hits, unsigned long long* m
 }
 
 // Block map: NB right-hand sides interleaved as x[row * NB + b], operator H_b = A + u[b] B.
-// Lanes first evaluate 32 candidate terms (index lookup once per hit), then sweep the
-// compacted hits with lane = right-hand side, so every gather reads NB contiguous values.
-template <typename R, int NB, bool HAS_B>
-__global__ void __launch_bounds__(kWarps * 32)
-k_block_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-               const R* __restrict__ u, int64_t rows) {
-    using C2 = typename Cx<R>::T;
-    static_assert(NB >= 1 && NB <= 32 && (NB & (NB - 1)) == 0, "NB must be a power of two <= 32");
-    constexpr int NSUB = 32 / NB;
-    __shared__ SharedTables sh;
-    __shared__ WarpScratch s_ws[kWarps];
-    __shared__ HitScratch<R> s_hits[kWarps];
-    stage_tables(sh, iv);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int r = lane % NB, sub = lane / NB;
-    WarpScratch& ws = s_ws[wid];
-    HitScratch<R>& hs = s_hits[wid];
-    const R ur = HAS_B ? u[r] : R(0);
-    const C2* __restrict__ A = amp_a<R>(ov);
-    const C2* __restrict__ B = amp_b<R>(ov);
-    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
-        const uint64_t s = __ldg(iv.basis + row);
-        R ar = 0, ai = 0;        // A (and A + uB) contributions of this lane's right-hand side
-        R br = 0, bi = 0;        // B-only contributions, scaled by u at the end
-        R dax = 0, day = 0, dbx = 0, dby = 0;   // diagonal amplitudes met by this lane
-        for_each_group_batch(s, ov, [&](int g) {
-            int total = stage_batch(g, ov, ws);
-            int gi = 0;
-            for (int f0 = 0; f0 < total; f0 += 32) {
-                int f = f0 + lane;
-                int64_t j = -1;
-                int t = 0;
-                bool neg = false;
-                if (f < total) j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
-                if (j == row) {   // diagonal term: its target is the row itself
-                    C2 a = load_amp(A, t);
-                    dax += a.x;
-                    day += a.y;
-                    if (HAS_B) {
-                        C2 b = load_amp(B, t);
-                        dbx += b.x;
-                        dby += b.y;
-                    }
-                    j = -1;
-                }
-                unsigned hm = __ballot_sync(kFull, j >= 0);
-                if (j >= 0) {
-                    int k = __popc(hm & ((1u << lane) - 1u));
-                    C2 a = load_amp(A, t);
-                    C2 b;
-                    b.x = 0; b.y = 0;
-                    if (HAS_B) b = load_amp(B, t);
-                    if (neg) { a.x = -a.x; a.y = -a.y; b.x = -b.x; b.y = -b.y; }
-                    hs.j[k] = (uint32_t)j;
-                    hs.a[k] = a;
-                    hs.b[k] = b;
-                }
-                __syncwarp();
-                const int nh = __popc(hm);
-#pragma unroll 4
-                for (int k = sub; k < nh; k += NSUB) {
-                    uint32_t jj = hs.j[k];
-                    C2 a = hs.a[k];
-                    C2 xv = x[(int64_t)jj * NB + r];
-                    if (HAS_B) {
-                        C2 b = hs.b[k];
-                        if (a.x == R(0) && a.y == R(0)) {     // same hit on every lane: uniform branch
-                            br += b.x * xv.x - b.y * xv.y;
-                            bi += b.x * xv.y + b.y * xv.x;
-                            continue;
-                        }
-                        a.x += ur * b.x;
-                        a.y += ur * b.y;
-                    }
-                    ar += a.x * xv.x - a.y * xv.y;
-                    ai += a.x * xv.y + a.y * xv.x;
-                }
-                __syncwarp();
-            }
-        });
-        if (HAS_B) {
-            ar += ur * br;
-            ai += ur * bi;
-        }
-        // diagonal part, applied once per row
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            dax += __shfl_xor_sync(kFull, dax, o);
-            day += __shfl_xor_sync(kFull, day, o);
-            if (HAS_B) {
-                dbx += __shfl_xor_sync(kFull, dbx, o);
-                dby += __shfl_xor_sync(kFull, dby, o);
-            }
-        }
-        if (sub == 0) {
-            R cx = dax, cy = day;
-            if (HAS_B) {
-                cx += ur * dbx;
-                cy += ur * dby;
-            }
-            C2 xd = x[row * NB + r];
-            ar += cx * xd.x - cy * xd.y;
-            ai += cx * xd.y + cy * xd.x;
-        }
-#pragma unroll
-        for (int o = NB; o < 32; o <<= 1) {
-            ar += __shfl_xor_sync(kFull, ar, o);
-            ai += __shfl_xor_sync(kFull, ai, o);
-        }
-        if (sub == 0) {
-            C2 out;
-            out.x = ar;
-            out.y = ai;
-            y[row * NB + r] = out;
-        }
-    }
-}
-
-// Block map specialised for 32 right-hand sides.  Candidate terms are evaluated as in
-// k_block_matvec (one index lookup per hit), but hits are compacted into three lists by
-// amplitude kind (B only, A only, both), and each hit's 32 values are read by LPH lanes with
-// RPL right-hand sides per lane (RPL = 4 for c64, 2 for c128, 16-byte loads), so one warp
-// iteration consumes HPI = 32 / LPH hits.  B-only hits accumulate into a separate sum that
-// is scaled by u once per row.
-template <typename R> struct Blk32;
-template <> struct Blk32<float> { static constexpr int RPL = 4; };
-template <> struct Blk32<double> { static constexpr int RPL = 2; };
+// Candidate terms are evaluated once per row for all NB
+// right-hand sides (one index lookup per hit); hits are compacted into three lists by amplitude
+// kind (B only, A only, both), and each hit's NB values are read by LPH = NB / RPL lanes with RPL
+// right-hand sides per lane (RPL = min(NB, 4) for c64; for c128 2 at NB = 32, else 1: 16-byte
+// loads), so one warp iteration consumes HPI = 32 / LPH hits.  B-only hits accumulate into
+// a separate sum that is scaled by u once per row.
+template <typename R> struct BlkMax;
+template <> struct BlkMax<float> { static constexpr int RPL = 4; };
+template <> struct BlkMax<double> { static constexpr int RPL = 2; };
+template <typename R, int NB> struct Blk {
+    static constexpr int RPL = NB < BlkMax<R>::RPL ? NB : BlkMax<R>::RPL;
+};
+// c128 below 32 right-hand sides: one 16-byte value per lane keeps the register count (and so the
+// occupancy) of the candidate stage; two per lane measured slower there
+template <int NB> struct Blk<double, NB> {
+    static constexpr int RPL = NB == 32 ? 2 : 1;
+};
 
 template <typename R> struct HitLists {
     uint32_t j[3][32];
@@ -412,30 +296,32 @@ template <typename R> struct HitLists {
     typename Cx<R>::T cb[32];
 };
 
-template <typename R>
-__device__ __forceinline__ void load_rpl(const typename Cx<R>::T* __restrict__ p, typename Cx<R>::T* v);
-template <>
-__device__ __forceinline__ void load_rpl<float>(const float2* __restrict__ p, float2* v) {
-    float4 a = __ldg(reinterpret_cast<const float4*>(p));
-    float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-    v[0] = make_float2(a.x, a.y);
-    v[1] = make_float2(a.z, a.w);
-    v[2] = make_float2(b.x, b.y);
-    v[3] = make_float2(b.z, b.w);
-}
-template <>
-__device__ __forceinline__ void load_rpl<double>(const double2* __restrict__ p, double2* v) {
-    v[0] = __ldg(p);
-    v[1] = __ldg(p + 1);
+// RPL consecutive complex values starting at p (p aligned to RPL values)
+template <typename R, int RPL>
+__device__ __forceinline__ void load_rpl(const typename Cx<R>::T* __restrict__ p, typename Cx<R>::T* v) {
+    if constexpr (std::is_same<R, float>::value && RPL == 4) {
+        float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+        v[0] = make_float2(a.x, a.y);
+        v[1] = make_float2(a.z, a.w);
+        v[2] = make_float2(b.x, b.y);
+        v[3] = make_float2(b.z, b.w);
+    } else if constexpr (std::is_same<R, float>::value && RPL == 2) {
+        float4 a = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = make_float2(a.x, a.y);
+        v[1] = make_float2(a.z, a.w);
+    } else {
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) v[q] = __ldg(p + q);
+    }
 }
 
-template <typename R, bool HAS_B>
-__global__ void __launch_bounds__(kWarps * 32)
-k_block_matvec32(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+template <typename R, int NB, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32, (std::is_same<R, double>::value && NB == 32) ? 3 : 4)
+k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
                  const R* __restrict__ u, int64_t rows) {
     using C2 = typename Cx<R>::T;
-    constexpr int NB = 32;
-    constexpr int RPL = Blk32<R>::RPL;
+    constexpr int RPL = Blk<R, NB>::RPL;
     constexpr int LPH = NB / RPL;      // lanes per hit
     constexpr int HPI = 32 / LPH;      // hits per warp iteration
     __shared__ SharedTables sh;
@@ -495,7 +381,7 @@ k_block_matvec32(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
                 const int n0 = __popc(m0), n1 = __popc(m1), n2 = __popc(m2);
                 for (int k = hslot; k < n0; k += HPI) {          // B only: accumulate, scale by u later
                     const C2 c = hl.c[0][k];
-                    load_rpl<R>(x + (int64_t)hl.j[0][k] * NB + r0, xv);
+                    load_rpl<R, RPL>(x + (int64_t)hl.j[0][k] * NB + r0, xv);
 #pragma unroll
                     for (int q = 0; q < RPL; ++q) {
                         ab[q].x += c.x * xv[q].x - c.y * xv[q].y;
@@ -504,7 +390,7 @@ k_block_matvec32(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
                 }
                 for (int k = hslot; k < n1; k += HPI) {          // A only
                     const C2 c = hl.c[1][k];
-                    load_rpl<R>(x + (int64_t)hl.j[1][k] * NB + r0, xv);
+                    load_rpl<R, RPL>(x + (int64_t)hl.j[1][k] * NB + r0, xv);
 #pragma unroll
                     for (int q = 0; q < RPL; ++q) {
                         aa[q].x += c.x * xv[q].x - c.y * xv[q].y;
@@ -513,7 +399,7 @@ k_block_matvec32(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
                 }
                 for (int k = hslot; k < n2; k += HPI) {          // both: A + u B per right-hand side
                     const C2 c = hl.c[2][k], cb = hl.cb[k];
-                    load_rpl<R>(x + (int64_t)hl.j[2][k] * NB + r0, xv);
+                    load_rpl<R, RPL>(x + (int64_t)hl.j[2][k] * NB + r0, xv);
 #pragma unroll
                     for (int q = 0; q < RPL; ++q) {
                         R cx = c.x + ur[q] * cb.x, cy = c.y + ur[q] * cb.y;
@@ -545,7 +431,7 @@ k_block_matvec32(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
         }
         if (hslot == 0) {
             C2 xd[RPL];
-            load_rpl<R>(x + row * NB + r0, xd);
+            load_rpl<R, RPL>(x + row * NB + r0, xd);
 #pragma unroll
             for (int q = 0; q < RPL; ++q) {
                 R cx = dax + ur[q] * dbx, cy = day + ur[q] * dby;
@@ -620,10 +506,10 @@ static void block_dispatch(const IndexView& iv, const OpView& ov, const typename
 #define MOMED_BLK(NBV)                                                                                   \
     case NBV:                                                                                            \
         if (hb) {                                                                                        \
-            auto k = k_block_matvec<R, NBV, true>;                                                       \
+            auto k = k_block_matvec_v<R, NBV, true>;                                                     \
             k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);                  \
         } else {                                                                                         \
-            auto k = k_block_matvec<R, NBV, false>;                                                      \
+            auto k = k_block_matvec_v<R, NBV, false>;                                                    \
             k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);                  \
         }                                                                                                \
         break;
@@ -633,15 +519,7 @@ static void block_dispatch(const IndexView& iv, const OpView& ov, const typename
         MOMED_BLK(4)
         MOMED_BLK(8)
         MOMED_BLK(16)
-        case 32:
-            if (hb) {
-                auto k = k_block_matvec32<R, true>;
-                k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);
-            } else {
-                auto k = k_block_matvec32<R, false>;
-                k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);
-            }
-            break;
+        MOMED_BLK(32)
         default:
             throw Error{MOMED_EINVAL, "block width must be a power of two <= 32"};
     }
