@@ -157,6 +157,9 @@ MOMED_API int  momed_last_kernel_ms(momed_handle* h, double* ms);
  * runs one EDsolve at a time).  `slots` worker contexts, each with its own stream, take
  * queued requests in arrival order as soon as a slot is free and the request's HBM estimate
  * fits the budget (0 = 85% of free memory); admitted solves run concurrently on the device.
+ * Queued requests on the same operator, sector basis and precision are solved together as one
+ * batched solve (3 to 32 of them, one right-hand side per u); a request alone runs the FP64
+ * single-vector solver; requests of at least 131072 states run one at a time.
  * Requests larger than the budget fail at once with MOMED_ENOMEM.  poll waits at most
  * wait_ms and returns MOMED_ETIMEOUT when the request is still queued or running;
  * status: 0 queued, 1 running, 2 done, 3 failed (return code is the failure's), 4 cancelled. */

@@ -88,7 +88,7 @@ constexpr int64_t kLargeRows = 1 << 17;
 // Smallest group that the batched solver serves faster per request than the single-vector solver.
 constexpr int kMinGroup = 3;
 // Largest nev for which a group takes the mixed-precision batched solver.
-constexpr int kMaxMixedNev = 8;
+constexpr int kMaxMixedNev = 12;
 
 // HBM a solve needs: basis, index tables (bounded), Krylov basis, Ritz/refinement buffers.
 // nb: right-hand sides of a batched solve (a power of two), 0 for the single-vector solver.
