@@ -770,6 +770,83 @@ k_bcombine_xq(const double2* __restrict__ X, int kx, const double2* __restrict__
 }
 
 
+// Inner products of ncols columns of V with up to kGramRhs right-hand-side blocks at once:
+// partial[b][j][i][r] = block's sum over rows of conj(V_i[n][r]) R_j[n][r].  Grid: x = row blocks,
+// y = groups of 8 columns (warp per column, as in k_bproj); every column packet read from HBM
+// serves all right-hand sides, which the block's warps share through L1.
+constexpr int kGramRhs = 4;
+struct GramRhs {
+    const double2* p[kGramRhs];
+};
+template <typename VT, int NB>
+__global__ void __launch_bounds__(kT)
+k_bgram(const VT* __restrict__ V, int64_t N, int ncols, GramRhs R, int nr, double2* __restrict__ partial) {
+    using P = Pack<VT, NB>;
+    constexpr int E = P::E;
+    constexpr int PR = NB / E;
+    constexpr int RS = 32 / PR;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int rp = lane % PR, rs = lane / PR;
+    const int i = blockIdx.y * 8 + wid;
+    if (i >= ncols) return;                     // warp-uniform
+    double ax[kGramRhs][E], ay[kGramRhs][E];
+#pragma unroll
+    for (int j = 0; j < kGramRhs; ++j)
+#pragma unroll
+        for (int q = 0; q < E; ++q) { ax[j][q] = 0.0; ay[j][q] = 0.0; }
+    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
+    const int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(N, r0 + per);
+    const typename P::T* col = reinterpret_cast<const typename P::T*>(V + (int64_t)i * N * NB);
+#pragma unroll 2
+    for (int64_t t = r0 + rs; t < r1; t += RS) {
+        double2 v[E];
+        P::get(col[t * PR + rp], v);
+#pragma unroll
+        for (int j = 0; j < kGramRhs; ++j) {
+            if (j < nr) {
+#pragma unroll
+                for (int q = 0; q < E; ++q) {
+                    const double2 w = __ldg(R.p[j] + t * NB + rp * E + q);
+                    ax[j][q] += v[q].x * w.x + v[q].y * w.y;
+                    ay[j][q] += v[q].x * w.y - v[q].y * w.x;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kGramRhs; ++j) {
+#pragma unroll
+        for (int q = 0; q < E; ++q) {
+            double sx = ax[j][q], sy = ay[j][q];
+#pragma unroll
+            for (int o = PR; o < 32; o <<= 1) {
+                sx += __shfl_xor_sync(0xffffffffu, sx, o);
+                sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            }
+            if (j < nr && rs == 0)
+                partial[(((int64_t)blockIdx.x * kGramRhs + j) * ncols + i) * NB + rp * E + q] = make_double2(sx, sy);
+        }
+    }
+}
+
+// out[e] = sum over blocks b < grid of partial[b * bstride + e] for e < count, one warp per
+// element (fixed order)
+__global__ void k_bsum_blocks(const double2* __restrict__ partial, int grid, int64_t bstride, int64_t count,
+                              double2* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t e = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (e >= count) return;
+    double sx = 0.0, sy = 0.0;
+    for (int b = lane; b < grid; b += 32) {
+        const double2 v = partial[(int64_t)b * bstride + e];
+        sx += v.x;
+        sy += v.y;
+    }
+    sx = wsum(sx);
+    sy = wsum(sy);
+    if (lane == 0) out[e] = make_double2(sx, sy);
+}
+
 template <int NB>
 int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32_t nu, double* vals, double* resid,
               double* vecs, momed_info* info) {
@@ -958,11 +1035,16 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
             DevBuf<double> thd, wtd;
             thd.resize((size_t)NB * k1);
             wtd.resize((size_t)NB * k1);
-            DevBuf<double2> red, Yd, Y2d, W2;
-            red.resize((size_t)(kMaxCols + 1) * NB);
+            DevBuf<double2> Yd, Y2d, W2;
             Yd.resize((size_t)k1 * d * NB);
             Y2d.resize((size_t)k1 * d2 * NB);
             W2.resize((size_t)k1 * stride);
+            // Gram partials [row block][kGramRhs][columns][NB] and the summed blocks [2 k1][columns][NB]
+            DevBuf<double2> gpart, gx, gq;
+            gpart.resize((size_t)LR.grid * kGramRhs * std::max(k1, m - k1) * NB);
+            const size_t gx_n = (size_t)2 * k1 * k1 * NB, gq_n = (size_t)2 * k1 * (m - k1) * NB;
+            gx.resize(gx_n);
+            gq.resize(gq_n);
             std::vector<int> failed(NB, 0);
             std::vector<std::vector<double>> last_t(NB);   // full Ritz spectrum of the last cycle
             const int rg = std::max(1, std::min<int>((int)((stride + 255) / 256), 512));
@@ -1034,37 +1116,48 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                 // FP64 Gram blocks: b_a^H H b_i and b_a^H b_i for the anchors i against [X, Q]
                 std::vector<std::vector<std::complex<double>>> G(NB, std::vector<std::complex<double>>((size_t)d * d)),
                     S(NB, std::vector<std::complex<double>>((size_t)d * d));
-                std::vector<double2> hr((size_t)(kMaxCols + 1) * NB);
-                auto gram = [&](const void* cols, bool fp32, int ncols, const double2* rhs) {
+                // FP64 Gram blocks: b_a^H H b_i and b_a^H b_i for the anchors i against [X, Q]; the
+                // 2 k1 right-hand sides (W_i, then X_i) go kGramRhs at a time
+                const int nrhs = 2 * k1;
+                auto gram = [&](const void* cols, bool fp32, int ncols, int g0, int nr, double2* out) {
                     const int rb = bproj_rowblocks(N, ncols, sms(), LR.grid, rows_tile<NB>());
+                    GramRhs R{};
+                    for (int j = 0; j < nr; ++j)
+                        R.p[j] = (g0 + j < k1 ? Wb.p + (size_t)(g0 + j) * stride : Xb.p + (size_t)(g0 + j - k1) * stride);
+                    for (int j = nr; j < kGramRhs; ++j) R.p[j] = R.p[0];
                     if (fp32)
-                        k_bproj<float2, double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
-                            reinterpret_cast<const float2*>(cols), N, ncols, rhs, LR.partial.p, nullptr);
+                        k_bgram<float2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
+                            reinterpret_cast<const float2*>(cols), N, ncols, R, nr, gpart.p);
                     else
-                        k_bproj<double2, double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
-                            reinterpret_cast<const double2*>(cols), N, ncols, rhs, LR.partial.p, nullptr);
-                    k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(LR.partial.p, rb, ncols + 1, red.p,
-                                                                             nullptr);
+                        k_bgram<double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
+                            reinterpret_cast<const double2*>(cols), N, ncols, R, nr, gpart.p);
+                    // the nr valid slabs lead each block's [kGramRhs][ncols][NB] partials
+                    const int64_t bstride = (int64_t)kGramRhs * ncols * NB, count = (int64_t)nr * ncols * NB;
+                    k_bsum_blocks<<<(unsigned)((count + 7) / 8), 256, 0, st>>>(gpart.p, rb, bstride, count, out);
                     note_launches(2);
-                    MOMED_CUDA_TRY(cudaMemcpyAsync(hr.data(), red.p, (size_t)(ncols + 1) * NB * sizeof(double2),
-                                                   cudaMemcpyDeviceToHost, st));
-                    MOMED_CUDA_TRY(cudaStreamSynchronize(st));
                 };
-                for (int i = 0; i < k1; ++i) {
-                    for (int pass = 0; pass < 2; ++pass) {
-                        const double2* rhs = (pass == 0 ? Wb.p : Xb.p) + (size_t)i * stride;
-                        auto& M = pass == 0 ? G : S;
-                        gram(Xb.p, false, k1, rhs);              // x_a^H rhs
-                        for (int q = 0; q < nu; ++q)
-                            for (int a = 0; a < k1; ++a)
-                                M[q][(size_t)i * d + a] = std::complex<double>(hr[a * NB + q].x, hr[a * NB + q].y);
-                        gram(LR.col(k1), true, p, rhs);          // q_j^H rhs
-                        for (int q = 0; q < nu; ++q)
-                            for (int j = 0; j < p; ++j) {
-                                std::complex<double> v(hr[j * NB + q].x, hr[j * NB + q].y);
-                                M[q][(size_t)i * d + k1 + j] = v;
-                                M[q][(size_t)(k1 + j) * d + i] = std::conj(v);
-                            }
+                for (int g0 = 0; g0 < nrhs; g0 += kGramRhs) {
+                    const int nr = std::min(kGramRhs, nrhs - g0);
+                    gram(Xb.p, false, k1, g0, nr, gx.p + (size_t)g0 * k1 * NB);          // x_a^H rhs
+                    gram(LR.col(k1), true, p, g0, nr, gq.p + (size_t)g0 * p * NB);       // q_j^H rhs
+                }
+                std::vector<double2> hx((size_t)gx_n), hq((size_t)gq_n);
+                MOMED_CUDA_TRY(cudaMemcpyAsync(hx.data(), gx.p, hx.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+                MOMED_CUDA_TRY(cudaMemcpyAsync(hq.data(), gq.p, hq.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+                MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+                for (int jr = 0; jr < nrhs; ++jr) {
+                    const int i = jr < k1 ? jr : jr - k1;
+                    auto& M = jr < k1 ? G : S;
+                    const double2* bx = hx.data() + (size_t)jr * k1 * NB;
+                    const double2* bq = hq.data() + (size_t)jr * p * NB;
+                    for (int q = 0; q < nu; ++q) {
+                        for (int a = 0; a < k1; ++a)
+                            M[q][(size_t)i * d + a] = std::complex<double>(bx[a * NB + q].x, bx[a * NB + q].y);
+                        for (int j = 0; j < p; ++j) {
+                            std::complex<double> v(bq[j * NB + q].x, bq[j * NB + q].y);
+                            M[q][(size_t)i * d + k1 + j] = v;
+                            M[q][(size_t)(k1 + j) * d + i] = std::conj(v);
+                        }
                     }
                 }
                 std::vector<double2> Yh((size_t)k1 * d * NB, make_double2(0.0, 0.0));
