@@ -605,9 +605,11 @@ struct BlockLanczos {
                 }
                 return out;
             }
-            // a third of the spare dimension beyond nev; measured on B200 (m 30, nev 4: 12 kept beat
-            // 10, 15, 20 and (3m + 2 nconv)/5 by 5-13%); large nev keeps its buffer of spare vectors
-            int keep = nev + (m - nev) / 3;
+            // Few wanted pairs (nev <= m/5) keep a third of the spare dimension beyond nev: measured
+            // on B200 at m 30, nev 4, 12 kept beat 10, 15, 20 and (3m + 2 nconv)/5 by 5-13%.  More
+            // wanted pairs keep (3m + 2 nconv)/5: at m 36, nev 12 a third of the spare dimension
+            // (20 kept) needed 1.7x the maps, and at nev 15-20 it was 0-3% slower.
+            int keep = 5 * nev <= m ? nev + (m - nev) / 3 : (3 * m + 2 * minconv) / 5;
             keep = std::max(keep, std::min(nwant, m - 2));
             keep = std::max(keep, nev);
             keep = std::min(keep, m - 2);

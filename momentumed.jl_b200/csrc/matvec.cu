@@ -290,10 +290,14 @@ template <int NB> struct Blk<double, NB> {
     static constexpr int RPL = NB == 32 ? 2 : 1;
 };
 
-template <typename R> struct HitLists {
-    uint32_t j[3][32];
-    typename Cx<R>::T c[3][32];
-    typename Cx<R>::T cb[32];
+// Per-warp rings of found hits, one per amplitude kind.  A batch of 32 candidates yields about
+// a dozen hits; they wait in the ring until 32 of a kind are pending, so the accumulation runs
+// whole iterations and keeps several gathers in flight.
+constexpr int kRing = 64;
+template <typename R> struct HitRing {
+    uint32_t j[3][kRing];
+    typename Cx<R>::T c[3][kRing];
+    typename Cx<R>::T cb[kRing];
 };
 
 // RPL consecutive complex values starting at p (p aligned to RPL values)
@@ -316,6 +320,41 @@ __device__ __forceinline__ void load_rpl(const typename Cx<R>::T* __restrict__ p
     }
 }
 
+// Accumulate the hits at ring positions start .. start + n - 1 (mod kRing) of amplitude kind KIND
+// into acc: each hit's NB values are read by NB / RPL lanes.  N > 0 fixes n = N at compile time.
+template <typename R, int NB, int KIND, int N>
+__device__ __forceinline__ void consume_hits(const HitRing<R>& hl, int start, int n, int hslot, int r0,
+                                             const typename Cx<R>::T* __restrict__ x, const R* ur,
+                                             typename Cx<R>::T* acc) {
+    using C2 = typename Cx<R>::T;
+    constexpr int RPL = Blk<R, NB>::RPL;
+    constexpr int HPI = 32 / (NB / RPL);
+    auto one = [&](int k) {
+        const int p = (start + k) & (kRing - 1);
+        const C2 c = hl.c[KIND][p];
+        C2 cb;
+        if constexpr (KIND == 2) cb = hl.cb[p];
+        C2 xv[RPL];
+        load_rpl<R, RPL>(x + (int64_t)hl.j[KIND][p] * NB + r0, xv);
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            R cx = c.x, cy = c.y;
+            if constexpr (KIND == 2) {
+                cx += ur[q] * cb.x;
+                cy += ur[q] * cb.y;
+            }
+            acc[q].x += cx * xv[q].x - cy * xv[q].y;
+            acc[q].y += cx * xv[q].y + cy * xv[q].x;
+        }
+    };
+    if constexpr (N > 0) {
+#pragma unroll 2
+        for (int i = 0; i < N / HPI; ++i) one(hslot + i * HPI);
+    } else {
+        for (int k = hslot; k < n; k += HPI) one(k);
+    }
+}
+
 template <typename R, int NB, bool HAS_B>
 __global__ void __launch_bounds__(kWarps * 32, (std::is_same<R, double>::value && NB == 32) ? 3 : 4)
 k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
@@ -323,15 +362,14 @@ k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
     using C2 = typename Cx<R>::T;
     constexpr int RPL = Blk<R, NB>::RPL;
     constexpr int LPH = NB / RPL;      // lanes per hit
-    constexpr int HPI = 32 / LPH;      // hits per warp iteration
     __shared__ SharedTables sh;
     __shared__ WarpScratch s_ws[kWarps];
-    __shared__ HitLists<R> s_hits[kWarps];
+    __shared__ HitRing<R> s_hits[kWarps];
     stage_tables(sh, iv);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int hslot = lane / LPH, r0 = (lane % LPH) * RPL;
     WarpScratch& ws = s_ws[wid];
-    HitLists<R>& hl = s_hits[wid];
+    HitRing<R>& hl = s_hits[wid];
     R ur[RPL];
 #pragma unroll
     for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? u[r0 + q] : R(0);
@@ -344,6 +382,7 @@ k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
 #pragma unroll
         for (int q = 0; q < RPL; ++q) { aa[q].x = 0; aa[q].y = 0; ab[q].x = 0; ab[q].y = 0; }
         R dax = 0, day = 0, dbx = 0, dby = 0;
+        int hd0 = 0, hd1 = 0, hd2 = 0, n0 = 0, n1 = 0, n2 = 0;   // ring heads and pending hits (warp-uniform)
         for_each_group_batch(s, ov, [&](int g) {
             int total = stage_batch(g, ov, ws);
             int gi = 0;
@@ -371,45 +410,38 @@ k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
                 const unsigned m2 = __ballot_sync(kFull, j >= 0 && kind == 2);
                 if (j >= 0) {
                     const unsigned mk = kind == 0 ? m0 : (kind == 1 ? m1 : m2);
-                    const int k = __popc(mk & lt);
-                    hl.j[kind][k] = (uint32_t)j;
-                    hl.c[kind][k] = kind == 0 ? b : a;
-                    if (kind == 2) hl.cb[k] = b;
+                    const int at = kind == 0 ? hd0 + n0 : (kind == 1 ? hd1 + n1 : hd2 + n2);
+                    const int p = (at + __popc(mk & lt)) & (kRing - 1);
+                    hl.j[kind][p] = (uint32_t)j;
+                    hl.c[kind][p] = kind == 0 ? b : a;
+                    if (kind == 2) hl.cb[p] = b;
                 }
+                n0 += __popc(m0);
+                n1 += __popc(m1);
+                n2 += __popc(m2);
                 __syncwarp();
-                C2 xv[RPL];
-                const int n0 = __popc(m0), n1 = __popc(m1), n2 = __popc(m2);
-                for (int k = hslot; k < n0; k += HPI) {          // B only: accumulate, scale by u later
-                    const C2 c = hl.c[0][k];
-                    load_rpl<R, RPL>(x + (int64_t)hl.j[0][k] * NB + r0, xv);
-#pragma unroll
-                    for (int q = 0; q < RPL; ++q) {
-                        ab[q].x += c.x * xv[q].x - c.y * xv[q].y;
-                        ab[q].y += c.x * xv[q].y + c.y * xv[q].x;
-                    }
+                if (HAS_B && n0 >= 32) {          // B only: accumulate, scale by u once per row
+                    consume_hits<R, NB, 0, 32>(hl, hd0, 32, hslot, r0, x, ur, ab);
+                    hd0 = (hd0 + 32) & (kRing - 1);
+                    n0 -= 32;
                 }
-                for (int k = hslot; k < n1; k += HPI) {          // A only
-                    const C2 c = hl.c[1][k];
-                    load_rpl<R, RPL>(x + (int64_t)hl.j[1][k] * NB + r0, xv);
-#pragma unroll
-                    for (int q = 0; q < RPL; ++q) {
-                        aa[q].x += c.x * xv[q].x - c.y * xv[q].y;
-                        aa[q].y += c.x * xv[q].y + c.y * xv[q].x;
-                    }
+                if (n1 >= 32) {                   // A only
+                    consume_hits<R, NB, 1, 32>(hl, hd1, 32, hslot, r0, x, ur, aa);
+                    hd1 = (hd1 + 32) & (kRing - 1);
+                    n1 -= 32;
                 }
-                for (int k = hslot; k < n2; k += HPI) {          // both: A + u B per right-hand side
-                    const C2 c = hl.c[2][k], cb = hl.cb[k];
-                    load_rpl<R, RPL>(x + (int64_t)hl.j[2][k] * NB + r0, xv);
-#pragma unroll
-                    for (int q = 0; q < RPL; ++q) {
-                        R cx = c.x + ur[q] * cb.x, cy = c.y + ur[q] * cb.y;
-                        aa[q].x += cx * xv[q].x - cy * xv[q].y;
-                        aa[q].y += cx * xv[q].y + cy * xv[q].x;
-                    }
+                if (HAS_B && n2 >= 32) {          // both: A + u B per right-hand side
+                    consume_hits<R, NB, 2, 32>(hl, hd2, 32, hslot, r0, x, ur, aa);
+                    hd2 = (hd2 + 32) & (kRing - 1);
+                    n2 -= 32;
                 }
                 __syncwarp();
             }
         });
+        if (HAS_B) consume_hits<R, NB, 0, 0>(hl, hd0, n0, hslot, r0, x, ur, ab);
+        consume_hits<R, NB, 1, 0>(hl, hd1, n1, hslot, r0, x, ur, aa);
+        if (HAS_B) consume_hits<R, NB, 2, 0>(hl, hd2, n2, hslot, r0, x, ur, aa);
+        __syncwarp();
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             dax += __shfl_xor_sync(kFull, dax, o);
