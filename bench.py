@@ -68,9 +68,11 @@ def parse():
     ap.add_argument("--krylovdim", type=int, default=0, help="Krylov dimension of the batched solver (default 30)")
     ap.add_argument("--profile-only", action="store_true", help="one short run for ncu (no timing output)")
     ap.add_argument("--workload", default="batch_3x9",
-                    choices=["batch_3x9", "plain_3x5", "plain_3x10", "two_comp_4x6"],
+                    choices=["batch_3x9", "plain_3x5", "plain_3x9", "plain_3x10", "two_comp_4x6"],
                     help="batch_3x9 (the headline); the others time plain single-vector solves")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving stream")
+    ap.add_argument("--method", default="map", choices=["map", "sparse"],
+                    help="plain workloads: matrix-free map, or the sparse method (device-built CSR + SpMV)")
     ap.add_argument("--serve-requests", type=int, default=80)
     ap.add_argument("--serve-meshes", default="3x5,3x9,3x10", help="subset of 3x5,3x9,3x10,4x9")
     ap.add_argument("--serve-slots", type=int, default=4)
@@ -380,9 +382,17 @@ def mv_bytes(N: int, nnz: int, nscat: int, s: int) -> float:
     return N * (8 + 2 * s) + nnz * s + nscat * (s + 24)
 
 
+def sp_bytes(N: int, nnz_sp: int, s: int) -> float:
+    """Algorithmic HBM bytes of one CSR SpMV: the column and value of every stored entry, the row
+    pointers, and x and y once each (x, at most a few tens of MB here, serves its gathers from L2)."""
+    return nnz_sp * (4 + s) + N * (8 + 2 * s)
+
+
 def run_plain_workload(args, rank, world, local):
-    """--workload plain_3x5 | plain_3x10 | two_comp_4x6: one sector per step solved by the plain
-    single-vector Lanczos (FP64, c128 map; the mixed-precision solve is timed beside it)."""
+    """--workload plain_3x5 | plain_3x9 | plain_3x10 | two_comp_4x6: one sector per step solved by the plain
+    single-vector Lanczos (FP64, c128 map; the mixed-precision solve is timed beside it).
+    --method sparse: the sparse method instead, each step building the sector's CSR matrix on
+    the device and solving with the CSR SpMV (build inside the timed step, as in EDsolve)."""
     import torch
 
     import momed
@@ -407,8 +417,12 @@ def run_plain_workload(args, rank, world, local):
     W, K = max(args.warmup, 0), max(args.steps, 1)
     order = sector_order(rank, world, len(sectors), W + K)
 
+    sparse = args.method == "sparse"
+
     def solve(sidx, prec):
         h.select_sector(sidx, len(sectors[sidx][1]))
+        if sparse:
+            h.build_sparse()
         return h.eigsolve(nev, krylovdim=kd, tol=1e-12, seed=1, want_vectors=False, precision=prec)
 
     if args.profile_only:
@@ -433,18 +447,26 @@ def run_plain_workload(args, rank, world, local):
         torch.cuda.synchronize()
     barrier(world)
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(K)]
-    n_mv, ms_mv = h.profile_read(_lib.KERNEL_MATVEC_C128)
+    n_mv, ms_mv = h.profile_read(_lib.KERNEL_SPMV_C128 if sparse else _lib.KERNEL_MATVEC_C128)
     h.profile(False)
     launches = _lib.kernel_launches() - launches0
     elapsed = all_max(sum(step_ms) / 1e3, world)
     value = all_sum(K, world) / elapsed
-    nb, nnz_mean = [], []
+    nb, nnz_mean, build_ms = [], [], []
     for i in range(K):
         sidx = order[W + i]
         h.select_sector(sidx, len(sectors[sidx][1]))
         st = h.stats()
-        nb.append(mv_bytes(len(sectors[sidx][1]), st["nnz"], len(pair[0]), 16))
-        nnz_mean.append(st["nnz"])
+        if sparse:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            nsp = h.build_sparse()
+            build_ms.append((time.perf_counter() - t0) * 1e3)
+            nb.append(sp_bytes(len(sectors[sidx][1]), nsp, 16))
+            nnz_mean.append(nsp)
+        else:
+            nb.append(mv_bytes(len(sectors[sidx][1]), st["nnz"], len(pair[0]), 16))
+            nnz_mean.append(st["nnz"])
     # the mixed-precision solve of the same sectors, for comparison
     t_mixed, err_mixed = [], []
     for i in range(K):
@@ -459,13 +481,15 @@ def run_plain_workload(args, rank, world, local):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         h.set_basis(basis)
+        if sparse:
+            h.build_sparse()
         v, vecs, _, _ = h.eigsolve(nev, krylovdim=kd, tol=1e-12, seed=1, want_vectors=True,
                                    precision=_lib.PREC_FP64)
         e2e_t.append(time.perf_counter() - t0)
         h2d.append(basis.nbytes)
         d2h.append(v.nbytes + vecs.nbytes)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu and not sparse:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O
         amp = pair[0] + pair[1]
@@ -495,8 +519,19 @@ def run_plain_workload(args, rank, world, local):
             except Exception:
                 pass
         N0 = len(sectors[order[W]][1])
+        metric = ("solves/s (sparse method: device-built CSR matrix + FP64 single-vector Lanczos, one sector "
+                  "per step)" if sparse else "solves/s (plain FP64 single-vector Lanczos, one sector per step)")
+        if sparse:
+            kernel = "CSR SpMV c128 (k_spmv<double>)"
+            extra = {"sparse": {"build_ms_mean": float(np.mean(build_ms)), "entries_mean": float(np.mean(nnz_mean)),
+                                "matrix_bytes_per_entry": 28,
+                                "algorithmic_bytes": "column + c128 value per entry, row pointers, x and y once "
+                                                     "(x gathers served from L2)"}}
+        else:
+            kernel = "map c128 (k_matvec<double>)"
+            extra = {}
         line = {
-            "metric": "solves/s (plain FP64 single-vector Lanczos, one sector per step)", "value": value,
+            "metric": metric, "value": value,
             "unit": "solves/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": elapsed * 1e3 / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": {"workload": f"{args.workload}: {w['a']}x{w['b']} mesh, N_each={w['N_each']}, "
@@ -507,7 +542,7 @@ def run_plain_workload(args, rank, world, local):
             "mixed_precision": {"solves_per_s": K / sum(t_mixed), "max_rel_eig_err_vs_fp64": max(err_mixed)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
-                         "kernel": "map c128 (k_matvec<double>)", "launches": n_mv, "avg_launch_ms": avg_ms,
+                         "kernel": kernel, "launches": n_mv, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": float(np.mean(nb)), "nnz": float(np.mean(nnz_mean))},
             "cpu_baseline": cpu,
             "e2e": {"value": K / sum(e2e_t), "unit": "solves/s", "h2d_bytes_per_step": int(np.mean(h2d)),
@@ -515,6 +550,7 @@ def run_plain_workload(args, rank, world, local):
             "gpu_launches": int(all_sum(launches, world)),
             "clocks": clk.summary(),
         }
+        line.update(extra)
         print(json.dumps(line), flush=True)
     h.close()
 

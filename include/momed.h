@@ -145,6 +145,23 @@ MOMED_API int  momed_eigsolve(momed_handle* h, const momed_solve_opts* opts, con
 MOMED_API int  momed_batch_solve(momed_handle* h, const momed_solve_opts* opts, const double* u, int32_t nu,
                        double* vals, double* resid, double* vecs, momed_info* info);
 
+/* GPU sparse method: EDsolve(...; method = :sparse, device = :gpu), whose matrix the reference
+ * builds on host threads (ED_HamiltonianMatrix_threaded_CSCdirect, sparse_matrix.jl:64-190),
+ * uploads (create_gpu_matrix, MomentumEDCUDAExt.jl:145-152) and multiplies inside
+ * krylov_matrix_solve (MomentumEDCUDAExt.jl:180-200).  momed_build_sparse builds H (at the
+ * current u) as a CSR matrix on the device from the working operator and basis: row i = output
+ * state, entry row_ptr[i] is the diagonal, then one entry per off-diagonal (row, term) hit
+ * (a pair reached by two terms keeps two entries).  While it is built, momed_matvec and
+ * momed_eigsolve use the CSR SpMV instead of the matrix-free map; a new basis, operator or u
+ * drops it, as does momed_release_sparse (momed_batch_solve always uses the map).  nnz
+ * receives the stored entries; the matrix takes 8 (N + 1) + 28 nnz bytes and MOMED_ENOMEM is
+ * returned when that exceeds the handle's budget or 90% of free device memory.
+ * momed_sparse_copy copies it to host arrays row_ptr[N + 1], col[nnz], val[2 nnz] (c128);
+ * any of them may be NULL. */
+MOMED_API int  momed_build_sparse(momed_handle* h, int64_t* nnz);
+MOMED_API int  momed_sparse_copy(momed_handle* h, int64_t* row_ptr, int32_t* col, double* val);
+MOMED_API int  momed_release_sparse(momed_handle* h);
+
 /* Diagnostics for roofline accounting: exact (row, term) hit count of the working operator
  * on the working basis, the index mode (0 = ranked tables, 1 = checked tables, 2 = search),
  * and the bytes of the lookup tables. */
@@ -188,6 +205,8 @@ MOMED_API int64_t momed_kernel_launches(void);
 #define MOMED_KERNEL_MATVEC_C64         1
 #define MOMED_KERNEL_BLOCK_MATVEC_C64   2
 #define MOMED_KERNEL_BLOCK_MATVEC_C128  3
+#define MOMED_KERNEL_SPMV_C128          4
+#define MOMED_KERNEL_SPMV_C64           5
 MOMED_API int  momed_profile(momed_handle* h, int32_t enable);
 MOMED_API int  momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms);
 

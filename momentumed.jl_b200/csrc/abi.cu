@@ -51,7 +51,7 @@ void prof_end(momed_handle* h, int kind) {
     if (!h->prof) return;
     h->prof_kind[(h->prof_used - 1) / 2] = kind;
     MOMED_CUDA_TRY(cudaEventRecord(h->prof_ev[h->prof_used++], h->stream));
-    ++h->prof_launches[kind & 3];
+    if (kind >= 0 && kind < 6) ++h->prof_launches[kind];
 }
 
 OpView Operator::view() const {
@@ -167,6 +167,7 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
     h->op_mask_or = mask_or;
     h->op_set = true;
     h->op_validated = false;
+    h->sparse.release();
 }
 
 // Build the index when the basis changed or the operator reaches bits outside it, and
@@ -266,6 +267,7 @@ void after_basis_change(momed_handle* h) {
     h->basis_or = v;
     h->index_dirty = true;
     h->op_validated = false;
+    h->sparse.release();
 }
 
 }  // namespace
@@ -446,6 +448,8 @@ int momed_set_param(momed_handle* h, double u) {
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {
         float uf = (float)u;
+        h->u = u;
+        if (h->sparse.built && h->op.has_b && h->sparse.u != u) h->sparse.release();   // values were built at the old u
         MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
         MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(uf), cudaMemcpyHostToDevice, h->stream));
         MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -470,7 +474,11 @@ int momed_matvec(momed_handle* h, const void* x, void* y, int32_t precision, int
             MOMED_CUDA_TRY(cudaMemcpyAsync(const_cast<void*>(dx), x, n * es, cudaMemcpyHostToDevice, st));
         }
         MOMED_CUDA_TRY(cudaEventRecord(h->ev0, st));
-        if (precision == MOMED_C128)
+        if (h->sparse.built && precision == MOMED_C128)
+            launch_spmv_c128(h->sparse, (const double2*)dx, (double2*)dy, n, st);
+        else if (h->sparse.built)
+            launch_spmv_c64(h->sparse, (const float2*)dx, (float2*)dy, n, st);
+        else if (precision == MOMED_C128)
             launch_matvec_c128(index_view(h), h->op.view(), (const double2*)dx, (double2*)dy,
                                h->op.has_b ? h->u_dev.p : nullptr, n, st);
         else
@@ -504,6 +512,40 @@ int momed_batch_solve(momed_handle* h, const momed_solve_opts* opts, const doubl
     });
 }
 
+int momed_build_sparse(momed_handle* h, int64_t* nnz) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        ensure_ready(h);
+        build_sparse(h, h->u);
+        if (nnz) *nnz = h->sparse.nnz;
+        return MOMED_OK;
+    });
+}
+
+int momed_sparse_copy(momed_handle* h, int64_t* row_ptr, int32_t* col, double* val) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(h->sparse.built, MOMED_ESTATE, "no sparse matrix (momed_build_sparse)");
+        const SparseMatrix& sp = h->sparse;
+        cudaStream_t st = h->stream;
+        if (row_ptr)
+            MOMED_CUDA_TRY(cudaMemcpyAsync(row_ptr, sp.row_ptr.p, (h->n + 1) * 8, cudaMemcpyDeviceToHost, st));
+        if (col) MOMED_CUDA_TRY(cudaMemcpyAsync(col, sp.col.p, sp.nnz * 4, cudaMemcpyDeviceToHost, st));
+        if (val) MOMED_CUDA_TRY(cudaMemcpyAsync(val, sp.val.p, sp.nnz * 16, cudaMemcpyDeviceToHost, st));
+        MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+        return MOMED_OK;
+    });
+}
+
+int momed_release_sparse(momed_handle* h) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->sparse.release();
+        return MOMED_OK;
+    });
+}
+
 int momed_stats(momed_handle* h, int64_t* nnz, int32_t* index_mode, int64_t* table_bytes) {
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {
@@ -528,14 +570,14 @@ int momed_profile(momed_handle* h, int32_t enable) {
     return guarded(h, [&]() {
         MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
         h->prof_used = 0;
-        for (int k = 0; k < 4; ++k) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; }
+        for (int k = 0; k < 6; ++k) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; }
         h->prof = enable != 0;
         return MOMED_OK;
     });
 }
 
 int momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms) {
-    if (!h || kind < 0 || kind > 3) return MOMED_EINVAL;
+    if (!h || kind < 0 || kind > 5) return MOMED_EINVAL;
     return guarded(h, [&]() {
         prof_drain(h);
         if (launches) *launches = h->prof_launches[kind];

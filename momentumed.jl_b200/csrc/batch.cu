@@ -235,7 +235,7 @@ k_bupdate(const VT* __restrict__ V, int64_t N, int ncols, const double2* __restr
 // launched with NB warps: warp r reduces the norm partials of right-hand side r
 template <int NB>
 __global__ void k_bdecide(const double2* coefA, int ncols, const double* npartial, int grid, int* flag, int* any,
-                          double* after) {
+                          double* after, double keep_frac) {
     __shared__ int s_any;
     if (threadIdx.x == 0) s_any = 0;
     __syncthreads();
@@ -246,12 +246,8 @@ __global__ void k_bdecide(const double2* coefA, int ncols, const double* npartia
     if (lane == 0) {
         double before = coefA[ncols * NB + r].x;
         after[r] = a;
-        // second pass when the first removed more than 1 - 0.1 of the squared norm (|w'| < 0.32 |w|).
-        // The classical 1/2 (|w'| < 0.71 |w|) flags nearly every Lanczos step, because w = H v
-        // carries alpha and beta along the two newest columns, and one flagged right-hand side
-        // makes the whole block repeat the pass.  Measured on B200 (3x9, 32 U0): 0.1 and 0.01 run
-        // the same maps and give the same eigenvalues (<= 7e-15 from FP64) as 1/2, 16% faster.
-        int f = (a < 0.1 * before) ? 1 : 0;
+        // second pass when less than keep_frac of the squared norm survived the first
+        int f = (a < keep_frac * before) ? 1 : 0;
         flag[r] = f;
         if (f) atomicOr(&s_any, 1);
     }
@@ -423,6 +419,7 @@ struct BlockLanczos {
     DevBuf<int> flag, any;
     DevBuf<RT> ud;
     int64_t launches = 0;
+    double dgks = 0.5;   // second Gram-Schmidt pass when |w'|^2 < dgks |w|^2 (set by run)
 
     BlockLanczos(momed_handle* hh, int mm, const std::vector<double>& u) : h(hh), N(hh->n), m(mm), st(hh->stream) {
         grid = std::max(1, std::min<int>((int)((N + rows_tile<NB>() - 1) / rows_tile<NB>()), sms() * 4));   // max row blocks
@@ -484,7 +481,7 @@ struct BlockLanczos {
         const int nc = j + 1;
         proj(nc, w, coefA.p, nullptr);
         update(nc, coefA.p, w, nullptr, nullptr);
-        k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p);
+        k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p, dgks);
         ++launches;
         proj(nc, w, coefB.p, any.p);
         update(nc, coefB.p, w, flag.p, any.p);
@@ -532,6 +529,13 @@ struct BlockLanczos {
     Out run(int nev, int nu, double tol, double rel_floor, int maxiter, uint64_t seed, int nwant, double2* vectors,
             const VT* start = nullptr, double eig_target = 0.0) {
         Out out;
+        // The classical 1/2 (|w'| < 0.71 |w|) flags nearly every Lanczos step, because w = H v
+        // carries alpha and beta along the two newest columns, and one flagged right-hand side
+        // makes the whole block repeat the pass.  Measured on B200: with FP64 bases, or few
+        // wanted pairs (nev <= m/5), 0.1 runs the same maps and gives the same eigenvalues as
+        // 1/2 (3x9, 32 U0, nev 4: 16% faster; 0.01 the same); an FP32 basis with nev 12 in m 36
+        // needed 1.65x the maps at 0.1, so FP32 with more wanted pairs keeps 1/2.
+        dgks = (std::is_same<VT, float2>::value && 5 * nev > m) ? 0.5 : 0.1;
         if (start) MOMED_CUDA_TRY(cudaMemcpyAsync(col(0), start, (size_t)N * NB * sizeof(VT), cudaMemcpyDeviceToDevice, st));
         else k_brandom<VT><<<ugrid, kT, 0, st>>>(col(0), N * NB, seed);
         normalize(col(0));
@@ -1041,6 +1045,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
             const int p = m - k1, d = k1 + p;
             const int d2 = 2 * k1 + p + 1;     // sources of W': W, X, Q and the next Lanczos vector
             BlockLanczos<float2, NB> LR(h, m, uv);
+            LR.dgks = 5 * nev > m ? 0.5 : 0.1;   // the rule of BlockLanczos::run for an FP32 basis
             DevBuf<double> thd, wtd;
             thd.resize((size_t)NB * k1);
             wtd.resize((size_t)NB * k1);

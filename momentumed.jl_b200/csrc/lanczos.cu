@@ -43,13 +43,24 @@ template <typename VT> struct Prec;
 template <> struct Prec<double2> { static constexpr int value = MOMED_C128; };
 template <> struct Prec<float2> { static constexpr int value = MOMED_C64; };
 
+// the CSR SpMV while a sparse matrix is built (momed_build_sparse), else the matrix-free map
 void apply_h(momed_handle* h, const double2* x, double2* y) {
     prof_begin(h);
+    if (h->sparse.built) {
+        launch_spmv_c128(h->sparse, x, y, h->n, h->stream);
+        prof_end(h, MOMED_KERNEL_SPMV_C128);
+        return;
+    }
     launch_matvec_c128(index_view(h), h->op.view(), x, y, h->op.has_b ? h->u_dev.p : nullptr, h->n, h->stream);
     prof_end(h, MOMED_KERNEL_MATVEC_C128);
 }
 void apply_h(momed_handle* h, const float2* x, float2* y) {
     prof_begin(h);
+    if (h->sparse.built) {
+        launch_spmv_c64(h->sparse, x, y, h->n, h->stream);
+        prof_end(h, MOMED_KERNEL_SPMV_C64);
+        return;
+    }
     launch_matvec_c64(index_view(h), h->op.view(), x, y, h->op.has_b ? h->u_dev32.p : nullptr, h->n, h->stream);
     prof_end(h, MOMED_KERNEL_MATVEC_C64);
 }

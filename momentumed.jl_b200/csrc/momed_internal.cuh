@@ -160,6 +160,26 @@ struct Operator {
     OpView view() const;
 };
 
+// CSR matrix of the working operator on the working basis (the sparse method, sparse.cu):
+// row_ptr[n + 1]; per entry a column, the FP64 value at u and its FP32 rounding.
+struct SparseMatrix {
+    bool built = false;
+    double u = 0.0;                // parameter the values were built at (H = A + u B)
+    int64_t nnz = 0;
+    DevBuf<int64_t> row_ptr;
+    DevBuf<int32_t> col;
+    DevBuf<double2> val;
+    DevBuf<float2> val32;
+    void release() {
+        built = false;
+        nnz = 0;
+        row_ptr.release();
+        col.release();
+        val.release();
+        val32.release();
+    }
+};
+
 struct Index {
     int32_t mode = INDEX_SEARCH;
     PartDesc hi{}, lo{};
@@ -183,11 +203,13 @@ struct momed_handle {
     bool index_dirty = true;
     uint64_t index_bits = 0;               // bits the index tables cover
     momed::Operator op;
+    momed::SparseMatrix sparse;           // built by momed_build_sparse; maps use it while built
     bool op_set = false;
     bool op_validated = false;
     uint64_t op_mask_or = 0;               // OR of all term masks
     int64_t nnz = 0;                       // (row, term) hits of the validated operator
     momed::DevBuf<double> u_dev;           // parameter u of H(u) = A + u B
+    double u = 1.0;                        // host copy of u
     momed::DevBuf<float> u_dev32;
     momed::DevBuf<uint32_t> binom;         // C(n, k), n, k <= 32
 
@@ -205,8 +227,8 @@ struct momed_handle {
     std::vector<cudaEvent_t> prof_ev;      // pairs (start, stop)
     std::vector<int> prof_kind;            // kind of each pair
     size_t prof_used = 0;                  // events used in the current record
-    int64_t prof_launches[4] = {0, 0, 0, 0};
-    double prof_ms[4] = {0, 0, 0, 0};      // folded-in time of pairs already read
+    int64_t prof_launches[6] = {0, 0, 0, 0, 0, 0};
+    double prof_ms[6] = {0, 0, 0, 0, 0, 0};      // folded-in time of pairs already read
 };
 
 namespace momed {
@@ -231,6 +253,12 @@ void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2
                              const float* u, int32_t nb, int64_t rows, cudaStream_t st);
 void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y,
                               const double* u, int32_t nb, int64_t rows, cudaStream_t st);
+
+// sparse.cu: CSR build at parameter u (after ensure_ready) and the CSR SpMV
+void build_sparse(momed_handle* h, double u);
+int64_t sparse_bytes_per_entry();
+void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int64_t rows, cudaStream_t st);
+void launch_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, int64_t rows, cudaStream_t st);
 
 // operator.cpp-side (in abi.cu)
 void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, const uint64_t* in,

@@ -1,0 +1,286 @@
+// GPU sparse method: the Hamiltonian stored as a CSR matrix built on the device, and y = H x
+// as a CSR SpMV.
+//
+// Reference: EDsolve(...; method = :sparse, device = :gpu) builds the matrix on host threads
+// (ED_HamiltonianMatrix_threaded_CSCdirect, MomentumED/src/method/sparse_matrix.jl:64-190: for
+// every basis state, every term of the Hermitian-completed list, index_fit drops targets
+// outside the subspace, duplicates summed), uploads it (create_gpu_matrix,
+// ext/MomentumEDCUDAExt.jl:145-152) and runs the library SpMV inside KrylovKit
+// (krylov_matrix_solve, MomentumEDCUDAExt.jl:180-200).  Here the matrix is built where it is
+// used, by the candidate machinery of the matrix-free map (candidates.cuh):
+//
+//   count pass   entries of row i = 1 (the diagonal) + its off-diagonal hits
+//   host scan    row_ptr (int64), the total checked against the device budget
+//   fill pass    row i: entry row_ptr[i] = (i, sum of the diagonal terms), then one entry
+//                (j, sign * amp) per off-diagonal hit in candidate order; the value is
+//                A + u B at the handle's current u (FP64), with an FP32 copy for c64 maps
+//
+// Rows are the output states, as in the map's H x (the reference's CSC columns are its input
+// states; H is Hermitian, so both hold the same numbers).  An off-diagonal (row, column) pair
+// reached by more than one term keeps one entry per term (the SpMV sums them); the reference
+// merges such entries.  Dense H is therefore identical up to the rounding of that sum.
+//
+// SpMV: one warp per row, lanes stride over the row's entries four at a time (column and value
+// streams coalesced, the x gathers in flight together), shuffle reduction, no atomics.  It
+// streams 4 + s bytes per entry from HBM (column, value) and gathers x, which stays in L2 for
+// sectors up to a few million states.
+#include <numeric>
+
+#include "candidates.cuh"
+
+namespace momed {
+
+namespace {
+
+__global__ void __launch_bounds__(kWarps * 32)
+k_sparse_count(IndexView iv, OpView ov, int32_t* __restrict__ counts, int64_t rows) {
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpScratch& ws = s_ws[wid];
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        int nh = 0;
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                if (f < total) {
+                    int t;
+                    bool neg;
+                    int64_t j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
+                    if (j >= 0 && j != row) ++nh;
+                }
+            }
+            __syncwarp();
+        });
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) nh += __shfl_xor_sync(kFull, nh, o);
+        if (lane == 0) counts[row] = 1 + nh;
+    }
+}
+
+// bad[0]: entries that fell outside their row's range (count and fill passes disagree)
+template <bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_sparse_fill(IndexView iv, OpView ov, const double* __restrict__ u_ptr, const int64_t* __restrict__ row_ptr,
+              int32_t* __restrict__ col, double2* __restrict__ val, float2* __restrict__ val32, int64_t rows,
+              unsigned long long* bad) {
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    WarpScratch& ws = s_ws[wid];
+    const double u = HAS_B ? *u_ptr : 0.0;
+    unsigned long long nbad = 0;
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        const int64_t base = row_ptr[row], end = row_ptr[row + 1];
+        int64_t pos = base + 1;            // warp-uniform: next free entry of the row
+        double dr = 0.0, di = 0.0;
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                int64_t j = -1;
+                int t = 0;
+                bool neg = false;
+                if (f < total) j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
+                double2 a = make_double2(0.0, 0.0);
+                if (j >= 0) {
+                    a = load_amp(ov.t_amp, t);
+                    if (HAS_B) {
+                        double2 b = load_amp(ov.t_ampb, t);
+                        a.x += u * b.x;
+                        a.y += u * b.y;
+                    }
+                    if (neg) { a.x = -a.x; a.y = -a.y; }
+                }
+                if (j == row) { dr += a.x; di += a.y; }
+                const bool off = j >= 0 && j != row;
+                const unsigned m = __ballot_sync(kFull, off);
+                if (off) {
+                    const int64_t p = pos + __popc(m & lt);
+                    if (p < end) {
+                        col[p] = (int32_t)j;
+                        val[p] = a;
+                        val32[p] = make_float2((float)a.x, (float)a.y);
+                    } else {
+                        ++nbad;
+                    }
+                }
+                pos += __popc(m);
+            }
+            __syncwarp();
+        });
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dr += __shfl_xor_sync(kFull, dr, o);
+            di += __shfl_xor_sync(kFull, di, o);
+        }
+        if (lane == 0) {
+            if (base < end) {
+                col[base] = (int32_t)row;
+                val[base] = make_double2(dr, di);
+                val32[base] = make_float2((float)dr, (float)di);
+            }
+            if (pos != end) ++nbad;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nbad += __shfl_xor_sync(kFull, nbad, o);
+    if (lane == 0 && nbad) atomicAdd(bad, nbad);
+}
+
+template <typename R> struct SpVal;
+template <> struct SpVal<double> { using T = double2; };
+template <> struct SpVal<float> { using T = float2; };
+
+template <typename R>
+__global__ void __launch_bounds__(kWarps * 32)
+k_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, const typename SpVal<R>::T* __restrict__ val,
+       const typename SpVal<R>::T* __restrict__ x, typename SpVal<R>::T* __restrict__ y, int64_t rows) {
+    using C2 = typename SpVal<R>::T;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const int64_t b = __ldg(row_ptr + row), e = __ldg(row_ptr + row + 1);
+        R ar = 0, ai = 0;
+        int64_t p = b + lane;
+        for (; p + 96 < e; p += 128) {      // four entries per lane in flight
+            int c[4];
+            C2 v[4], xv[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                c[q] = __ldg(col + p + 32 * q);
+                v[q] = __ldg(val + p + 32 * q);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) xv[q] = __ldg(x + c[q]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                ar += v[q].x * xv[q].x - v[q].y * xv[q].y;
+                ai += v[q].x * xv[q].y + v[q].y * xv[q].x;
+            }
+        }
+        for (; p < e; p += 32) {
+            const int c = __ldg(col + p);
+            const C2 v = __ldg(val + p), xv = __ldg(x + c);
+            ar += v.x * xv.x - v.y * xv.y;
+            ai += v.x * xv.y + v.y * xv.x;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ar += __shfl_xor_sync(kFull, ar, o);
+            ai += __shfl_xor_sync(kFull, ai, o);
+        }
+        if (lane == 0) {
+            C2 out;
+            out.x = ar;
+            out.y = ai;
+            y[row] = out;
+        }
+    }
+}
+
+int spmv_grid(int64_t rows) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    int64_t need = (rows + kWarps - 1) / kWarps;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * 8));   // 8 blocks of 8 warps per SM
+}
+
+}  // namespace
+
+int64_t sparse_bytes_per_entry() { return 4 + 16 + 8; }
+
+void build_sparse(momed_handle* h, double u) {
+    SparseMatrix& sp = h->sparse;
+    sp.release();
+    const int64_t n = h->n;
+    cudaStream_t st = h->stream;
+    MOMED_REQUIRE(n <= (int64_t)INT32_MAX, MOMED_EINVAL, "sparse method: basis larger than 2^31-1 states");
+    const IndexView iv = index_view(h);
+    const OpView ov = h->op.view();
+
+    DevBuf<int32_t> counts;
+    counts.resize(std::max<int64_t>(n, 1));
+    k_sparse_count<<<persistent_grid(k_sparse_count, n), kWarps * 32, 0, st>>>(iv, ov, counts.p, n);
+    MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
+    std::vector<int32_t> hc(n);
+    MOMED_CUDA_TRY(cudaMemcpyAsync(hc.data(), counts.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+    counts.release();
+    std::vector<int64_t> rp(n + 1);
+    rp[0] = 0;
+    for (int64_t i = 0; i < n; ++i) rp[i + 1] = rp[i] + hc[i];
+    const int64_t nnz = rp[n];
+
+    // admission: row pointers plus column, FP64 value and FP32 value per entry
+    const int64_t need = (n + 1) * 8 + nnz * sparse_bytes_per_entry();
+    size_t free_b = 0, total_b = 0;
+    MOMED_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    int64_t limit = (int64_t)(0.9 * (double)free_b);
+    if (h->hbm_budget > 0) limit = std::min<int64_t>(limit, h->hbm_budget);
+    if (need > limit)
+        throw Error{MOMED_ENOMEM, "sparse method: the matrix needs " + std::to_string(need) + " bytes, " +
+                                     std::to_string(limit) + " available"};
+
+    sp.row_ptr.resize(n + 1);
+    sp.col.resize(std::max<int64_t>(nnz, 1));
+    sp.val.resize(std::max<int64_t>(nnz, 1));
+    sp.val32.resize(std::max<int64_t>(nnz, 1));
+    MOMED_CUDA_TRY(cudaMemcpyAsync(sp.row_ptr.p, rp.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st));
+    h->counters.resize(16);
+    MOMED_CUDA_TRY(cudaMemsetAsync(h->counters.p + 3, 0, sizeof(unsigned long long), st));
+    DevBuf<double> ud;
+    const bool hb = h->op.has_b;
+    if (hb) {
+        ud.resize(1);
+        MOMED_CUDA_TRY(cudaMemcpyAsync(ud.p, &u, sizeof(u), cudaMemcpyHostToDevice, st));
+        auto k = k_sparse_fill<true>;
+        k<<<persistent_grid(k, n), kWarps * 32, 0, st>>>(iv, ov, ud.p, sp.row_ptr.p, sp.col.p, sp.val.p, sp.val32.p,
+                                                          n, h->counters.p + 3);
+    } else {
+        auto k = k_sparse_fill<false>;
+        k<<<persistent_grid(k, n), kWarps * 32, 0, st>>>(iv, ov, nullptr, sp.row_ptr.p, sp.col.p, sp.val.p, sp.val32.p,
+                                                          n, h->counters.p + 3);
+    }
+    MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
+    unsigned long long bad = 0;
+    MOMED_CUDA_TRY(cudaMemcpyAsync(&bad, h->counters.p + 3, sizeof(bad), cudaMemcpyDeviceToHost, st));
+    MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+    if (bad != 0) {
+        sp.release();
+        throw Error{MOMED_EINVAL, "sparse method: count and fill passes disagree on " + std::to_string(bad) + " rows"};
+    }
+    sp.nnz = nnz;
+    sp.u = u;
+    sp.built = true;
+}
+
+void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int64_t rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    k_spmv<double><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val.p, x, y, rows);
+    MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
+}
+
+void launch_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, int64_t rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    k_spmv<float><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val32.p, x, y, rows);
+    MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
+}
+
+}  // namespace momed

@@ -158,7 +158,10 @@ __global__ void k_decide(const double2* coefA, int ncols, const double2* partial
     if (threadIdx.x != 0) return;
     double before = coefA[ncols].x;
     scal[1] = after;
-    *flag = (after < 0.5 * before) ? 1 : 0;
+    // second pass when the first removed more than 1 - 0.1 of the squared norm (|w'| < 0.32 |w|);
+    // the classical 1/2 flags nearly every Lanczos step (w = H v carries alpha and beta along the
+    // two newest columns) without changing the eigenpairs
+    *flag = (after < 0.1 * before) ? 1 : 0;
 }
 
 __global__ void k_finalize(const double2* coefA, const double2* coefB, int ncols, const double2* partial2, int grid,

@@ -10,7 +10,8 @@ from ._lib import Handle, MomedError, NotConverged, Server, version
 from .core import (MBS64, HilbertSubspace, MBOperator, MBS64Vector, Scatter, ScatterList, hermitian_complete,
                    index_fit, make_mask64, occ_list, parity_mask, scat_occ_number, sort_merge_scatlist)
 from .methods import (DEFAULT_GPU, GPU_AVAILABLE, EDsolve, LinearMap, activate_b200, activate_gpu_device,
-                      create_gpu_linearmap, krylov_map_solve, release_gpu_memory)
+                      create_gpu_linearmap, create_gpu_matrix, krylov_map_solve, krylov_matrix_solve,
+                      release_gpu_memory)
 from .preparation import (ED_momentum_subspaces, ED_scatterlist_onebody, ED_scatterlist_twobody,
                           ED_sortedScatterList_onebody, ED_sortedScatterList_twobody, EDPara, MBS_totalmomentum,
                           group_momentum_pairs, momentum_residue)
@@ -20,7 +21,7 @@ __all__ = [
     "MBS64", "HilbertSubspace", "MBOperator", "MBS64Vector", "Scatter", "ScatterList", "hermitian_complete",
     "index_fit", "make_mask64", "occ_list", "parity_mask", "scat_occ_number", "sort_merge_scatlist",
     "DEFAULT_GPU", "GPU_AVAILABLE", "EDsolve", "LinearMap", "activate_b200", "activate_gpu_device",
-    "create_gpu_linearmap", "krylov_map_solve", "release_gpu_memory",
+    "create_gpu_linearmap", "create_gpu_matrix", "krylov_map_solve", "krylov_matrix_solve", "release_gpu_memory",
     "ED_momentum_subspaces", "ED_scatterlist_onebody", "ED_scatterlist_twobody", "ED_sortedScatterList_onebody",
     "ED_sortedScatterList_twobody", "EDPara", "MBS_totalmomentum", "group_momentum_pairs", "momentum_residue",
 ]

@@ -71,6 +71,9 @@ SIGNATURES = {
                                  C.POINTER(Info)]),
     "momed_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_int32, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(Info)]),
+    "momed_build_sparse": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "momed_sparse_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "momed_release_sparse": (C.c_int, [C.c_void_p]),
     "momed_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "momed_last_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "momed_kernel_launches": (C.c_int64, []),
@@ -92,7 +95,8 @@ SIGNATURES.update({
     "momed_serve_stop": (C.c_int, [C.c_void_p]),
 })
 
-KERNEL_MATVEC_C128, KERNEL_MATVEC_C64, KERNEL_BLOCK_MATVEC_C64, KERNEL_BLOCK_MATVEC_C128 = range(4)
+(KERNEL_MATVEC_C128, KERNEL_MATVEC_C64, KERNEL_BLOCK_MATVEC_C64, KERNEL_BLOCK_MATVEC_C128, KERNEL_SPMV_C128,
+ KERNEL_SPMV_C64) = range(6)
 QUEUED, RUNNING, DONE, FAILED, CANCELLED = range(5)
 
 
@@ -287,6 +291,10 @@ class Handle:
     def set_param(self, u: float):
         self._check(lib().momed_set_param(self._h, float(u)))
 
+    def set_hbm_budget(self, nbytes: int):
+        """Device-memory limit for this handle's admissions (0 = free memory)."""
+        self._check(lib().momed_set_hbm_budget(self._h, int(nbytes)))
+
     # ---------------------------------------------------------------- compute
     def matvec(self, x: np.ndarray) -> np.ndarray:
         """y = H x with host arrays (complex128 or complex64)."""
@@ -312,6 +320,30 @@ class Handle:
         n, ms = C.c_int64(), C.c_double()
         self._check(lib().momed_profile_read(self._h, kind, C.byref(n), C.byref(ms)))
         return n.value, ms.value
+
+    # ---------------------------------------------------------------- sparse method
+    def build_sparse(self) -> int:
+        """CSR matrix of the working operator (at the current u) on the device; maps and
+        eigsolve use it until the basis, operator or u changes.  Returns the stored entries."""
+        nnz = C.c_int64()
+        self._check(lib().momed_build_sparse(self._h, C.byref(nnz)))
+        self._sparse_nnz = nnz.value
+        return nnz.value
+
+    def sparse_copy(self):
+        """(row_ptr int64[n + 1], col int32[nnz], val complex128[nnz]) of the built matrix."""
+        nnz = getattr(self, "_sparse_nnz", None)
+        if nnz is None:
+            raise MomedError(ESTATE, "no sparse matrix (build_sparse)")
+        rp = np.empty(self.n + 1, np.int64)
+        col = np.empty(max(nnz, 1), np.int32)
+        val = np.empty(max(nnz, 1), np.complex128)
+        self._check(lib().momed_sparse_copy(self._h, _p(rp), _p(col), _p(val)))
+        return rp, col[:nnz], val[:nnz]
+
+    def release_sparse(self):
+        self._check(lib().momed_release_sparse(self._h))
+        self._sparse_nnz = None
 
     def stats(self):
         nnz, mode, tb = C.c_int64(), C.c_int32(), C.c_int64()

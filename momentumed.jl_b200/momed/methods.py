@@ -4,7 +4,9 @@
   - GPU plugin hooks ........ MomentumED/src/method/gpu_interface.jl:13-94
       GPU_AVAILABLE, DEFAULT_GPU, activate_gpu_device, create_gpu_linearmap,
       krylov_map_solve, release_gpu_memory
-  - ``EDsolve`` ............. MomentumED/src/MomentumED.jl:375-480 (method=:map, device=:gpu)
+  - ``EDsolve`` ............. MomentumED/src/MomentumED.jl:375-480 (method=:map or :sparse, device=:gpu)
+  - sparse method ........... create_gpu_matrix / krylov_matrix_solve (MomentumEDCUDAExt.jl:145-200), the
+                              matrix built on the device instead of by sparse_matrix.jl:64-190
 
 The device map computes H x (the CPU LinearMap semantics, linear_map.jl:100-118);
 the reference's KernelAbstractions kernel computes conj(H) x, so its eigenvectors
@@ -130,6 +132,46 @@ def krylov_map_solve(H: B200LinearMap, N_eigen: int, *, ishermitian: bool = True
     return vals, [vecs[i] for i in range(len(vals))], info
 
 
+class B200SparseMatrix:
+    """The device CSR matrix of the sparse method (the role of the CuSparseMatrixCSR that
+    create_gpu_matrix uploads, MomentumEDCUDAExt.jl:145-152).  The reference builds the matrix on
+    host threads (ED_HamiltonianMatrix_threaded_CSCdirect, sparse_matrix.jl:64-190) and uploads
+    it; here it is built on the device from the same Hermitian-completed term list."""
+
+    def __init__(self, A: LinearMap, device: int = 0):
+        self._map = B200LinearMap(A, device)
+        self.handle = self._map.handle
+        self.space = A.space
+        self.element_type = A.element_type
+        self.nnz = self.handle.build_sparse()
+
+    @property
+    def size(self):
+        n = len(self.space)
+        return (n, n)
+
+    def __call__(self, x, y=None):
+        return self._map(x, y)           # the handle multiplies by the CSR matrix while it is built
+
+    def to_host(self):
+        """(row_ptr, col, val) of the CSR matrix: row i lists the diagonal first, then one entry
+        per off-diagonal (row, term) hit."""
+        return self.handle.sparse_copy()
+
+    def release(self):
+        self.handle.close()
+
+
+def create_gpu_matrix(A: LinearMap, device: str = "b200") -> B200SparseMatrix:
+    return B200SparseMatrix(A)
+
+
+def krylov_matrix_solve(H: B200SparseMatrix, N_eigen: int, **kw):
+    """Lowest N_eigen eigenpairs (:SR) of the device CSR matrix (krylov_matrix_solve,
+    MomentumEDCUDAExt.jl:180-200); same keywords and results as krylov_map_solve."""
+    return krylov_map_solve(H, N_eigen, **kw)
+
+
 def release_gpu_memory(device: str = "b200", level: int = 2):
     """Device buffers belong to handles and are freed when a handle closes; nothing to collect."""
     return None
@@ -138,7 +180,8 @@ def release_gpu_memory(device: str = "b200", level: int = 2):
 def EDsolve(subspace: HilbertSubspace, Hamiltonian: MBOperator, *, N: int, method: str = "map",
             device: str = "gpu", showtime: bool = False, ishermitian: bool = True, element_type=None,
             index_type=np.int32, map_warning_dim: int = 20000, method_info: bool = True, **krylovkit_kwargs):
-    """Lowest N eigenpairs of ``Hamiltonian`` in ``subspace`` (MomentumED.jl:375-480, :map on the GPU).
+    """Lowest N eigenpairs of ``Hamiltonian`` in ``subspace`` (MomentumED.jl:375-480, :map or :sparse
+    on the GPU).
 
     Returns ``(energies, vectors)`` with ``vectors`` a list of ``MBS64Vector``.
     ``krylovkit_kwargs`` accepts krylovdim, tol, maxiter, vec0, seed and precision ("fp64"/"mixed").
@@ -156,10 +199,10 @@ def EDsolve(subspace: HilbertSubspace, Hamiltonian: MBOperator, *, N: int, metho
         raise AssertionError(f"Unknown device: {device}.")
     if ishermitian and not Hamiltonian.isupper():
         raise AssertionError("Use upper_hermitian form of Hamiltonian operator when ishermitian = true.")
-    if method != "map" or device == "cpu":
-        raise NotImplementedError("this backend provides method=:map on the GPU; the sparse/dense and CPU "
-                                  "paths stay in the reference")
-    if len(subspace) < map_warning_dim and method_info:
+    if method == "dense" or device == "cpu":
+        raise NotImplementedError("this backend provides method=:map and method=:sparse on the GPU; the dense "
+                                  "and CPU paths stay in the reference")
+    if method == "map" and len(subspace) < map_warning_dim and method_info:
         warnings.warn(f"Linear map may be slow for dim={len(subspace)}. Consider using :sparse method.")
     if device == "gpu":
         if DEFAULT_GPU[0] == "nogpu":
@@ -172,9 +215,14 @@ def EDsolve(subspace: HilbertSubspace, Hamiltonian: MBOperator, *, N: int, metho
     _throw_gpu_unavailable(device)
     t0 = time.perf_counter()
     H_map = LinearMap(Hamiltonian, subspace)
-    H_gpu = create_gpu_linearmap(H_map, device)
+    if method == "sparse":
+        H_gpu = create_gpu_matrix(H_map, device)
+        solve = krylov_matrix_solve
+    else:
+        H_gpu = create_gpu_linearmap(H_map, device)
+        solve = krylov_map_solve
     try:
-        vals, vecs, info = krylov_map_solve(H_gpu, N, ishermitian=ishermitian, **krylovkit_kwargs)
+        vals, vecs, info = solve(H_gpu, N, ishermitian=ishermitian, **krylovkit_kwargs)
     finally:
         H_gpu.release()
     if showtime:

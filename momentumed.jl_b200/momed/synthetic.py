@@ -113,6 +113,7 @@ def mesh_para(a: int, b: int, seed: int, Nc_mix: int = 1, Nc_conserve: int = 1, 
 WORKLOADS = {
     "plain_3x5": dict(a=3, b=5, N_each=(5,), nev=10, seed=0, Nc_conserve=1),
     "plain_3x10": dict(a=3, b=10, N_each=(10,), nev=6, seed=1, Nc_conserve=1, krylovdim=64),
+    "plain_3x9": dict(a=3, b=9, N_each=(9,), nev=4, seed=2, Nc_conserve=1),
     "batch_3x9": dict(a=3, b=9, N_each=(9,), nev=4, seed=2, Nc_conserve=1, n_u=32, u_range=(0.5, 2.0)),
     "two_comp_4x6": dict(a=4, b=6, N_each=(4, 4), nev=8, seed=3, Nc_conserve=2),
 }

@@ -939,6 +939,66 @@ OR_API void or_dense_hamiltonian(const uint64_t* basis, int64_t N, const or_scat
     }
 }
 
+/* The sparse method's matrix: ED_HamiltonianMatrix_threaded_CSCdirect
+ * (MomentumED/src/method/sparse_matrix.jl:64-190) with the Hermitian-completed list
+ * (the else branch, 117-124): column j is the input state basis[j]; every term with
+ * in within it gives (scat * mbs_in, multiplication.jl:55-69) an output state, dropped
+ * when index_fit fails (hilbert_subspace.jl:67-72) or the amplitude is zero; the column's
+ * (row, value) pairs are sorted by row and duplicates summed (141-156).  0-based CSC:
+ * colptr[N + 1]; rowval / nzval (interleaved complex) hold at most cap entries.  Returns
+ * the entries (more than cap: only the count is exact). */
+OR_API int64_t or_sparse_csc(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat,
+                             int64_t* colptr, int64_t* rowval, double* nzval, int64_t cap) {
+    typedef struct { int64_t i; double re, im; } entry;
+    entry* buf = (entry*)malloc((size_t)(nscat > 0 ? nscat : 1) * sizeof(entry));
+    int64_t nnz = 0;
+    colptr[0] = 0;
+    for (int64_t j = 0; j < N; ++j) {
+        const uint64_t st = basis[j];
+        int64_t nb = 0;
+        for (int64_t s = 0; s < nscat; ++s) {
+            const or_scat* sc = &list[s];
+            if ((st & sc->in) != sc->in) continue;
+            uint64_t tgt;
+            double re, im;
+            if (sc->in == sc->out) { tgt = st; re = sc->re; im = sc->im; }
+            else {
+                uint64_t mid = st & ~sc->in;
+                if ((mid & sc->out) != 0) continue;
+                tgt = mid | sc->out;
+                int sign = 1 - 2 * (__builtin_popcountll(mid & sc->pm) & 1);
+                re = sign * sc->re; im = sign * sc->im;
+            }
+            if (re == 0.0 && im == 0.0) continue;
+            int64_t i = searchsortedfirst(basis, N, tgt);
+            if (i >= N || basis[i] != tgt) continue;
+            buf[nb].i = i; buf[nb].re = re; buf[nb].im = im;
+            ++nb;
+        }
+        /* a stable sort keeps the list order among equal rows, so the sums below are formed
+         * in the same order as the reference's accumulation */
+        for (int64_t a = 1; a < nb; ++a) {
+            entry e = buf[a];
+            int64_t b = a - 1;
+            while (b >= 0 && buf[b].i > e.i) { buf[b + 1] = buf[b]; --b; }
+            buf[b + 1] = e;
+        }
+        int64_t k = 0;
+        while (k < nb) {
+            int64_t i = buf[k].i;
+            double re = buf[k].re, im = buf[k].im;
+            int64_t q = k + 1;
+            while (q < nb && buf[q].i == i) { re += buf[q].re; im += buf[q].im; ++q; }
+            if (nnz < cap) { rowval[nnz] = i; nzval[2 * nnz] = re; nzval[2 * nnz + 1] = im; }
+            ++nnz;
+            k = q;
+        }
+        colptr[j + 1] = nnz;
+    }
+    free(buf);
+    return nnz;
+}
+
 /* Exact nonzero count of the gather (row, term) hits, the nnz of the roofline formula. */
 OR_API int64_t or_count_hits(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat, int nthreads) {
 #ifdef _OPENMP

@@ -108,6 +108,9 @@ def lib():
         L.or_matvec_c128.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]
         L.or_matvec_c64.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]
         L.or_dense_hamiltonian.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
+        L.or_sparse_csc.restype = C.c_int64
+        L.or_sparse_csc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.c_int64]
         L.or_count_hits.restype = C.c_int64
         L.or_count_hits.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int]
         L.or_symeig.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -379,6 +382,21 @@ def dense_hamiltonian(basis: np.ndarray, full_list: np.ndarray) -> np.ndarray:
     H = np.zeros((len(basis), len(basis)), np.complex128)
     lib().or_dense_hamiltonian(_ptr(basis), len(basis), _ptr(full_list), len(full_list), _ptr(H))
     return H
+
+
+def sparse_csc(basis: np.ndarray, full_list: np.ndarray):
+    """The sparse method's matrix (sparse_matrix.jl:64-190): 0-based CSC (colptr, rowval, nzval)
+    with rows sorted inside each column and duplicates summed."""
+    basis = np.ascontiguousarray(basis, np.uint64)
+    full_list = np.ascontiguousarray(full_list, SCAT_DTYPE)
+    N = len(basis)
+    colptr = np.zeros(N + 1, np.int64)
+    nnz = lib().or_sparse_csc(_ptr(basis), N, _ptr(full_list), len(full_list), _ptr(colptr), None, None, 0)
+    rowval = np.zeros(max(nnz, 1), np.int64)
+    nzval = np.zeros(max(nnz, 1), np.complex128)
+    lib().or_sparse_csc(_ptr(basis), N, _ptr(full_list), len(full_list), _ptr(colptr), _ptr(rowval), _ptr(nzval),
+                        nnz)
+    return colptr, rowval[:nnz], nzval[:nnz]
 
 
 def count_hits(basis: np.ndarray, full_list: np.ndarray, nthreads: int = 0) -> int:

@@ -160,3 +160,22 @@ def test_parity_mask_julia_shift_semantics():
     assert O.parity_mask(1 << 63) == 0
     assert O.parity_mask((1 << 1) | (1 << 5)) == 0b011100
     assert O.parity_mask(0) == 0
+
+
+def test_sparse_csc_restatement_matches_dense():
+    """The oracle's restatement of the sparse method's matrix builder (sparse_matrix.jl:64-190)
+    against its row-oriented dense builder: same matrix, rows sorted and unique per column."""
+    S = O.Synth(3, 5, 0)
+    full = O.hermitian_complete(O.sort_merge(np.concatenate([S.onebody(), S.twobody()])))
+    sectors, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    for basis in sectors[::5]:
+        cp, rv, nz = O.sparse_csc(basis, full)
+        D = O.dense_hamiltonian(basis, full)
+        N = len(basis)
+        M = np.zeros((N, N), np.complex128)
+        for j in range(N):
+            seg = rv[cp[j]:cp[j + 1]]
+            assert np.all(np.diff(seg) > 0)
+            M[seg, j] = nz[cp[j]:cp[j + 1]]
+        assert np.array_equal(M, D)
+        assert len(nz) == np.count_nonzero(D)
