@@ -71,6 +71,8 @@ def parse():
                     choices=["batch_3x9", "plain_3x5", "plain_3x9", "plain_3x10", "two_comp_4x6"],
                     help="batch_3x9 (the headline); the others time plain single-vector solves")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving stream")
+    ap.add_argument("--sparse-batch", type=int, default=1,
+                    help="also time the headline sweep on the sparse method (1) or not (0)")
     ap.add_argument("--method", default="map", choices=["map", "sparse"],
                     help="plain workloads: matrix-free map, or the sparse method (device-built CSR + SpMV)")
     ap.add_argument("--serve-requests", type=int, default=80)
@@ -298,27 +300,34 @@ def serve_bench(args, device: int):
     def pct(x, q):
         return float(np.percentile(np.asarray(x), q)) if len(x) else None
 
-    # plain: one request at a time, FP64 single-vector Lanczos, live against arrivals
-    plain_vals, plain_lat, plain_service = [], [], []
-    cur = None
-    t0 = time.perf_counter()
-    for r in reqs:
-        now = time.perf_counter() - t0
-        if now < r["arrival"]:
-            time.sleep(r["arrival"] - now)
-        s0 = time.perf_counter()
-        if cur != r["mesh"]:
-            h.set_scatter_pair(*ops[r["mesh"]])
-            cur = r["mesh"]
-        h.set_basis(sectors[r["mesh"]][r["sector"]])
-        h.set_param(r["u"])
-        v, _, _, _ = h.eigsolve(r["nev"], krylovdim=serve_krylovdim(r["nev"]), tol=r["tol"], maxiter=300,
-                                want_vectors=False, precision=_lib.PREC_FP64)
-        s1 = time.perf_counter()
-        plain_vals.append(v)
-        plain_service.append(s1 - s0)
-        plain_lat.append(s1 - t0 - r["arrival"])
-    plain_span = time.perf_counter() - t0
+    # plain: one request at a time, FP64 single-vector Lanczos, live against arrivals; once with
+    # the matrix-free map and once with the sparse method (the matrix built for each request)
+    def run_plain(sparse):
+        vals_, lat_, service_ = [], [], []
+        cur = None
+        t0 = time.perf_counter()
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if now < r["arrival"]:
+                time.sleep(r["arrival"] - now)
+            s0 = time.perf_counter()
+            if cur != r["mesh"]:
+                h.set_scatter_pair(*ops[r["mesh"]])
+                cur = r["mesh"]
+            h.set_basis(sectors[r["mesh"]][r["sector"]])
+            h.set_param(r["u"])
+            if sparse:
+                h.build_sparse()
+            v, _, _, _ = h.eigsolve(r["nev"], krylovdim=serve_krylovdim(r["nev"]), tol=r["tol"], maxiter=300,
+                                    want_vectors=False, precision=_lib.PREC_FP64)
+            s1 = time.perf_counter()
+            vals_.append(v)
+            service_.append(s1 - s0)
+            lat_.append(s1 - t0 - r["arrival"])
+        return vals_, lat_, service_, time.perf_counter() - t0
+
+    plain_vals, plain_lat, plain_service, plain_span = run_plain(False)
+    sp_vals, sp_lat, sp_service, sp_span = run_plain(True)
     h.close()
 
     def run_server():
@@ -366,12 +375,22 @@ def serve_bench(args, device: int):
                    "slowest_solves": [{"mesh": k[0], "nev": v, "device_s": round(k[3], 3), "matvecs": k[2]}
                                       for k, v in slow],
                    "precision": "mixed requests: batched mixed solver for groups on one sector, FP64 "
-                                "single-vector solver for a request alone",
+                                "single-vector solver for a request alone (sparse method when its "
+                                "matrix fits the budget)",
                    "all_converged": bool(all(s_conv)), "max_rel_eig_err_vs_plain_fp64": max(errs)},
         "plain_one_at_a_time": {"solves_per_s": n / plain_span, "latency_ms_p50": 1e3 * pct(plain_lat, 50),
                                 "latency_ms_p99": 1e3 * pct(plain_lat, 99),
-                                "service_ms_p50": 1e3 * pct(plain_service, 50), "precision": "fp64"},
+                                "service_ms_p50": 1e3 * pct(plain_service, 50), "precision": "fp64",
+                                "method": "map"},
+        "plain_sparse_one_at_a_time": {"solves_per_s": n / sp_span, "latency_ms_p50": 1e3 * pct(sp_lat, 50),
+                                       "latency_ms_p99": 1e3 * pct(sp_lat, 99),
+                                       "service_ms_p50": 1e3 * pct(sp_service, 50), "precision": "fp64",
+                                       "method": "sparse (matrix built per request)",
+                                       "max_rel_eig_err_vs_map": max(
+                                           float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0)))
+                                           for a, b in zip(sp_vals, plain_vals))},
         "speedup_served_vs_plain": (n / s_span) / (n / plain_span),
+        "speedup_served_vs_plain_sparse": (n / s_span) / (n / sp_span),
     }
 
 
@@ -714,6 +733,38 @@ def main():
                  "sample": f"{len(picks)} U0 values on each of the {len(all_vals)} timed sectors",
                  "max_rel_eig_err_batched_vs_fp64": max(errs)}
 
+    # ---------------------------------------------------------------- the same sweep on the sparse method
+    # (each step builds the sector's CSR entries with A and B parts, then the batched solver runs its
+    # FP32 maps as a block SpMV over them; reported beside the map-based headline, not as it)
+    sparse_batched = None
+    if rank == 0 and world == 1 and args.sparse_batch:
+        h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+
+        def step_sparse(sidx):
+            h.select_sector(sidx, len(sectors[sidx][1]))
+            h.build_sparse()
+            return h.batch_solve(u, NEV, krylovdim=KRYLOV, tol=1e-12, precision=_lib.PREC_MIXED)
+
+        step_sparse(order[0])                              # warm-up
+        h.profile(True)
+        sev = [torch.cuda.Event(enable_timing=True) for _ in range(K + 1)]
+        errs = []
+        torch.cuda.synchronize()
+        sev[0].record(stream)
+        for i, (sidx, bvals, _) in enumerate(all_vals):
+            sv, _, _, _ = step_sparse(sidx)
+            sev[i + 1].record(stream)
+            errs.append(float(np.max(np.abs(sv - bvals) / np.maximum(np.abs(bvals), 1.0))))
+        torch.cuda.synchronize()
+        sms = [sev[i].elapsed_time(sev[i + 1]) for i in range(K)]
+        n_bsp, ms_bsp = h.profile_read(_lib.KERNEL_BLOCK_SPMV_C64)
+        h.profile(False)
+        h.release_sparse()
+        sparse_batched = {"solves_per_s": 1e3 * K * NU / sum(sms), "ms_per_step": sum(sms) / K,
+                          "block_spmv_launches": n_bsp, "block_spmv_avg_ms": ms_bsp / max(n_bsp, 1),
+                          "max_rel_eig_err_vs_map_batched": max(errs),
+                          "note": "build of the sector's entries inside each step; same sectors and U0 grid"}
+
     # ---------------------------------------------------------------- CPU baseline (rank 0, N = 1)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -754,6 +805,7 @@ def main():
                            "per_solve_p99": float(np.percentile(lat, 99))},
             "plain_gpu_lanczos": plain,
             "speedup_vs_plain": (value / world) / plain["solves_per_s"] if plain else None,
+            "sparse_method_batched": sparse_batched,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": MV_DRAM_BYTES, "peak_source": peak_src,
                          "kernel": "block matvec c64 x32 (k_block_matvec_v<float, 32>)",

@@ -153,8 +153,10 @@ MOMED_API int  momed_batch_solve(momed_handle* h, const momed_solve_opts* opts, 
  * state, entry row_ptr[i] is the diagonal, then one entry per off-diagonal (row, term) hit
  * (a pair reached by two terms keeps two entries).  While it is built, momed_matvec and
  * momed_eigsolve use the CSR SpMV instead of the matrix-free map; a new basis, operator or u
- * drops it, as does momed_release_sparse (momed_batch_solve always uses the map).  nnz
- * receives the stored entries; the matrix takes 8 (N + 1) + 28 nnz bytes and MOMED_ENOMEM is
+ * drops it, as does momed_release_sparse.  momed_batch_solve then runs its FP32 maps as a
+ * block SpMV over the same entries (values A + u B per right-hand side; its FP64 maps stay
+ * matrix-free).  nnz receives the stored entries; the matrix takes 8 (N + 1) + 28 nnz bytes
+ * (44 nnz for H(u) = A + u B, which also keeps the A and B parts) and MOMED_ENOMEM is
  * returned when that exceeds the handle's budget or 90% of free device memory.
  * momed_sparse_copy copies it to host arrays row_ptr[N + 1], col[nnz], val[2 nnz] (c128);
  * any of them may be NULL. */
@@ -174,9 +176,11 @@ MOMED_API int  momed_last_kernel_ms(momed_handle* h, double* ms);
  * runs one EDsolve at a time).  `slots` worker contexts, each with its own stream, take
  * queued requests in arrival order as soon as a slot is free and the request's HBM estimate
  * fits the budget (0 = 85% of free memory); admitted solves run concurrently on the device.
- * Queued requests on the same operator, sector basis and precision are solved together as one
- * batched solve (3 to 32 of them, one right-hand side per u); a request alone runs the FP64
- * single-vector solver; requests of at least 131072 states run one at a time.
+ * Queued mixed-precision requests (nev <= 12) on the same operator and sector basis are solved
+ * together as one batched solve (3 to 32 of them, one right-hand side per u); any other request
+ * runs alone on the FP64 single-vector solver.  A solve of at least 4096 states uses the sparse
+ * method (momed_build_sparse) when its matrix fits what the budget has left; requests of at
+ * least 131072 states run one at a time.
  * Requests larger than the budget fail at once with MOMED_ENOMEM.  poll waits at most
  * wait_ms and returns MOMED_ETIMEOUT when the request is still queued or running;
  * status: 0 queued, 1 running, 2 done, 3 failed (return code is the failure's), 4 cancelled. */
@@ -207,6 +211,7 @@ MOMED_API int64_t momed_kernel_launches(void);
 #define MOMED_KERNEL_BLOCK_MATVEC_C128  3
 #define MOMED_KERNEL_SPMV_C128          4
 #define MOMED_KERNEL_SPMV_C64           5
+#define MOMED_KERNEL_BLOCK_SPMV_C64     6
 MOMED_API int  momed_profile(momed_handle* h, int32_t enable);
 MOMED_API int  momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms);
 

@@ -51,7 +51,7 @@ void prof_end(momed_handle* h, int kind) {
     if (!h->prof) return;
     h->prof_kind[(h->prof_used - 1) / 2] = kind;
     MOMED_CUDA_TRY(cudaEventRecord(h->prof_ev[h->prof_used++], h->stream));
-    if (kind >= 0 && kind < 6) ++h->prof_launches[kind];
+    if (kind >= 0 && kind < 7) ++h->prof_launches[kind];
 }
 
 OpView Operator::view() const {
@@ -570,14 +570,14 @@ int momed_profile(momed_handle* h, int32_t enable) {
     return guarded(h, [&]() {
         MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
         h->prof_used = 0;
-        for (int k = 0; k < 6; ++k) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; }
+        for (int k = 0; k < 7; ++k) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; }
         h->prof = enable != 0;
         return MOMED_OK;
     });
 }
 
 int momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms) {
-    if (!h || kind < 0 || kind > 5) return MOMED_EINVAL;
+    if (!h || kind < 0 || kind > 6) return MOMED_EINVAL;
     return guarded(h, [&]() {
         prof_drain(h);
         if (launches) *launches = h->prof_launches[kind];

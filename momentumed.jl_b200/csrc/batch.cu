@@ -393,6 +393,11 @@ template <typename VT> struct BlockMv;
 template <> struct BlockMv<float2> {
     static void run(momed_handle* h, const float2* x, float2* y, const float* u, int nb) {
         prof_begin(h);
+        if (h->sparse.built) {   // the sparse method's entries (momed_build_sparse)
+            launch_block_spmv_c64(h->sparse, x, y, h->op.has_b ? u : nullptr, nb, h->n, h->stream);
+            prof_end(h, MOMED_KERNEL_BLOCK_SPMV_C64);
+            return;
+        }
         launch_block_matvec_c64(index_view(h), h->op.view(), x, y, u, nb, h->n, h->stream);
         prof_end(h, MOMED_KERNEL_BLOCK_MATVEC_C64);
     }

@@ -170,6 +170,9 @@ struct SparseMatrix {
     DevBuf<int32_t> col;
     DevBuf<double2> val;
     DevBuf<float2> val32;
+    // the A and B parts of H(u) = A + u B per entry (c64), for the batched solver's block SpMV
+    // (parametrised operators only; a single operator's block SpMV reads val32)
+    DevBuf<float2> pa32, pb32;
     void release() {
         built = false;
         nnz = 0;
@@ -177,6 +180,8 @@ struct SparseMatrix {
         col.release();
         val.release();
         val32.release();
+        pa32.release();
+        pb32.release();
     }
 };
 
@@ -227,8 +232,8 @@ struct momed_handle {
     std::vector<cudaEvent_t> prof_ev;      // pairs (start, stop)
     std::vector<int> prof_kind;            // kind of each pair
     size_t prof_used = 0;                  // events used in the current record
-    int64_t prof_launches[6] = {0, 0, 0, 0, 0, 0};
-    double prof_ms[6] = {0, 0, 0, 0, 0, 0};      // folded-in time of pairs already read
+    int64_t prof_launches[7] = {0, 0, 0, 0, 0, 0, 0};
+    double prof_ms[7] = {0, 0, 0, 0, 0, 0, 0};      // folded-in time of pairs already read
 };
 
 namespace momed {
@@ -256,7 +261,9 @@ void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const doubl
 
 // sparse.cu: CSR build at parameter u (after ensure_ready) and the CSR SpMV
 void build_sparse(momed_handle* h, double u);
-int64_t sparse_bytes_per_entry();
+int64_t sparse_bytes_per_entry(bool pair);
+void launch_block_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, const float* u, int32_t nb,
+                           int64_t rows, cudaStream_t st);
 void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int64_t rows, cudaStream_t st);
 void launch_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, int64_t rows, cudaStream_t st);
 

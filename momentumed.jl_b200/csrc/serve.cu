@@ -9,7 +9,8 @@
 // request on the same operator, sector basis and precision (up to 32, as long as the group
 // fits the budget) and solves them as one batched solve, one right-hand side per request's
 // parameter u; the block map then evaluates each candidate term once for the whole group.  A
-// request alone runs the FP64 single-vector solver, the fastest form for one right-hand side.  A request larger than the whole budget fails at once with MOMED_ENOMEM; a request
+// request alone runs the FP64 single-vector solver, the fastest form for one right-hand side,
+// with the sparse method (a CSR matrix built on the device) when the matrix fits the budget.  A request larger than the whole budget fails at once with MOMED_ENOMEM; a request
 // can be cancelled while queued; every wait the API offers is bounded and returns
 // MOMED_ETIMEOUT when it runs out.
 //
@@ -87,8 +88,12 @@ namespace {
 constexpr int64_t kLargeRows = 1 << 17;
 // Smallest group that the batched solver serves faster per request than the single-vector solver.
 constexpr int kMinGroup = 3;
-// Largest nev for which a group takes the mixed-precision batched solver.
+// Largest nev of a request that may join a group (groups run the mixed-precision batched solver).
 constexpr int kMaxMixedNev = 12;
+// A request alone of at least this many states is solved with the sparse method when its CSR
+// matrix fits what the budget has left: the matrix costs about two maps to build and its SpMV
+// runs 3-4x faster than the map on large sectors.  Below it both are launch-bound.
+constexpr int64_t kSparseMinRows = 1 << 12;
 
 // HBM a solve needs: basis, index tables (bounded), Krylov basis, Ritz/refinement buffers.
 // nb: right-hand sides of a batched solve (a power of two), 0 for the single-vector solver.
@@ -173,11 +178,16 @@ void worker_loop(momed_server* S, int slot) {
             // continuous batching: queued requests on the same operator, sector and precision join
             // the head when the group reaches kMinGroup (smaller groups cost as much per solve as
             // the single-vector solver)
+            // Only mixed-precision requests with nev <= kMaxMixedNev form groups: an FP64 group (the
+            // block Lanczos in FP64 on the matrix-free map) took longer than its requests solved
+            // one by one with the sparse method (3x10, nev 15/8/11: 6.4 s against ~0.8 s each).
             const int64_t N = (int64_t)r->basis.size();
-            for (auto it = S->queue.begin(); it != S->queue.end() && grp.size() < 32; ++it) {
+            const bool groupable = r->opts.precision == MOMED_PREC_MIXED && r->opts.nev <= kMaxMixedNev;
+            for (auto it = S->queue.begin(); groupable && it != S->queue.end() && grp.size() < 32; ++it) {
                 const auto& q = *it;
                 const bool same = q->status == 0 && q->op == r->op && q->opts.precision == r->opts.precision &&
-                                  q->bhash == r->bhash && (int64_t)q->basis.size() == N &&
+                                  q->opts.nev <= kMaxMixedNev && q->bhash == r->bhash &&
+                                  (int64_t)q->basis.size() == N &&
                                   std::memcmp(q->basis.data(), r->basis.data(), (size_t)N * 8) == 0;
                 if (!same) continue;
                 grp.push_back(q);
@@ -231,24 +241,57 @@ void worker_loop(momed_server* S, int slot) {
             const int nev = (int)std::min<int64_t>(o.nev, N);
             gvals.assign((size_t)nu * nev, 0.0);
             gres.assign((size_t)nu * nev, 0.0);
+            const double u = r->u;
             if (nu == 1) {
-                // one right-hand side: the FP64 single-vector solver (a mixed request gets FP64
-                // arithmetic throughout, which is faster here and at least as accurate)
-                double u = r->u;
                 float uf = (float)u;
                 MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
                 MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(uf), cudaMemcpyHostToDevice, h->stream));
                 MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
-                o.precision = MOMED_PREC_FP64;
-                rc = momed_eigsolve_impl(h, &o, nullptr, gvals.data(), gres.data(), nullptr, &ginfo);
-            } else {
-                std::vector<double> us(nu);
-                for (int i = 0; i < nu; ++i) us[i] = grp[i]->u;
-                // many eigenpairs per parameter: the FP64 block Lanczos converges in fewer steps
-                // than the mixed-precision refinement
-                if (o.nev > kMaxMixedNev) o.precision = MOMED_PREC_FP64;
-                rc = momed_batch_solve_impl(h, &o, us.data(), nu, gvals.data(), gres.data(), nullptr, &ginfo);
             }
+            // the sparse method when its matrix fits what the budget has left (its bytes are held
+            // for this solve only); a group's batched solver then runs its FP32 maps as a block SpMV
+            int64_t sp_bytes = 0;
+            if (N >= kSparseMinRows) {
+                ensure_ready(h);                      // index and validation: h->nnz counts every hit
+                const int64_t need = (N + 1) * 8 + (h->nnz + N) * sparse_bytes_per_entry(h->op.has_b);
+                std::lock_guard<std::mutex> lk(S->mu);
+                if (S->used + need <= S->budget) {
+                    S->used += need;
+                    sp_bytes = need;
+                }
+            }
+            auto unreserve = [&]() {
+                h->sparse.release();
+                if (sp_bytes > 0) {
+                    std::lock_guard<std::mutex> lk(S->mu);
+                    S->used -= sp_bytes;
+                    sp_bytes = 0;
+                }
+            };
+            try {
+                if (sp_bytes > 0) {
+                    try {
+                        build_sparse(h, u);
+                    } catch (const Error& e) {
+                        if (e.code != MOMED_ENOMEM) throw;
+                        unreserve();          // the device is shorter than the budget: use the map
+                    }
+                }
+                if (nu == 1) {
+                    // one right-hand side: the FP64 single-vector solver (a mixed request gets FP64
+                    // arithmetic throughout, which is faster here and at least as accurate)
+                    o.precision = MOMED_PREC_FP64;
+                    rc = momed_eigsolve_impl(h, &o, nullptr, gvals.data(), gres.data(), nullptr, &ginfo);
+                } else {
+                    std::vector<double> us(nu);
+                    for (int i = 0; i < nu; ++i) us[i] = grp[i]->u;
+                    rc = momed_batch_solve_impl(h, &o, us.data(), nu, gvals.data(), gres.data(), nullptr, &ginfo);
+                }
+            } catch (...) {
+                unreserve();
+                throw;
+            }
+            unreserve();
             if (rc == MOMED_ENOTCONV) rc = MOMED_OK;   // results written; info.converged tells
             for (int i = 0; i < nu; ++i) {
                 const int ni = (int)std::min<int64_t>(grp[i]->opts.nev, N);

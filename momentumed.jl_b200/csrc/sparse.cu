@@ -63,11 +63,12 @@ k_sparse_count(IndexView iv, OpView ov, int32_t* __restrict__ counts, int64_t ro
 }
 
 // bad[0]: entries that fell outside their row's range (count and fill passes disagree)
+// pa32 / pb32 (HAS_B only, may be null): the A and B parts of each entry, rounded to c64
 template <bool HAS_B>
 __global__ void __launch_bounds__(kWarps * 32)
 k_sparse_fill(IndexView iv, OpView ov, const double* __restrict__ u_ptr, const int64_t* __restrict__ row_ptr,
-              int32_t* __restrict__ col, double2* __restrict__ val, float2* __restrict__ val32, int64_t rows,
-              unsigned long long* bad) {
+              int32_t* __restrict__ col, double2* __restrict__ val, float2* __restrict__ val32,
+              float2* __restrict__ pa32, float2* __restrict__ pb32, int64_t rows, unsigned long long* bad) {
     __shared__ SharedTables sh;
     __shared__ WarpScratch s_ws[kWarps];
     stage_tables(sh, iv);
@@ -80,7 +81,7 @@ k_sparse_fill(IndexView iv, OpView ov, const double* __restrict__ u_ptr, const i
         const uint64_t s = __ldg(iv.basis + row);
         const int64_t base = row_ptr[row], end = row_ptr[row + 1];
         int64_t pos = base + 1;            // warp-uniform: next free entry of the row
-        double dr = 0.0, di = 0.0;
+        double dr = 0.0, di = 0.0, dar = 0.0, dai = 0.0, dbr = 0.0, dbi = 0.0;
         for_each_group_batch(s, ov, [&](int g) {
             int total = stage_batch(g, ov, ws);
             int gi = 0;
@@ -90,17 +91,23 @@ k_sparse_fill(IndexView iv, OpView ov, const double* __restrict__ u_ptr, const i
                 int t = 0;
                 bool neg = false;
                 if (f < total) j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
-                double2 a = make_double2(0.0, 0.0);
+                double2 a = make_double2(0.0, 0.0), ta = a, tb = a;   // a = A + u B, ta = A, tb = B
                 if (j >= 0) {
-                    a = load_amp(ov.t_amp, t);
+                    ta = load_amp(ov.t_amp, t);
+                    if (neg) { ta.x = -ta.x; ta.y = -ta.y; }
+                    a = ta;
                     if (HAS_B) {
-                        double2 b = load_amp(ov.t_ampb, t);
-                        a.x += u * b.x;
-                        a.y += u * b.y;
+                        tb = load_amp(ov.t_ampb, t);
+                        if (neg) { tb.x = -tb.x; tb.y = -tb.y; }
+                        a.x += u * tb.x;
+                        a.y += u * tb.y;
                     }
-                    if (neg) { a.x = -a.x; a.y = -a.y; }
                 }
-                if (j == row) { dr += a.x; di += a.y; }
+                if (j == row) {
+                    dr += a.x; di += a.y;
+                    dar += ta.x; dai += ta.y;
+                    dbr += tb.x; dbi += tb.y;
+                }
                 const bool off = j >= 0 && j != row;
                 const unsigned m = __ballot_sync(kFull, off);
                 if (off) {
@@ -109,6 +116,10 @@ k_sparse_fill(IndexView iv, OpView ov, const double* __restrict__ u_ptr, const i
                         col[p] = (int32_t)j;
                         val[p] = a;
                         val32[p] = make_float2((float)a.x, (float)a.y);
+                        if (HAS_B && pa32) {
+                            pa32[p] = make_float2((float)ta.x, (float)ta.y);
+                            pb32[p] = make_float2((float)tb.x, (float)tb.y);
+                        }
                     } else {
                         ++nbad;
                     }
@@ -121,12 +132,22 @@ k_sparse_fill(IndexView iv, OpView ov, const double* __restrict__ u_ptr, const i
         for (int o = 16; o > 0; o >>= 1) {
             dr += __shfl_xor_sync(kFull, dr, o);
             di += __shfl_xor_sync(kFull, di, o);
+            if (HAS_B) {
+                dar += __shfl_xor_sync(kFull, dar, o);
+                dai += __shfl_xor_sync(kFull, dai, o);
+                dbr += __shfl_xor_sync(kFull, dbr, o);
+                dbi += __shfl_xor_sync(kFull, dbi, o);
+            }
         }
         if (lane == 0) {
             if (base < end) {
                 col[base] = (int32_t)row;
                 val[base] = make_double2(dr, di);
                 val32[base] = make_float2((float)dr, (float)di);
+                if (HAS_B && pa32) {
+                    pa32[base] = make_float2((float)dar, (float)dai);
+                    pb32[base] = make_float2((float)dbr, (float)dbi);
+                }
             }
             if (pos != end) ++nbad;
         }
@@ -186,6 +207,78 @@ k_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, con
     }
 }
 
+// Block SpMV for the batched solver: NB right-hand sides interleaved as x[row * NB + r], the
+// operator of right-hand side r is A + u[r] B (u null: val32 for all).  Each entry's NB values
+// are read by NB / RPL lanes, RPL = min(NB, 4) values per lane (16-byte loads), so a warp
+// iteration consumes 32 RPL / NB entries, two iterations in flight.
+template <int NB, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_block_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, const float2* __restrict__ pa,
+             const float2* __restrict__ pb, const float2* __restrict__ x, float2* __restrict__ y,
+             const float* __restrict__ u, int64_t rows) {
+    constexpr int RPL = NB < 4 ? NB : 4;
+    constexpr int LPH = NB / RPL;      // lanes per entry
+    constexpr int HPI = 32 / LPH;      // entries per warp iteration
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int hslot = lane / LPH, r0 = (lane % LPH) * RPL;
+    float ur[RPL];
+#pragma unroll
+    for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? __ldg(u + r0 + q) : 0.f;
+    auto entry = [&](int64_t p, float2* acc) {
+        const int c = __ldg(col + p);
+        const float2 a = __ldg(pa + p);
+        float2 b = make_float2(0.f, 0.f);
+        if (HAS_B) b = __ldg(pb + p);
+        float2 xv[RPL];
+        const float2* xp = x + (int64_t)c * NB + r0;
+        if constexpr (RPL == 4) {
+            const float4 v0 = __ldg(reinterpret_cast<const float4*>(xp));
+            const float4 v1 = __ldg(reinterpret_cast<const float4*>(xp) + 1);
+            xv[0] = make_float2(v0.x, v0.y);
+            xv[1] = make_float2(v0.z, v0.w);
+            xv[2] = make_float2(v1.x, v1.y);
+            xv[3] = make_float2(v1.z, v1.w);
+        } else {
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) xv[q] = __ldg(xp + q);
+        }
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            float cx = a.x, cy = a.y;
+            if (HAS_B) {
+                cx += ur[q] * b.x;
+                cy += ur[q] * b.y;
+            }
+            acc[q].x += cx * xv[q].x - cy * xv[q].y;
+            acc[q].y += cx * xv[q].y + cy * xv[q].x;
+        }
+    };
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const int64_t b0 = __ldg(row_ptr + row), e = __ldg(row_ptr + row + 1);
+        float2 acc[RPL];
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) acc[q] = make_float2(0.f, 0.f);
+        int64_t p = b0 + hslot;
+        for (; p + HPI < e; p += 2 * HPI) {
+            entry(p, acc);
+            entry(p + HPI, acc);
+        }
+        if (p < e) entry(p, acc);
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+#pragma unroll
+            for (int o = LPH; o < 32; o <<= 1) {
+                acc[q].x += __shfl_xor_sync(kFull, acc[q].x, o);
+                acc[q].y += __shfl_xor_sync(kFull, acc[q].y, o);
+            }
+        }
+        if (hslot == 0) {
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) y[row * NB + r0 + q] = acc[q];
+        }
+    }
+}
+
 int spmv_grid(int64_t rows) {
     static int sms = 0;
     if (sms == 0) {
@@ -200,7 +293,8 @@ int spmv_grid(int64_t rows) {
 
 }  // namespace
 
-int64_t sparse_bytes_per_entry() { return 4 + 16 + 8; }
+// column, FP64 value and its FP32 rounding; a parametrised operator also keeps A and B in c64
+int64_t sparse_bytes_per_entry(bool pair) { return 4 + 16 + 8 + (pair ? 16 : 0); }
 
 void build_sparse(momed_handle* h, double u) {
     SparseMatrix& sp = h->sparse;
@@ -226,7 +320,8 @@ void build_sparse(momed_handle* h, double u) {
     const int64_t nnz = rp[n];
 
     // admission: row pointers plus column, FP64 value and FP32 value per entry
-    const int64_t need = (n + 1) * 8 + nnz * sparse_bytes_per_entry();
+    const bool hb = h->op.has_b;
+    const int64_t need = (n + 1) * 8 + nnz * sparse_bytes_per_entry(hb);
     size_t free_b = 0, total_b = 0;
     MOMED_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     int64_t limit = (int64_t)(0.9 * (double)free_b);
@@ -239,21 +334,24 @@ void build_sparse(momed_handle* h, double u) {
     sp.col.resize(std::max<int64_t>(nnz, 1));
     sp.val.resize(std::max<int64_t>(nnz, 1));
     sp.val32.resize(std::max<int64_t>(nnz, 1));
+    if (hb) {
+        sp.pa32.resize(std::max<int64_t>(nnz, 1));
+        sp.pb32.resize(std::max<int64_t>(nnz, 1));
+    }
     MOMED_CUDA_TRY(cudaMemcpyAsync(sp.row_ptr.p, rp.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st));
     h->counters.resize(16);
     MOMED_CUDA_TRY(cudaMemsetAsync(h->counters.p + 3, 0, sizeof(unsigned long long), st));
     DevBuf<double> ud;
-    const bool hb = h->op.has_b;
     if (hb) {
         ud.resize(1);
         MOMED_CUDA_TRY(cudaMemcpyAsync(ud.p, &u, sizeof(u), cudaMemcpyHostToDevice, st));
         auto k = k_sparse_fill<true>;
         k<<<persistent_grid(k, n), kWarps * 32, 0, st>>>(iv, ov, ud.p, sp.row_ptr.p, sp.col.p, sp.val.p, sp.val32.p,
-                                                          n, h->counters.p + 3);
+                                                          sp.pa32.p, sp.pb32.p, n, h->counters.p + 3);
     } else {
         auto k = k_sparse_fill<false>;
         k<<<persistent_grid(k, n), kWarps * 32, 0, st>>>(iv, ov, nullptr, sp.row_ptr.p, sp.col.p, sp.val.p, sp.val32.p,
-                                                          n, h->counters.p + 3);
+                                                          nullptr, nullptr, n, h->counters.p + 3);
     }
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
@@ -279,6 +377,36 @@ void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int6
 void launch_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
     k_spmv<float><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val32.p, x, y, rows);
+    MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
+}
+
+}  // namespace momed
+
+namespace momed {
+
+void launch_block_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, const float* u, int32_t nb,
+                           int64_t rows, cudaStream_t st) {
+    if (rows <= 0) return;
+    const bool hb = u != nullptr && sp.pb32.p != nullptr;
+    const float2* pa = hb ? sp.pa32.p : sp.val32.p;
+    const int g = spmv_grid(rows);
+#define MOMED_BSP(NBV)                                                                                   \
+    case NBV:                                                                                            \
+        if (hb) k_block_spmv<NBV, true><<<g, kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, pa, sp.pb32.p, x, y, u, rows); \
+        else k_block_spmv<NBV, false><<<g, kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, pa, nullptr, x, y, nullptr, rows); \
+        break;
+    switch (nb) {
+        MOMED_BSP(1)
+        MOMED_BSP(2)
+        MOMED_BSP(4)
+        MOMED_BSP(8)
+        MOMED_BSP(16)
+        MOMED_BSP(32)
+        default:
+            throw Error{MOMED_EINVAL, "block width must be a power of two <= 32"};
+    }
+#undef MOMED_BSP
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }

@@ -96,7 +96,7 @@ SIGNATURES.update({
 })
 
 (KERNEL_MATVEC_C128, KERNEL_MATVEC_C64, KERNEL_BLOCK_MATVEC_C64, KERNEL_BLOCK_MATVEC_C128, KERNEL_SPMV_C128,
- KERNEL_SPMV_C64) = range(6)
+ KERNEL_SPMV_C64, KERNEL_BLOCK_SPMV_C64) = range(7)
 QUEUED, RUNNING, DONE, FAILED, CANCELLED = range(5)
 
 

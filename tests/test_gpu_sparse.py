@@ -187,3 +187,65 @@ def test_sparse_budget_refusal(h):
         h.set_hbm_budget(0)
     x = np.ones(len(ref[0]), np.complex128)
     assert np.all(np.isfinite(h.matvec(x)))   # the handle still maps (matrix-free)
+
+
+def test_batch_solve_on_sparse_entries_matches_map(h):
+    """The batched solver's FP32 maps as a block SpMV over the sparse method's entries (A and B
+    parts per entry): same eigenvalues as with the matrix-free block map, and LAPACK's."""
+    from momed.core import pair_operator
+    from momed.synthetic import u_grid
+    para, _ = mesh_para(3, 5, 0)
+    A = momed.MBOperator(momed.ED_scatterlist_onebody(para), upper_hermitian=True)
+    B = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=True)
+    amp_a, amp_b, in_, out, pm = pair_operator(A, B)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    basis = ref[6]
+    h.set_basis(basis)
+    h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
+    u = u_grid(8, 0.5, 2.0)
+    v_map, _, _, _ = h.batch_solve(u, 4, krylovdim=30, tol=1e-12)
+    h.build_sparse()
+    h.profile(True)
+    v_sp, vecs, res, info = h.batch_solve(u, 4, krylovdim=30, tol=1e-12, want_vectors=True)
+    n_bsp, _ = h.profile_read(momed._lib.KERNEL_BLOCK_SPMV_C64)
+    n_bmv, _ = h.profile_read(momed._lib.KERNEL_BLOCK_MATVEC_C64)
+    h.profile(False)
+    assert n_bsp > 0 and n_bmv == 0
+    assert np.max(np.abs(v_sp - v_map) / np.maximum(np.abs(v_map), 1.0)) < 1e-10
+    for q in range(len(u)):
+        w = np.linalg.eigvalsh(O.dense_hamiltonian(basis, oracle_list(amp_a + u[q] * amp_b, in_, out, pm)))
+        assert np.max(np.abs(v_sp[q] - w[:4]) / np.maximum(np.abs(w[:4]), 1.0)) < 1e-10
+    h.release_sparse()
+
+
+def test_batch_solve_on_sparse_entries_3x9_sector(h):
+    """The headline's shape (173,583 states, 32 U0 values, nev 4) on the sparse entries."""
+    from momed.core import pair_operator
+    from momed.synthetic import u_grid
+    para, _ = mesh_para(3, 9, 2)
+    A = momed.MBOperator(momed.ED_scatterlist_onebody(para), upper_hermitian=True)
+    B = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=True)
+    got = h.enumerate_basis(O.mesh_klist(3, 9), (3, 9), 1, 1, (9,), momentum_list=[(2, 5)])
+    h.set_basis(got[0][1])
+    h.set_scatter_pair(*pair_operator(A, B))
+    u = u_grid(32, 0.5, 2.0)
+    v_map, _, _, _ = h.batch_solve(u, 4, krylovdim=30, tol=1e-10)
+    h.build_sparse()
+    v_sp, _, res, info = h.batch_solve(u, 4, krylovdim=30, tol=1e-10)
+    h.release_sparse()
+    assert info["converged"] >= 4
+    assert np.max(np.abs(v_sp - v_map) / np.maximum(np.abs(v_map), 1.0)) < 1e-10
+
+
+def test_batch_solve_single_operator_on_sparse_entries(h):
+    full, ofull = full_lists(3, 5, 0)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    basis = ref[4]
+    h.set_basis(basis)
+    h.set_scatter(full.amp.astype(np.complex128), full.in_, full.out, full.pm)
+    h.build_sparse()
+    v, _, _, _ = h.batch_solve(np.array([0.3, 1.0, 2.0, 5.0]), 5, krylovdim=30, tol=1e-12)
+    h.release_sparse()
+    w = np.linalg.eigvalsh(O.dense_hamiltonian(basis, ofull))
+    for q in range(4):                                   # a single operator: every u solves H = A
+        assert np.max(np.abs(v[q] - w[:5]) / np.maximum(np.abs(w[:5]), 1.0)) < 1e-10
