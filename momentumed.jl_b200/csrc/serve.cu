@@ -71,6 +71,7 @@ struct momed_server {
     std::deque<std::shared_ptr<Request>> queue;
     std::unordered_map<int64_t, std::shared_ptr<Request>> all;
     std::vector<std::shared_ptr<const HostOperator>> ops;   // read by workers under mu
+    std::vector<double> op_hits_per_row;                    // learned from validated solves (0: none yet)
     std::vector<std::thread> workers;
     std::vector<momed_handle*> handles;
     int64_t next_id = 1;
@@ -182,7 +183,17 @@ void worker_loop(momed_server* S, int slot) {
             // block Lanczos in FP64 on the matrix-free map) took longer than its requests solved
             // one by one with the sparse method (3x10, nev 15/8/11: 6.4 s against ~0.8 s each).
             const int64_t N = (int64_t)r->basis.size();
-            const bool groupable = r->opts.precision == MOMED_PREC_MIXED && r->opts.nev <= kMaxMixedNev;
+            // A request whose sparse matrix will fit is solved alone on it: measured on the serving
+            // stream, a group of three 3x10 requests (nev 12) took 7.2 s on the batched solver and
+            // ~0.8 s each alone on the sparse method.  The matrix size comes from the hits per row
+            // that earlier solves on the operator measured.
+            bool sparse_fits = false;
+            if (N >= kSparseMinRows && opp && r->op < (int32_t)S->op_hits_per_row.size()) {
+                const double hpr = S->op_hits_per_row[r->op];
+                const int64_t sp = (N + 1) * 8 + (int64_t)((hpr + 1.0) * (double)N) * sparse_bytes_per_entry(opp->has_b);
+                sparse_fits = hpr > 0.0 && S->used + r->bytes + sp <= S->budget;
+            }
+            const bool groupable = r->opts.precision == MOMED_PREC_MIXED && r->opts.nev <= kMaxMixedNev && !sparse_fits;
             for (auto it = S->queue.begin(); groupable && it != S->queue.end() && grp.size() < 32; ++it) {
                 const auto& q = *it;
                 const bool same = q->status == 0 && q->op == r->op && q->opts.precision == r->opts.precision &&
@@ -255,6 +266,7 @@ void worker_loop(momed_server* S, int slot) {
                 ensure_ready(h);                      // index and validation: h->nnz counts every hit
                 const int64_t need = (N + 1) * 8 + (h->nnz + N) * sparse_bytes_per_entry(h->op.has_b);
                 std::lock_guard<std::mutex> lk(S->mu);
+                S->op_hits_per_row[r->op] = (double)h->nnz / (double)N;
                 if (S->used + need <= S->budget) {
                     S->used += need;
                     sp_bytes = need;
@@ -368,6 +380,7 @@ MOMED_API int momed_serve_register_operator(momed_server* S, const double* amp_a
     else op.parity.clear();
     std::lock_guard<std::mutex> lk(S->mu);
     S->ops.push_back(std::make_shared<const HostOperator>(std::move(op)));
+    S->op_hits_per_row.push_back(0.0);
     *op_id = (int32_t)S->ops.size() - 1;
     return MOMED_OK;
 }
