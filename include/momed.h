@@ -163,6 +163,14 @@ MOMED_API int  momed_batch_solve(momed_handle* h, const momed_solve_opts* opts, 
 MOMED_API int  momed_build_sparse(momed_handle* h, int64_t* nnz);
 MOMED_API int  momed_sparse_copy(momed_handle* h, int64_t* row_ptr, int32_t* col, double* val);
 MOMED_API int  momed_release_sparse(momed_handle* h);
+/* create_gpu_matrix(H::SparseMatrixCSC, Val(:b200)) (MomentumEDCUDAExt.jl:145-152): upload a
+ * host matrix of size n as CSR (0-based row_ptr[n + 1], col[nnz], val[2 nnz] c128; for the
+ * Hermitian CSC matrix that SparseHmltMatrix returns, pass its colptr and rowval with conjugated
+ * values).  Validated on the host (monotone row_ptr from 0, columns in [0, n)).  The handle then
+ * multiplies by it (momed_matvec, momed_eigsolve) with no basis or operator; a later basis drops
+ * it, and momed_release_sparse empties the handle. */
+MOMED_API int  momed_set_sparse_csr(momed_handle* h, int64_t n, const int64_t* row_ptr, const int32_t* col,
+                                    const double* val);
 
 /* Diagnostics for roofline accounting: exact (row, term) hit count of the working operator
  * on the working basis, the index mode (0 = ranked tables, 1 = checked tables, 2 = search),

@@ -173,6 +173,8 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
 // Build the index when the basis changed or the operator reaches bits outside it, and
 // validate the operator once: zero targets outside the basis enables the unchecked lookup.
 void ensure_ready(momed_handle* h) {
+    MOMED_REQUIRE(!h->sparse_only, MOMED_ESTATE,
+                  "the handle holds an uploaded matrix without a basis (momed_set_sparse_csr); set a basis first");
     MOMED_REQUIRE(h->n > 0, MOMED_ESTATE, "set a basis first (momed_set_basis / momed_select_sector)");
     MOMED_REQUIRE(h->op_set, MOMED_ESTATE, "set an operator first (momed_set_scatter)");
     if (h->index_dirty || (h->op_mask_or & ~h->index_bits)) {
@@ -268,6 +270,7 @@ void after_basis_change(momed_handle* h) {
     h->index_dirty = true;
     h->op_validated = false;
     h->sparse.release();
+    h->sparse_only = false;
 }
 
 }  // namespace
@@ -462,7 +465,7 @@ int momed_matvec(momed_handle* h, const void* x, void* y, int32_t precision, int
     return guarded(h, [&]() {
         MOMED_REQUIRE(x && y, MOMED_EINVAL, "null vector");
         MOMED_REQUIRE(precision == MOMED_C128 || precision == MOMED_C64, MOMED_EINVAL, "unknown precision");
-        ensure_ready(h);
+        if (!h->sparse.built) ensure_ready(h);
         const int64_t n = h->n;
         cudaStream_t st = h->stream;
         const size_t es = precision == MOMED_C128 ? 16 : 8;
@@ -542,6 +545,33 @@ int momed_release_sparse(momed_handle* h) {
     return guarded(h, [&]() {
         MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
         h->sparse.release();
+        if (h->sparse_only) {          // nothing left to multiply by: back to an empty handle
+            h->sparse_only = false;
+            h->n = 0;
+        }
+        return MOMED_OK;
+    });
+}
+
+int momed_set_sparse_csr(momed_handle* h, int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(n >= 1 && n <= (int64_t)INT32_MAX, MOMED_EINVAL, "matrix size must be in [1, 2^31 - 1]");
+        MOMED_REQUIRE(row_ptr && col && val, MOMED_EINVAL, "row_ptr, col and val are required");
+        MOMED_REQUIRE(row_ptr[0] == 0, MOMED_EINVAL, "row_ptr[0] must be 0");
+        for (int64_t i = 0; i < n; ++i)
+            MOMED_REQUIRE(row_ptr[i + 1] >= row_ptr[i], MOMED_EINVAL, "row_ptr must not decrease");
+        const int64_t nnz = row_ptr[n];
+        for (int64_t p = 0; p < nnz; ++p)
+            MOMED_REQUIRE(col[p] >= 0 && (int64_t)col[p] < n, MOMED_EINVAL, "column index out of range");
+        MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        upload_sparse(h, n, row_ptr, col, val);
+        h->basis.release();
+        h->n = n;
+        h->basis_or = 0;
+        h->index_dirty = true;
+        h->op_validated = false;
+        h->sparse_only = true;
         return MOMED_OK;
     });
 }

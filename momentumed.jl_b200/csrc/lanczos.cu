@@ -386,7 +386,7 @@ using namespace momed;
 
 int momed_eigsolve_impl(momed_handle* h, const momed_solve_opts* o, const double* vec0, double* vals, double* resid,
                         void* vecs, momed_info* info) {
-    ensure_ready(h);
+    if (!h->sparse.built) ensure_ready(h);   // a built sparse matrix needs no index or operator check
     const int64_t N = h->n;
     const int nev = (int)std::min<int64_t>(o->nev, N);
     MOMED_REQUIRE(o->nev >= 1, MOMED_EINVAL, "N should be at least 1");

@@ -209,6 +209,7 @@ struct momed_handle {
     uint64_t index_bits = 0;               // bits the index tables cover
     momed::Operator op;
     momed::SparseMatrix sparse;           // built by momed_build_sparse; maps use it while built
+    bool sparse_only = false;              // an uploaded matrix (momed_set_sparse_csr) without a basis
     bool op_set = false;
     bool op_validated = false;
     uint64_t op_mask_or = 0;               // OR of all term masks
@@ -261,6 +262,7 @@ void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const doubl
 
 // sparse.cu: CSR build at parameter u (after ensure_ready) and the CSR SpMV
 void build_sparse(momed_handle* h, double u);
+void upload_sparse(momed_handle* h, int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val);
 int64_t sparse_bytes_per_entry(bool pair);
 void launch_block_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, const float* u, int32_t nb,
                            int64_t rows, cudaStream_t st);

@@ -279,6 +279,11 @@ k_block_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ co
     }
 }
 
+__global__ void k_round_c64(const double2* __restrict__ v, float2* __restrict__ o, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        o[i] = make_float2((float)v[i].x, (float)v[i].y);
+}
+
 int spmv_grid(int64_t rows) {
     static int sms = 0;
     if (sms == 0) {
@@ -364,6 +369,39 @@ void build_sparse(momed_handle* h, double u) {
     }
     sp.nnz = nnz;
     sp.u = u;
+    sp.built = true;
+}
+
+// A host CSR matrix (validated by the caller: row_ptr monotone from 0, columns in [0, n)).
+void upload_sparse(momed_handle* h, int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val) {
+    SparseMatrix& sp = h->sparse;
+    sp.release();
+    cudaStream_t st = h->stream;
+    const int64_t nnz = row_ptr[n];
+    const int64_t need = (n + 1) * 8 + nnz * sparse_bytes_per_entry(false);
+    size_t free_b = 0, total_b = 0;
+    MOMED_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+    int64_t limit = (int64_t)(0.9 * (double)free_b);
+    if (h->hbm_budget > 0) limit = std::min<int64_t>(limit, h->hbm_budget);
+    if (need > limit)
+        throw Error{MOMED_ENOMEM, "sparse method: the matrix needs " + std::to_string(need) + " bytes, " +
+                                     std::to_string(limit) + " available"};
+    sp.row_ptr.resize(n + 1);
+    sp.col.resize(std::max<int64_t>(nnz, 1));
+    sp.val.resize(std::max<int64_t>(nnz, 1));
+    sp.val32.resize(std::max<int64_t>(nnz, 1));
+    MOMED_CUDA_TRY(cudaMemcpyAsync(sp.row_ptr.p, row_ptr, (n + 1) * 8, cudaMemcpyHostToDevice, st));
+    if (nnz > 0) {
+        MOMED_CUDA_TRY(cudaMemcpyAsync(sp.col.p, col, nnz * 4, cudaMemcpyHostToDevice, st));
+        MOMED_CUDA_TRY(cudaMemcpyAsync(sp.val.p, val, nnz * 16, cudaMemcpyHostToDevice, st));
+        const int g = (int)std::min<int64_t>((nnz + 255) / 256, 148 * 16);
+        k_round_c64<<<g, 256, 0, st>>>(sp.val.p, sp.val32.p, nnz);
+        MOMED_CUDA_TRY(cudaGetLastError());
+        note_launches(1);
+    }
+    MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+    sp.nnz = nnz;
+    sp.u = h->u;
     sp.built = true;
 }
 

@@ -1,7 +1,8 @@
 # MomentumEDB200Ext — package extension that plugs libmomed_b200.so into MomentumED.jl's
 # GPU hooks (MomentumED/src/method/gpu_interface.jl:13-21) so that
 #     EDsolve(subspace, H::MBOperator; method=:map, device=:gpu, N=...)
-# runs on a B200.  No reference file is edited: the extension registers :b200 in the
+#     EDsolve(subspace, H::MBOperator; method=:sparse, device=:gpu, N=...)
+# run on a B200.  No reference file is edited: the extension registers :b200 in the
 # mutable GPU_AVAILABLE dict and makes it the DEFAULT_GPU, and EDsolve resolves :gpu to it
 # (MomentumED.jl:446-453).
 #
@@ -12,6 +13,9 @@ module MomentumEDB200Ext
 using MomentumED
 using MomentumED.Methods: GPU_AVAILABLE, DEFAULT_GPU, LinearMap, AbstractGPULinearMap
 import MomentumED.Methods: create_gpu_linearmap, krylov_map_solve, release_gpu_memory
+import MomentumED.Methods: create_gpu_matrix, krylov_matrix_solve
+using SparseArrays: SparseMatrixCSC, sparse
+using LinearAlgebra: Hermitian
 
 const libmomed = get(ENV, "MOMED_B200_LIB", joinpath(@__DIR__, "..", "lib", "libmomed_b200.so"))
 
@@ -109,6 +113,50 @@ function krylov_map_solve(H::B200LinearMap{bits, F}, N_eigen::Int64; ishermitian
     vals = zeros(Float64, nev)
     resid = zeros(Float64, nev)
     vecs = zeros(ComplexF64, m, nev)            # column i = eigenvector i (layout [nev][N] in C)
+    v0 = vec0 === nothing ? C_NULL : pointer(ComplexF64.(vec0))
+    info = MomedInfo()
+    check(H.handle, ccall((:momed_eigsolve, libmomed), Cint,
+                          (Ptr{Cvoid}, Ref{MomedSolveOpts}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{ComplexF64},
+                           Ref{MomedInfo}),
+                          H.handle, opts, v0, vals, resid, vecs, info))
+    return vals, [Vector{Complex{F}}(vecs[:, i]) for i in 1:nev], info
+end
+
+# Sparse method hooks (EDsolve(...; method=:sparse, device=:gpu), MomentumEDCUDAExt.jl:145-200).
+# create_gpu_matrix receives the host CSC that SparseHmltMatrix built; H is Hermitian, so its
+# CSC columns with conjugated values are the CSR rows of H (momed_set_sparse_csr).
+mutable struct B200SparseMatrix{F <: AbstractFloat}
+    handle::Ptr{Cvoid}
+    n::Int
+end
+Base.size(A::B200SparseMatrix) = (A.n, A.n)
+
+function create_gpu_matrix(H::SparseMatrixCSC{Complex{F}}, ::Val{:b200}) where {F}
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(C_NULL, ccall((:momed_create, libmomed), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, h))
+    n = size(H, 2)
+    rowptr = Int64.(H.colptr) .- 1
+    col = Int32.(H.rowval) .- Int32(1)
+    val = conj.(ComplexF64.(H.nzval))
+    check(h[], ccall((:momed_set_sparse_csr, libmomed), Cint,
+                     (Ptr{Cvoid}, Int64, Ptr{Int64}, Ptr{Int32}, Ptr{ComplexF64}), h[], n, rowptr, col, val))
+    M = B200SparseMatrix{F}(h[], n)
+    finalizer(m -> (m.handle != C_NULL && ccall((:momed_destroy, libmomed), Cint, (Ptr{Cvoid},), m.handle);
+                    m.handle = C_NULL), M)
+    return M
+end
+create_gpu_matrix(H::Hermitian{C, SparseMatrixCSC{C}}, v::Val{:b200}) where {C <: Complex} =
+    create_gpu_matrix(sparse(H), v)
+
+function krylov_matrix_solve(H::B200SparseMatrix{F}, N_eigen::Int64; ishermitian::Bool = true,
+                             vec0 = nothing, krylovdim::Int = 30, tol::Real = 1e-12, maxiter::Int = 100,
+                             seed::Integer = 0, precision::Symbol = :fp64, kwargs...) where {F}
+    ishermitian || error("the B200 sparse method solves Hermitian problems")
+    nev = min(N_eigen, H.n)
+    opts = MomedSolveOpts(nev, krylovdim, maxiter, precision === :mixed ? 1 : 0, tol, seed, 1, 0)
+    vals = zeros(Float64, nev)
+    resid = zeros(Float64, nev)
+    vecs = zeros(ComplexF64, H.n, nev)
     v0 = vec0 === nothing ? C_NULL : pointer(ComplexF64.(vec0))
     info = MomedInfo()
     check(H.handle, ccall((:momed_eigsolve, libmomed), Cint,

@@ -74,6 +74,7 @@ SIGNATURES = {
     "momed_build_sparse": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "momed_sparse_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_release_sparse": (C.c_int, [C.c_void_p]),
+    "momed_set_sparse_csr": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "momed_last_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "momed_kernel_launches": (C.c_int64, []),
@@ -340,6 +341,18 @@ class Handle:
         val = np.empty(max(nnz, 1), np.complex128)
         self._check(lib().momed_sparse_copy(self._h, _p(rp), _p(col), _p(val)))
         return rp, col[:nnz], val[:nnz]
+
+    def set_sparse_csr(self, row_ptr, col, val):
+        """Upload a host CSR matrix (int64 row_ptr[n + 1], int32 col, complex128 val); the handle
+        then multiplies by it with no basis or operator (create_gpu_matrix of a host matrix)."""
+        rp = np.ascontiguousarray(row_ptr, np.int64)
+        c = np.ascontiguousarray(col, np.int32)
+        v = np.ascontiguousarray(val, np.complex128)
+        if len(c) != rp[-1] or len(v) != rp[-1]:
+            raise MomedError(EINVAL, "col and val must hold row_ptr[-1] entries")
+        self._check(lib().momed_set_sparse_csr(self._h, len(rp) - 1, _p(rp), _p(c), _p(v)))
+        self.n = len(rp) - 1
+        self._sparse_nnz = int(rp[-1])
 
     def release_sparse(self):
         self._check(lib().momed_release_sparse(self._h))

@@ -122,7 +122,7 @@ def krylov_map_solve(H: B200LinearMap, N_eigen: int, *, ishermitian: bool = True
     """Lowest N_eigen eigenpairs (:SR) of the device map; returns (vals, vecs, info)."""
     if not ishermitian:
         raise NotImplementedError("the non-Hermitian map is not part of this backend")
-    m = len(H.space)
+    m = H.size[0]
     N_eigen = min(N_eigen, m)
     prec = _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64
     vals, vecs, resid, info = H.handle.eigsolve(N_eigen, krylovdim=krylovdim, tol=tol, maxiter=maxiter,
@@ -162,8 +162,37 @@ class B200SparseMatrix:
         self.handle.close()
 
 
-def create_gpu_matrix(A: LinearMap, device: str = "b200") -> B200SparseMatrix:
-    return B200SparseMatrix(A)
+class B200HostSparseMatrix:
+    """A host sparse matrix uploaded to the device (create_gpu_matrix of the reference's host
+    matrix, MomentumEDCUDAExt.jl:145-152): any scipy.sparse matrix, stored as CSR."""
+
+    def __init__(self, H, device: int = 0):
+        import scipy.sparse as sps
+        csr = sps.csr_matrix(H, dtype=np.complex128)
+        csr.sort_indices()
+        self.handle = _lib.Handle(device)
+        self.handle.set_sparse_csr(csr.indptr, csr.indices, csr.data)
+        self.nnz = csr.nnz
+        self.size = csr.shape
+        self.element_type = np.complex128
+
+    def __call__(self, x, y=None):
+        out = self.handle.matvec(np.asarray(x, np.complex128))
+        if y is not None:
+            y[...] = out
+            return y
+        return out
+
+    def release(self):
+        self.handle.close()
+
+
+def create_gpu_matrix(A, device: str = "b200"):
+    """A LinearMap: the matrix is built on the device from its basis and term list.  A host
+    scipy.sparse matrix (what SparseHmltMatrix builds, sparse_matrix.jl:64-190): uploaded."""
+    if isinstance(A, LinearMap):
+        return B200SparseMatrix(A)
+    return B200HostSparseMatrix(A)
 
 
 def krylov_matrix_solve(H: B200SparseMatrix, N_eigen: int, **kw):

@@ -249,3 +249,48 @@ def test_batch_solve_single_operator_on_sparse_entries(h):
     w = np.linalg.eigvalsh(O.dense_hamiltonian(basis, ofull))
     for q in range(4):                                   # a single operator: every u solves H = A
         assert np.max(np.abs(v[q] - w[:5]) / np.maximum(np.abs(w[:5]), 1.0)) < 1e-10
+
+
+def test_sparse_subset_basis_drops_absent_targets(h):
+    """A basis that is not a whole sector (every other state): targets outside it are dropped as
+    index_fit drops them (hilbert_subspace.jl:67-72), in the matrix and in its SpMV."""
+    full, ofull = full_lists(3, 5, 0)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    basis = ref[3][::2].copy()
+    h.set_basis(basis)
+    h.set_scatter(full.amp.astype(np.complex128), full.in_, full.out, full.pm)
+    h.build_sparse()
+    assert_same_matrix(device_csc(h, len(basis)), oracle_csc(basis, ofull))
+    x = np.random.default_rng(9).normal(size=len(basis)) + 0.2j
+    assert rel(h.matvec(x), O.matvec(basis, ofull, x)) < 1e-13
+    h.release_sparse()
+
+
+def test_uploaded_host_matrix_dropin(h):
+    """create_gpu_matrix of a host matrix (the reference's sparse GPU hook receives the CSC that
+    SparseHmltMatrix builds): the oracle's CSC uploaded, multiplied and solved on the device."""
+    full, ofull = full_lists(3, 5, 0)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    basis = ref[9]
+    Hcsc = oracle_csc(basis, ofull)
+    G = momed.create_gpu_matrix(Hcsc)
+    try:
+        x = np.random.default_rng(11).normal(size=len(basis)) + 0.4j
+        assert rel(G(x), O.matvec(basis, ofull, x)) < 1e-13
+        vals, vecs, info = momed.krylov_matrix_solve(G, 10, krylovdim=30, tol=1e-12, seed=2)
+        w = np.linalg.eigvalsh(O.dense_hamiltonian(basis, ofull))
+        assert np.max(np.abs(vals - w[:10]) / np.maximum(np.abs(w[:10]), 1.0)) < 1e-10
+        with pytest.raises(momed.MomedError) as e:        # no basis: operator calls are refused
+            G.handle.stats()
+        assert e.value.code == momed._lib.ESTATE
+    finally:
+        G.release()
+    # the Hermitian CSC passed as CSR with conjugated values (what the Julia hook does)
+    hd = momed.Handle(0)
+    try:
+        hd.set_sparse_csr(Hcsc.indptr, Hcsc.indices, np.conj(Hcsc.data))
+        assert rel(hd.matvec(x), O.matvec(basis, ofull, x)) < 1e-13
+        with pytest.raises(momed.MomedError):
+            hd.set_sparse_csr(np.array([0, 1]), np.array([5], np.int32), np.ones(1))   # column out of range
+    finally:
+        hd.close()
