@@ -172,6 +172,14 @@ MOMED_API int  momed_release_sparse(momed_handle* h);
 MOMED_API int  momed_set_sparse_csr(momed_handle* h, int64_t n, const int64_t* row_ptr, const int32_t* col,
                                     const double* val);
 
+/* ED_bracket(bra, op, ket) (EDCore/src/multiplication.jl:153-190, 239-245): <bra| H |ket> with
+ * the working operator (its Hermitian-completed list, at the current u), ket (c128, host) on the
+ * working basis and bra (c128, host) on bra_basis[n_bra] (sorted; NULL = the working basis, then
+ * n_bra is ignored).  Targets outside the bra space are dropped (index_fit).  Computed as one
+ * fused map-and-dot kernel (no H ket vector is written); out[2] = (re, im). */
+MOMED_API int  momed_bracket(momed_handle* h, const uint64_t* bra_basis, int64_t n_bra, const double* bra,
+                             const double* ket, double* out);
+
 /* Diagnostics for roofline accounting: exact (row, term) hit count of the working operator
  * on the working basis, the index mode (0 = ranked tables, 1 = checked tables, 2 = search),
  * and the bytes of the lookup tables. */

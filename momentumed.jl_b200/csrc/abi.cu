@@ -576,6 +576,48 @@ int momed_set_sparse_csr(momed_handle* h, int64_t n, const int64_t* row_ptr, con
     });
 }
 
+int momed_bracket(momed_handle* h, const uint64_t* bra_basis, int64_t n_bra, const double* bra, const double* ket,
+                  double* out) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(bra && ket && out, MOMED_EINVAL, "bra, ket and out are required");
+        MOMED_REQUIRE(!bra_basis || n_bra >= 1, MOMED_EINVAL, "bad bra basis");
+        ensure_ready(h);
+        const int64_t n = h->n;
+        cudaStream_t st = h->stream;
+        IndexView iv = index_view(h);
+        DevBuf<uint64_t> rows_b;
+        const uint64_t* rows = h->basis.p;
+        int64_t nrows = n;
+        if (bra_basis) {
+            for (int64_t i = 1; i < n_bra; ++i)
+                MOMED_REQUIRE(bra_basis[i] > bra_basis[i - 1], MOMED_EINVAL, "bra basis must be sorted ascending");
+            rows_b.resize(n_bra);
+            MOMED_CUDA_TRY(cudaMemcpyAsync(rows_b.p, bra_basis, n_bra * 8, cudaMemcpyHostToDevice, st));
+            rows = rows_b.p;
+            nrows = n_bra;
+            // targets of another space may be absent from this one: compare keys on every lookup
+            if (iv.mode == INDEX_RANKED) iv.mode = INDEX_CHECKED;
+        }
+        DevBuf<double2> kd, bd, part;
+        kd.resize(n);
+        bd.resize(nrows);
+        MOMED_CUDA_TRY(cudaMemcpyAsync(kd.p, ket, n * 16, cudaMemcpyHostToDevice, st));
+        MOMED_CUDA_TRY(cudaMemcpyAsync(bd.p, bra, nrows * 16, cudaMemcpyHostToDevice, st));
+        const int grid = bracket_grid(nrows);
+        part.resize(grid);
+        launch_bracket(iv, h->op.view(), rows, bd.p, kd.p, h->op.has_b ? h->u_dev.p : nullptr, nrows, part.p, grid, st);
+        std::vector<double2> hp(grid);
+        MOMED_CUDA_TRY(cudaMemcpyAsync(hp.data(), part.p, grid * 16, cudaMemcpyDeviceToHost, st));
+        MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+        double re = 0.0, im = 0.0;
+        for (const double2& v : hp) { re += v.x; im += v.y; }
+        out[0] = re;
+        out[1] = im;
+        return MOMED_OK;
+    });
+}
+
 int momed_stats(momed_handle* h, int64_t* nnz, int32_t* index_mode, int64_t* table_bytes) {
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {

@@ -86,6 +86,74 @@ k_matvec(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typen
     }
 }
 
+// <bra| H |ket> without writing H ket: rows run over the bra space (row_states), targets are
+// looked up in the ket space (iv; checked keys when the two spaces differ, so a target outside the
+// ket space is dropped as index_fit drops it).  A lane folds conj(bra[row]) into its share of each
+// row, a block writes one partial sum; the host adds the partials in block order.
+template <bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_bracket(IndexView iv, OpView ov, const uint64_t* __restrict__ row_states, const double2* __restrict__ bra,
+          const double2* __restrict__ ket, const double* __restrict__ u_ptr, int64_t rows,
+          double2* __restrict__ partial) {
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    __shared__ double2 s_sum[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpScratch& ws = s_ws[wid];
+    const double u = HAS_B ? *u_ptr : 0.0;
+    double wr = 0.0, wi = 0.0;
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(row_states + row);
+        double ar = 0.0, ai = 0.0;
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                if (f < total) {
+                    while (ws.pref[gi + 1] <= f) ++gi;
+                    const int t = ws.start[gi] + (f - ws.pref[gi]);
+                    const uint64_t om = ws.out[gi];
+                    const uint64_t tin = __ldg(ov.t_in + t);
+                    const uint64_t mid = s & ~om;
+                    if ((mid & tin) == 0) {
+                        const bool neg = (__popcll(mid & __ldg(ov.t_pm + t)) & 1) != 0;
+                        const int64_t j = lookup_index(iv, mid | tin, sh.base_hi, sh.base_lo, sh.binom);
+                        if (j >= 0) {
+                            double2 a = __ldg(ov.t_amp + t);
+                            if (HAS_B) {
+                                const double2 b = __ldg(ov.t_ampb + t);
+                                a.x += u * b.x;
+                                a.y += u * b.y;
+                            }
+                            const double2 xv = __ldg(ket + j);
+                            const double pr = a.x * xv.x - a.y * xv.y, pi = a.x * xv.y + a.y * xv.x;
+                            if (neg) { ar -= pr; ai -= pi; } else { ar += pr; ai += pi; }
+                        }
+                    }
+                }
+            }
+            __syncwarp();
+        });
+        const double2 bv = __ldg(bra + row);            // conj(bra) times this lane's share of the row
+        wr += bv.x * ar + bv.y * ai;
+        wi += bv.x * ai - bv.y * ar;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        wr += __shfl_xor_sync(kFull, wr, o);
+        wi += __shfl_xor_sync(kFull, wi, o);
+    }
+    if (lane == 0) s_sum[wid] = make_double2(wr, wi);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double2 acc = make_double2(0.0, 0.0);
+        for (int w = 0; w < kWarps; ++w) { acc.x += s_sum[w].x; acc.y += s_sum[w].y; }
+        partial[blockIdx.x] = acc;
+    }
+}
+
 // Counts hits (targets found) and misses (targets outside the basis) without touching x.
 __global__ void __launch_bounds__(kWarps * 32)
 k_count(IndexView iv, OpView ov, unsigned long long* hits, unsigned long long* misses, int64_t rows) {
@@ -363,6 +431,16 @@ void launch_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, f
         auto k = k_matvec<float, false>;
         k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, nullptr, rows);
     }
+    MOMED_CUDA_TRY(cudaGetLastError());
+    note_launches(1);
+}
+
+int bracket_grid(int64_t rows) { return persistent_grid(k_bracket<false>, rows); }
+
+void launch_bracket(const IndexView& iv, const OpView& ov, const uint64_t* row_states, const double2* bra,
+                    const double2* ket, const double* u, int64_t rows, double2* partial, int grid, cudaStream_t st) {
+    if (u && ov.t_ampb) k_bracket<true><<<grid, kWarps * 32, 0, st>>>(iv, ov, row_states, bra, ket, u, rows, partial);
+    else k_bracket<false><<<grid, kWarps * 32, 0, st>>>(iv, ov, row_states, bra, ket, nullptr, rows, partial);
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }

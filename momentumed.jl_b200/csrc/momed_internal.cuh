@@ -254,6 +254,11 @@ void launch_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, f
                        const float* u_scale, int64_t rows, cudaStream_t st);
 void launch_count_hits(const IndexView& iv, const OpView& ov, unsigned long long* hits,
                        unsigned long long* misses, int64_t rows, cudaStream_t st);
+// <bra| H |ket>: rows over row_states (the bra space), lookups in iv (the ket space); one partial
+// sum per block (grid from bracket_grid)
+int bracket_grid(int64_t rows);
+void launch_bracket(const IndexView& iv, const OpView& ov, const uint64_t* row_states, const double2* bra,
+                    const double2* ket, const double* u, int64_t rows, double2* partial, int grid, cudaStream_t st);
 // block matvec: nb right-hand sides interleaved [row][nb], H_u = A + u[b] B
 void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y,
                              const float* u, int32_t nb, int64_t rows, cudaStream_t st);

@@ -75,6 +75,7 @@ SIGNATURES = {
     "momed_sparse_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_release_sparse": (C.c_int, [C.c_void_p]),
     "momed_set_sparse_csr": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "momed_bracket": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "momed_last_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "momed_kernel_launches": (C.c_int64, []),
@@ -321,6 +322,20 @@ class Handle:
         n, ms = C.c_int64(), C.c_double()
         self._check(lib().momed_profile_read(self._h, kind, C.byref(n), C.byref(ms)))
         return n.value, ms.value
+
+    def bracket(self, bra: np.ndarray, ket: np.ndarray, bra_basis=None) -> complex:
+        """<bra| H |ket>: ket on the working basis, bra on bra_basis (None: the working basis)."""
+        k = np.ascontiguousarray(ket, np.complex128)
+        b = np.ascontiguousarray(bra, np.complex128)
+        out = np.zeros(2)
+        if bra_basis is None:
+            self._check(lib().momed_bracket(self._h, None, 0, _p(b), _p(k), _p(out)))
+        else:
+            bb = np.ascontiguousarray(bra_basis, np.uint64)
+            if len(bb) != len(b):
+                raise MomedError(EINVAL, "bra and bra_basis lengths differ")
+            self._check(lib().momed_bracket(self._h, _p(bb), len(bb), _p(b), _p(k), _p(out)))
+        return complex(out[0], out[1])
 
     # ---------------------------------------------------------------- sparse method
     def build_sparse(self) -> int:

@@ -999,6 +999,54 @@ OR_API int64_t or_sparse_csc(const uint64_t* basis, int64_t N, const or_scat* li
     return nnz;
 }
 
+/* <bra| op |ket>: mul_add_bracket / mul_add_bracket_scatlist (EDCore/src/multiplication.jl:153-190)
+ * over a term list; with upper != 0 every off-diagonal term also adds its conjugate back-scatter
+ * (upper_hermitian).  bra lives on bra_basis, ket on ket_basis (sorted lists); targets outside the
+ * bra space are dropped (index_fit).  Vectors are interleaved complex. */
+OR_API void or_bracket(const uint64_t* bra_basis, int64_t nbra, const double* bra, const uint64_t* ket_basis,
+                       int64_t nket, const double* ket, const or_scat* list, int64_t nscat, int upper,
+                       double* out) {
+    double sr = 0.0, si = 0.0;
+    for (int64_t s = 0; s < nscat; ++s) {
+        const or_scat* sc = &list[s];
+        double br = 0.0, bi = 0.0;
+        for (int64_t j = 0; j < nket; ++j) {
+            const uint64_t st = ket_basis[j];
+            if ((st & sc->in) != sc->in) continue;
+            uint64_t tgt;
+            double ar, ai;
+            if (sc->in == sc->out) { tgt = st; ar = sc->re; ai = sc->im; }
+            else {
+                uint64_t mid = st & ~sc->in;
+                if ((mid & sc->out) != 0) continue;
+                tgt = mid | sc->out;
+                int sign = 1 - 2 * (__builtin_popcountll(mid & sc->pm) & 1);
+                ar = sign * sc->re; ai = sign * sc->im;
+            }
+            if (ar == 0.0 && ai == 0.0) continue;
+            int64_t i = searchsortedfirst(bra_basis, nbra, tgt);
+            if (i >= nbra || bra_basis[i] != tgt) continue;
+            /* conj(bra[i]) * amp * ket[j] */
+            double kr = ket[2 * j], ki = ket[2 * j + 1], pr = ar * kr - ai * ki, pi = ar * ki + ai * kr;
+            double cr = bra[2 * i], ci = -bra[2 * i + 1];
+            br += cr * pr - ci * pi;
+            bi += cr * pi + ci * pr;
+            if (upper && i != j) {
+                /* conj(bra[j]) * conj(amp) * ket[i] (the same space for bra and ket) */
+                double kr2 = ket[2 * i], ki2 = ket[2 * i + 1];
+                double qr = ar * kr2 + ai * ki2, qi = ar * ki2 - ai * kr2;
+                double dr = bra[2 * j], di = -bra[2 * j + 1];
+                br += dr * qr - di * qi;
+                bi += dr * qi + di * qr;
+            }
+        }
+        sr += br;
+        si += bi;
+    }
+    out[0] = sr;
+    out[1] = si;
+}
+
 /* Exact nonzero count of the gather (row, term) hits, the nnz of the roofline formula. */
 OR_API int64_t or_count_hits(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat, int nthreads) {
 #ifdef _OPENMP

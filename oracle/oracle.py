@@ -108,6 +108,8 @@ def lib():
         L.or_matvec_c128.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]
         L.or_matvec_c64.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]
         L.or_dense_hamiltonian.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
+        L.or_bracket.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                 C.c_int64, C.c_int, C.c_void_p]
         L.or_sparse_csc.restype = C.c_int64
         L.or_sparse_csc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_int64]
@@ -382,6 +384,19 @@ def dense_hamiltonian(basis: np.ndarray, full_list: np.ndarray) -> np.ndarray:
     H = np.zeros((len(basis), len(basis)), np.complex128)
     lib().or_dense_hamiltonian(_ptr(basis), len(basis), _ptr(full_list), len(full_list), _ptr(H))
     return H
+
+
+def bracket(bra_basis, bra, ket_basis, ket, scat_list, upper: bool = False) -> complex:
+    """<bra| op |ket> over a term list (multiplication.jl:153-190); upper: upper_hermitian list."""
+    bb = np.ascontiguousarray(bra_basis, np.uint64)
+    kb = np.ascontiguousarray(ket_basis, np.uint64)
+    bv = np.ascontiguousarray(bra, np.complex128)
+    kv = np.ascontiguousarray(ket, np.complex128)
+    lst = np.ascontiguousarray(scat_list, SCAT_DTYPE)
+    out = np.zeros(2)
+    lib().or_bracket(_ptr(bb), len(bb), _ptr(bv), _ptr(kb), len(kb), _ptr(kv), _ptr(lst), len(lst), int(upper),
+                     _ptr(out))
+    return complex(out[0], out[1])
 
 
 def sparse_csc(basis: np.ndarray, full_list: np.ndarray):

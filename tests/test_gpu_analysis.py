@@ -1,0 +1,91 @@
+"""Analysis of eigenvectors on the device: ED_bracket (EDCore/src/multiplication.jl:153-245)
+against the oracle's restatement of mul_add_bracket, within 1e-12 relative."""
+import numpy as np
+import pytest
+
+import oracle as O
+import momed
+from momed import core
+from momed.synthetic import mesh_para
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def h():
+    hd = momed.Handle(0)
+    yield hd
+    hd.close()
+
+
+def as_oracle(lst):
+    o = np.zeros(len(lst.amp), O.SCAT_DTYPE)
+    o["re"], o["im"], o["out"], o["in"], o["pm"] = lst.amp.real, lst.amp.imag, lst.out, lst.in_, lst.pm
+    return o
+
+
+def relc(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+def test_bracket_same_space_hamiltonian(h):
+    para, _ = mesh_para(3, 5, 0)
+    op = momed.MBOperator(momed.ED_scatterlist_onebody(para), momed.ED_scatterlist_twobody(para),
+                          upper_hermitian=True)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    space = core.HilbertSubspace(ref[4])
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=len(space)) + 1j * rng.normal(size=len(space))
+    y = rng.normal(size=len(space)) + 1j * rng.normal(size=len(space))
+    got = momed.ED_bracket(core.MBS64Vector(y, space), op, core.MBS64Vector(x, space), handle=h)
+    want = O.bracket(ref[4], y, ref[4], x, as_oracle(op.scats), upper=True)
+    assert relc(got, want) < 1e-12
+    assert relc(got, np.vdot(y, O.matvec(ref[4], as_oracle(core.hermitian_complete(op)), x))) < 1e-12
+
+
+def test_bracket_across_momentum_sectors(h):
+    """rho_q = sum_k c+_{k+q} c_k moves a state from sector K to K + q: bra and ket on different
+    subspaces, targets outside the bra space dropped."""
+    a, b = 3, 5
+    kl = O.mesh_klist(a, b)
+    Nk = a * b
+    q = (1, 2)
+    amp, out, inn = [], [], []
+    for k in range(Nk):
+        kq = ((kl[0, k] + q[0]) % a) + a * ((kl[1, k] + q[1]) % b)
+        amp.append(1.0 + 0.1j * k)
+        out.append(1 << int(kq))
+        inn.append(1 << k)
+    lst = core.ScatterList(np.array(amp), np.array(out, np.uint64), np.array(inn, np.uint64))
+    op = momed.MBOperator(lst, upper_hermitian=False)
+    ref, ks = O.momentum_subspaces(kl, (a, b), (5,))
+    ks = [tuple(int(v) for v in k) for k in np.asarray(ks).reshape(len(ref), -1)]
+    iK = 3
+    K = ks[iK]
+    target = ((K[0] + q[0]) % a, (K[1] + q[1]) % b)
+    iB = ks.index(target)
+    rng = np.random.default_rng(1)
+    ket = rng.normal(size=len(ref[iK])) + 1j * rng.normal(size=len(ref[iK]))
+    bra = rng.normal(size=len(ref[iB])) + 1j * rng.normal(size=len(ref[iB]))
+    got = momed.ED_bracket(core.MBS64Vector(bra, core.HilbertSubspace(ref[iB])), op,
+                           core.MBS64Vector(ket, core.HilbertSubspace(ref[iK])), handle=h)
+    want = O.bracket(ref[iB], bra, ref[iK], ket, as_oracle(op.scats), upper=False)
+    assert abs(want) > 1e-6
+    assert relc(got, want) < 1e-12
+    # a bra in the ket's own sector sees nothing: every target leaves it
+    self_b = rng.normal(size=len(ref[iK])) + 0j
+    got0 = momed.ED_bracket(core.MBS64Vector(self_b, core.HilbertSubspace(ref[iK])), op,
+                            core.MBS64Vector(ket, core.HilbertSubspace(ref[iK])), handle=h)
+    assert abs(got0) < 1e-12
+
+
+def test_bracket_expectation_of_eigenvector(h):
+    """<psi| H |psi> of a computed eigenvector equals its eigenvalue."""
+    para, _ = mesh_para(3, 5, 0)
+    op = momed.MBOperator(momed.ED_scatterlist_onebody(para), momed.ED_scatterlist_twobody(para),
+                          upper_hermitian=True)
+    subs, _ = momed.ED_momentum_subspaces(para, (5,), handle=h)
+    E, vecs = momed.EDsolve(subs[1], op, N=3, method="map", device="gpu", method_info=False)
+    for e, v in zip(E, vecs):
+        val = momed.ED_bracket(v, op, v, handle=h)
+        assert abs(val.imag) < 1e-10 and abs(val.real - e) / abs(e) < 1e-10

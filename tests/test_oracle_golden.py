@@ -179,3 +179,21 @@ def test_sparse_csc_restatement_matches_dense():
             M[seg, j] = nz[cp[j]:cp[j + 1]]
         assert np.array_equal(M, D)
         assert len(nz) == np.count_nonzero(D)
+
+
+def test_bracket_restatement_forms_agree():
+    """mul_add_bracket with the upper_hermitian list (multiplication.jl:153-173) equals the bracket
+    with the completed list and the dot product with the oracle map."""
+    S = O.Synth(3, 5, 0)
+    upper = O.sort_merge(np.concatenate([S.onebody(), S.twobody()]))
+    full = O.hermitian_complete(upper)
+    sectors, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    b = sectors[2]
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=len(b)) + 1j * rng.normal(size=len(b))
+    y = rng.normal(size=len(b)) + 1j * rng.normal(size=len(b))
+    v_up = O.bracket(b, y, b, x, upper, upper=True)
+    v_full = O.bracket(b, y, b, x, full, upper=False)
+    v_map = np.vdot(y, O.matvec(b, full, x))
+    assert abs(v_up - v_map) < 1e-12 * abs(v_map)
+    assert abs(v_full - v_map) < 1e-12 * abs(v_map)
