@@ -180,6 +180,12 @@ MOMED_API int  momed_set_sparse_csr(momed_handle* h, int64_t n, const int64_t* r
 MOMED_API int  momed_bracket(momed_handle* h, const uint64_t* bra_basis, int64_t n_bra, const double* bra,
                              const double* ket, double* out);
 
+/* PES_1rdm(psi) (MomentumED/src/analysis/particle_reduced_density_matrix.jl:4-33): the one-body
+ * reduced density matrix rdm[i][j] = <psi| c+_i c_j |psi> over orbitals 0..norb-1 (norb <= 64;
+ * the reference's bits), psi (c128, host) on the working basis (no operator needed).  rdm:
+ * [norb][norb] c128 row-major, Hermitian. */
+MOMED_API int  momed_rdm1(momed_handle* h, const double* psi, int32_t norb, double* rdm);
+
 /* Diagnostics for roofline accounting: exact (row, term) hit count of the working operator
  * on the working basis, the index mode (0 = ranked tables, 1 = checked tables, 2 = search),
  * and the bytes of the lookup tables. */

@@ -618,6 +618,15 @@ int momed_bracket(momed_handle* h, const uint64_t* bra_basis, int64_t n_bra, con
     });
 }
 
+int momed_rdm1(momed_handle* h, const double* psi, int32_t norb, double* rdm) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(psi && rdm, MOMED_EINVAL, "psi and rdm are required");
+        rdm1(h, psi, norb, rdm);
+        return MOMED_OK;
+    });
+}
+
 int momed_stats(momed_handle* h, int64_t* nnz, int32_t* index_mode, int64_t* table_bytes) {
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {

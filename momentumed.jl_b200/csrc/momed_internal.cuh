@@ -265,6 +265,9 @@ void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2
 void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y,
                               const double* u, int32_t nb, int64_t rows, cudaStream_t st);
 
+// analysis.cu: one-body reduced density matrix of psi on the working basis ([norb][norb] c128)
+void rdm1(momed_handle* h, const double* psi, int norb, double* rdm);
+
 // sparse.cu: CSR build at parameter u (after ensure_ready) and the CSR SpMV
 void build_sparse(momed_handle* h, double u);
 void upload_sparse(momed_handle* h, int64_t n, const int64_t* row_ptr, const int32_t* col, const double* val);

@@ -76,6 +76,7 @@ SIGNATURES = {
     "momed_release_sparse": (C.c_int, [C.c_void_p]),
     "momed_set_sparse_csr": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_bracket": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "momed_rdm1": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "momed_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "momed_last_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "momed_kernel_launches": (C.c_int64, []),
@@ -336,6 +337,13 @@ class Handle:
                 raise MomedError(EINVAL, "bra and bra_basis lengths differ")
             self._check(lib().momed_bracket(self._h, _p(bb), len(bb), _p(b), _p(k), _p(out)))
         return complex(out[0], out[1])
+
+    def rdm1(self, psi: np.ndarray, norb: int) -> np.ndarray:
+        """One-body reduced density matrix [norb, norb] of psi on the working basis."""
+        v = np.ascontiguousarray(psi, np.complex128)
+        out = np.zeros((norb, norb), np.complex128)
+        self._check(lib().momed_rdm1(self._h, _p(v), int(norb), _p(out)))
+        return out
 
     # ---------------------------------------------------------------- sparse method
     def build_sparse(self) -> int:

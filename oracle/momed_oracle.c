@@ -1047,6 +1047,40 @@ OR_API void or_bracket(const uint64_t* bra_basis, int64_t nbra, const double* br
     out[1] = si;
 }
 
+/* PES_1rdm (MomentumED/src/analysis/particle_reduced_density_matrix.jl:4-33): the one-body
+ * reduced density matrix rdm[i][j] = <psi| c+_i c_j |psi> over orbitals 1..bits, computed for
+ * i <= j (sign from scat_occ_number of the intermediate state at i and j) and completed by
+ * rdm[i][j] = conj(rdm[j][i]).  rdm: [bits][bits] interleaved complex, row-major. */
+OR_API void or_rdm1(const uint64_t* basis, int64_t N, const double* psi, int bits, double* rdm) {
+    memset(rdm, 0, (size_t)bits * bits * 16);
+    for (int i = 1; i <= bits; ++i)
+        for (int j = i; j <= bits; ++j) {
+            double sr = 0.0, si = 0.0;
+            for (int64_t x = 0; x < N; ++x) {
+                uint64_t in = basis[x];
+                uint64_t bj = jl_one_shl(j - 1), bi = jl_one_shl(i - 1);
+                if ((in & bj) == 0) continue;
+                uint64_t mid = in & ~bj;
+                if (mid & bi) continue;
+                uint64_t out = mid | bi;
+                int64_t y = searchsortedfirst(basis, N, out);
+                if (y >= N || basis[y] != out) continue;
+                int par = or_scat_occ_number_1(mid, i, bits) + or_scat_occ_number_1(mid, j, bits);
+                /* conj(psi[y]) * psi[x] */
+                double pr = psi[2 * y] * psi[2 * x] + psi[2 * y + 1] * psi[2 * x + 1];
+                double pi = psi[2 * y] * psi[2 * x + 1] - psi[2 * y + 1] * psi[2 * x];
+                if (par & 1) { sr -= pr; si -= pi; } else { sr += pr; si += pi; }
+            }
+            rdm[2 * ((size_t)(i - 1) * bits + (j - 1))] = sr;
+            rdm[2 * ((size_t)(i - 1) * bits + (j - 1)) + 1] = si;
+        }
+    for (int i = 1; i <= bits; ++i)
+        for (int j = 1; j < i; ++j) {
+            rdm[2 * ((size_t)(i - 1) * bits + (j - 1))] = rdm[2 * ((size_t)(j - 1) * bits + (i - 1))];
+            rdm[2 * ((size_t)(i - 1) * bits + (j - 1)) + 1] = -rdm[2 * ((size_t)(j - 1) * bits + (i - 1)) + 1];
+        }
+}
+
 /* Exact nonzero count of the gather (row, term) hits, the nnz of the roofline formula. */
 OR_API int64_t or_count_hits(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat, int nthreads) {
 #ifdef _OPENMP

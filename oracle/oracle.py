@@ -110,6 +110,7 @@ def lib():
         L.or_dense_hamiltonian.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
         L.or_bracket.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                  C.c_int64, C.c_int, C.c_void_p]
+        L.or_rdm1.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p]
         L.or_sparse_csc.restype = C.c_int64
         L.or_sparse_csc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_int64]
@@ -397,6 +398,15 @@ def bracket(bra_basis, bra, ket_basis, ket, scat_list, upper: bool = False) -> c
     lib().or_bracket(_ptr(bb), len(bb), _ptr(bv), _ptr(kb), len(kb), _ptr(kv), _ptr(lst), len(lst), int(upper),
                      _ptr(out))
     return complex(out[0], out[1])
+
+
+def rdm1(basis, psi, bits: int) -> np.ndarray:
+    """PES_1rdm (particle_reduced_density_matrix.jl:4-33): [bits, bits] complex matrix."""
+    bb = np.ascontiguousarray(basis, np.uint64)
+    v = np.ascontiguousarray(psi, np.complex128)
+    out = np.zeros((bits, bits), np.complex128)
+    lib().or_rdm1(_ptr(bb), len(bb), _ptr(v), int(bits), _ptr(out))
+    return out
 
 
 def sparse_csc(basis: np.ndarray, full_list: np.ndarray):

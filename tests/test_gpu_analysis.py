@@ -89,3 +89,39 @@ def test_bracket_expectation_of_eigenvector(h):
     for e, v in zip(E, vecs):
         val = momed.ED_bracket(v, op, v, handle=h)
         assert abs(val.imag) < 1e-10 and abs(val.real - e) / abs(e) < 1e-10
+
+
+def test_rdm1_matches_oracle_across_sectors(h):
+    """PES_1rdm on a basis that holds every momentum sector (c+_i c_j moves between them, so the
+    matrix has off-diagonal entries) and on one sector (diagonal: the occupations)."""
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    union = np.sort(np.concatenate(ref))
+    rng = np.random.default_rng(2)
+    psi = rng.normal(size=len(union)) + 1j * rng.normal(size=len(union))
+    psi /= np.linalg.norm(psi)
+    got = momed.PES_1rdm(core.MBS64Vector(psi, core.HilbertSubspace(union, 15)), handle=h)
+    want = O.rdm1(union, psi, 15)
+    assert np.max(np.abs(got - want)) < 1e-12
+    assert np.max(np.abs(want - np.diag(np.diag(want)))) > 1e-3          # off-diagonal entries present
+    assert abs(np.trace(got) - 5) < 1e-12
+    one = ref[6]
+    phi = rng.normal(size=len(one)) + 1j * rng.normal(size=len(one))
+    phi /= np.linalg.norm(phi)
+    got1 = momed.PES_1rdm(core.MBS64Vector(phi, core.HilbertSubspace(one, 15)), handle=h)
+    assert np.max(np.abs(got1 - O.rdm1(one, phi, 15))) < 1e-12
+
+
+def test_rdm1_two_component_eigenvector(h):
+    """Two conserved components (48 orbitals at 4x6; here 4x3, 24 orbitals): the matrix of a
+    computed eigenvector against the oracle."""
+    para, _ = mesh_para(4, 3, 5, Nc_conserve=2)
+    subs, _ = momed.ED_momentum_subspaces(para, (3, 3), handle=h)
+    op = momed.MBOperator(momed.ED_scatterlist_onebody(para), momed.ED_scatterlist_twobody(para),
+                          upper_hermitian=True)
+    E, vecs = momed.EDsolve(subs[0], op, N=2, method="map", device="gpu", method_info=False)
+    bits = subs[0].bits
+    got = momed.PES_1rdm(vecs[0], handle=h)
+    want = O.rdm1(subs[0].list, vecs[0].vec, bits)
+    assert got.shape == (bits, bits)
+    assert np.max(np.abs(got - want)) < 1e-12
+    assert abs(np.trace(got).real - 6) < 1e-9

@@ -197,3 +197,19 @@ def test_bracket_restatement_forms_agree():
     v_map = np.vdot(y, O.matvec(b, full, x))
     assert abs(v_up - v_map) < 1e-12 * abs(v_map)
     assert abs(v_full - v_map) < 1e-12 * abs(v_map)
+
+
+def test_rdm1_restatement_properties():
+    """PES_1rdm restated (particle_reduced_density_matrix.jl:4-33): Hermitian, trace = electrons,
+    diagonal = occupations, and within one momentum sector (one component) diagonal."""
+    sectors, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    b = sectors[0]
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=len(b)) + 1j * rng.normal(size=len(b))
+    x /= np.linalg.norm(x)
+    R = O.rdm1(b, x, 15)
+    occ = np.array([[(int(s) >> i) & 1 for i in range(15)] for s in b])
+    assert np.allclose(R, R.conj().T)
+    assert abs(np.trace(R) - 5) < 1e-12
+    assert np.allclose(np.diag(R).real, (np.abs(x) ** 2) @ occ)
+    assert np.max(np.abs(R - np.diag(np.diag(R)))) == 0.0
