@@ -191,3 +191,19 @@ def test_queued_requests_on_one_sector_are_batched(workload):
         ref, _, _, _ = h.eigsolve(3, tol=1e-12, seed=1, want_vectors=False)
         assert np.max(np.abs(res[r][0] - ref) / np.maximum(np.abs(ref), 1.0)) < 1e-10
     h.close()
+
+
+def test_sparse_method_and_map_fallback_by_budget(workload):
+    """A 3x8 request (~30k states) is solved on the sparse method when its matrix fits the budget
+    and on the matrix-free map when only the Krylov state fits: the same eigenvalues either way."""
+    p35, p38, b35, b38 = workload
+    vals = {}
+    for budget in (8 << 30, 96 << 20):           # room for the matrix / for the solve only
+        srv = _lib.Server(0, slots=1, hbm_budget=budget)
+        op = srv.register_operator(*p38)
+        rid = srv.submit(op, b38[1], 1.1, 4, tol=1e-12, seed=5)
+        vals[budget] = wait_all(srv, [rid], {rid: 4})[rid][0]
+        assert srv.stats()["failed"] == 0
+        srv.stop()
+    a, b = vals[8 << 30], vals[96 << 20]
+    assert np.max(np.abs(a - b) / np.abs(b)) < 1e-10
