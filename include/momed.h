@@ -186,6 +186,13 @@ MOMED_API int  momed_bracket(momed_handle* h, const uint64_t* bra_basis, int64_t
  * [norb][norb] c128 row-major, Hermitian. */
 MOMED_API int  momed_rdm1(momed_handle* h, const double* psi, int32_t norb, double* rdm);
 
+/* ED_step_inner_prod (MomentumED/src/analysis/manybody_quantum_geometry.jl:48-94): for g
+ * vectors psi_f[g][N], psi_i[g][N] (c128, host) on the working basis and orbital overlaps
+ * orb[norb] (c128), out[j][k] = sum_x conj(psi_f[j][x]) psi_i[k][x] prod_{o occupied in x} orb[o]
+ * ([g][g] c128; g <= 32, norb <= 64). */
+MOMED_API int  momed_step_inner_prod(momed_handle* h, const double* psi_f, const double* psi_i, int32_t g,
+                                     const double* orb, int32_t norb, double* out);
+
 /* Diagnostics for roofline accounting: exact (row, term) hit count of the working operator
  * on the working basis, the index mode (0 = ranked tables, 1 = checked tables, 2 = search),
  * and the bytes of the lookup tables. */

@@ -627,6 +627,16 @@ int momed_rdm1(momed_handle* h, const double* psi, int32_t norb, double* rdm) {
     });
 }
 
+int momed_step_inner_prod(momed_handle* h, const double* psi_f, const double* psi_i, int32_t g, const double* orb,
+                          int32_t norb, double* out) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(psi_f && psi_i && orb && out, MOMED_EINVAL, "psi_f, psi_i, orb and out are required");
+        step_inner_prod(h, psi_f, psi_i, g, orb, norb, out);
+        return MOMED_OK;
+    });
+}
+
 int momed_stats(momed_handle* h, int64_t* nnz, int32_t* index_mode, int64_t* table_bytes) {
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {

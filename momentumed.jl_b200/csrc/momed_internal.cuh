@@ -267,6 +267,9 @@ void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const doubl
 
 // analysis.cu: one-body reduced density matrix of psi on the working basis ([norb][norb] c128)
 void rdm1(momed_handle* h, const double* psi, int norb, double* rdm);
+// ED_step_inner_prod of g vectors [g][N] on the working basis, orbital overlaps orb[norb] ([g][g] c128)
+void step_inner_prod(momed_handle* h, const double* psi_f, const double* psi_i, int g, const double* orb, int norb,
+                     double* out);
 
 // sparse.cu: CSR build at parameter u (after ensure_ready) and the CSR SpMV
 void build_sparse(momed_handle* h, double u);

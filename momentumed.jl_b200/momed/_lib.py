@@ -77,6 +77,8 @@ SIGNATURES = {
     "momed_set_sparse_csr": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_bracket": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_rdm1": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "momed_step_inner_prod": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
+                                        C.c_void_p]),
     "momed_stats": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "momed_last_kernel_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
     "momed_kernel_launches": (C.c_int64, []),
@@ -343,6 +345,17 @@ class Handle:
         v = np.ascontiguousarray(psi, np.complex128)
         out = np.zeros((norb, norb), np.complex128)
         self._check(lib().momed_rdm1(self._h, _p(v), int(norb), _p(out)))
+        return out
+
+    def step_inner_prod(self, psi_f: np.ndarray, psi_i: np.ndarray, orb: np.ndarray) -> np.ndarray:
+        """[g, g] many-body connection step of [g, N] vectors on the working basis."""
+        f = np.ascontiguousarray(np.atleast_2d(psi_f), np.complex128)
+        i = np.ascontiguousarray(np.atleast_2d(psi_i), np.complex128)
+        o = np.ascontiguousarray(orb, np.complex128)
+        if f.shape != i.shape or f.shape[1] != self.n:
+            raise MomedError(EINVAL, "psi_f and psi_i must both be [g, N] on the working basis")
+        out = np.zeros((f.shape[0], f.shape[0]), np.complex128)
+        self._check(lib().momed_step_inner_prod(self._h, _p(f), _p(i), f.shape[0], _p(o), len(o), _p(out)))
         return out
 
     # ---------------------------------------------------------------- sparse method

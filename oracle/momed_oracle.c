@@ -1081,6 +1081,34 @@ OR_API void or_rdm1(const uint64_t* basis, int64_t N, const double* psi, int bit
         }
 }
 
+/* ED_step_inner_prod (MomentumED/src/analysis/manybody_quantum_geometry.jl:48-94): for g vectors
+ * psi_f[j], psi_i[k] on one basis, out[j][k] = sum_x conj(psi_f[j][x]) psi_i[k][x] * prod of
+ * orb[o] over the occupied orbitals o of basis[x] (ascending, occ_list).  Vectors [g][N],
+ * orb [norb], out [g][g], all interleaved complex. */
+OR_API void or_step_inner_prod(const uint64_t* basis, int64_t N, const double* psi_f, const double* psi_i, int g,
+                               const double* orb, int norb, double* out) {
+    memset(out, 0, (size_t)g * g * 16);
+    for (int64_t x = 0; x < N; ++x) {
+        double pr = 1.0, pi = 0.0;
+        for (int o = 0; o < norb; ++o) {
+            if (!((basis[x] >> o) & 1ULL)) continue;
+            double r, i;
+            cmul(pr, pi, orb[2 * o], orb[2 * o + 1], &r, &i);
+            pr = r; pi = i;
+        }
+        for (int j = 0; j < g; ++j)
+            for (int k = 0; k < g; ++k) {
+                double fr = psi_f[2 * ((size_t)j * N + x)], fi = -psi_f[2 * ((size_t)j * N + x) + 1];
+                double ir = psi_i[2 * ((size_t)k * N + x)], ii = psi_i[2 * ((size_t)k * N + x) + 1];
+                double cr, ci, vr, vi;
+                cmul(fr, fi, ir, ii, &cr, &ci);
+                cmul(cr, ci, pr, pi, &vr, &vi);
+                out[2 * ((size_t)j * g + k)] += vr;
+                out[2 * ((size_t)j * g + k) + 1] += vi;
+            }
+    }
+}
+
 /* Exact nonzero count of the gather (row, term) hits, the nnz of the roofline formula. */
 OR_API int64_t or_count_hits(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat, int nthreads) {
 #ifdef _OPENMP

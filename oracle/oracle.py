@@ -111,6 +111,8 @@ def lib():
         L.or_bracket.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                  C.c_int64, C.c_int, C.c_void_p]
         L.or_rdm1.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p]
+        L.or_step_inner_prod.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                         C.c_void_p]
         L.or_sparse_csc.restype = C.c_int64
         L.or_sparse_csc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_int64]
@@ -406,6 +408,18 @@ def rdm1(basis, psi, bits: int) -> np.ndarray:
     v = np.ascontiguousarray(psi, np.complex128)
     out = np.zeros((bits, bits), np.complex128)
     lib().or_rdm1(_ptr(bb), len(bb), _ptr(v), int(bits), _ptr(out))
+    return out
+
+
+def step_inner_prod(basis, psi_f, psi_i, orb) -> np.ndarray:
+    """ED_step_inner_prod (manybody_quantum_geometry.jl:48-94): [g, g] from [g, N] vectors."""
+    bb = np.ascontiguousarray(basis, np.uint64)
+    f = np.ascontiguousarray(np.atleast_2d(psi_f), np.complex128)
+    i = np.ascontiguousarray(np.atleast_2d(psi_i), np.complex128)
+    o = np.ascontiguousarray(orb, np.complex128)
+    g = f.shape[0]
+    out = np.zeros((g, g), np.complex128)
+    lib().or_step_inner_prod(_ptr(bb), len(bb), _ptr(f), _ptr(i), g, _ptr(o), len(o), _ptr(out))
     return out
 
 

@@ -125,3 +125,23 @@ def test_rdm1_two_component_eigenvector(h):
     assert got.shape == (bits, bits)
     assert np.max(np.abs(got - want)) < 1e-12
     assert abs(np.trace(got).real - 6) < 1e-9
+
+
+@pytest.mark.parametrize("g", [1, 3])
+def test_step_inner_prod_matches_oracle(h, g):
+    """ED_step_inner_prod (manybody_quantum_geometry.jl:48-94), Abelian (g = 1) and non-Abelian."""
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    basis = ref[5]
+    space = core.HilbertSubspace(basis, 15)
+    rng = np.random.default_rng(g)
+    f = rng.normal(size=(g, len(basis))) + 1j * rng.normal(size=(g, len(basis)))
+    i = rng.normal(size=(g, len(basis))) + 1j * rng.normal(size=(g, len(basis)))
+    orb = np.exp(1j * rng.uniform(0, 2 * np.pi, 15)) * rng.uniform(0.9, 1.0, 15)
+    want = O.step_inner_prod(basis, f, i, orb)
+    if g == 1:
+        got = momed.ED_step_inner_prod(core.MBS64Vector(f[0], space), core.MBS64Vector(i[0], space), orb, handle=h)
+        assert abs(got - want[0, 0]) < 1e-12 * abs(want[0, 0])
+    else:
+        got = momed.ED_step_inner_prod([core.MBS64Vector(v, space) for v in f],
+                                       [core.MBS64Vector(v, space) for v in i], orb, handle=h)
+        assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(want))

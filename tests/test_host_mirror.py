@@ -172,3 +172,19 @@ def test_serving_stream_is_seeded_poisson():
     assert all(0 <= r["sector"] < counts[r["mesh"]] for r in a)
     assert all(1 <= r["nev"] <= 20 and 0.5 <= r["u"] <= 2.0 and r["tol"] == 1e-10 for r in a)
     assert serve_requests(5, meshes, counts, seed=5) != a[:5]
+
+
+def test_connection_gaugefixing_host():
+    """ED_connection_gaugefixing (manybody_quantum_geometry.jl:14-45): the suggested element (one
+    vector) or the determinant of the suggested elements (g vectors) becomes real and positive."""
+    import momed
+    from momed import core
+    space = core.HilbertSubspace(np.arange(1, 9, dtype=np.uint64), 4)
+    rng = np.random.default_rng(0)
+    v = core.MBS64Vector(rng.normal(size=8) + 1j * rng.normal(size=8), space)
+    momed.ED_connection_gaugefixing(v, 3)
+    assert abs(v.vec[2].imag) < 1e-14 and v.vec[2].real > 0
+    vs = [core.MBS64Vector(rng.normal(size=8) + 1j * rng.normal(size=8), space) for _ in range(2)]
+    momed.ED_connection_gaugefixing(vs, [2, 5])
+    d = np.linalg.det(np.array([[w.vec[i - 1] for w in vs] for i in (2, 5)]))
+    assert abs(d.imag) < 1e-12 and d.real > 0
