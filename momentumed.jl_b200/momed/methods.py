@@ -70,6 +70,7 @@ class LinearMap:
         self.scat_list: ScatterList = hermitian_complete(op)
         self.space = space
         self.element_type = et
+        self.hermitian = op.upper_hermitian      # the completed list of an upper operator is Hermitian
 
     @property
     def size(self):
@@ -77,15 +78,22 @@ class LinearMap:
         return (n, n)
 
 
+def adjoint_list(s: ScatterList) -> ScatterList:
+    """Terms of the adjoint operator: conj(amp), in and out swapped, sorted by (in, out)."""
+    order = np.lexsort((s.in_, s.out))
+    return ScatterList(np.conj(s.amp[order]), s.in_[order], s.out[order], s.pm[order], s.bits, s.element_type)
+
+
 class B200LinearMap:
     """The device map (the role of CuLinearMap, MomentumEDCUDAExt.jl:55-139)."""
 
-    def __init__(self, A: LinearMap, device: int = 0, handle: _lib.Handle | None = None):
+    def __init__(self, A: LinearMap, device: int = 0, handle: _lib.Handle | None = None, adjoint: bool = False):
         self.space = A.space
         self.element_type = A.element_type
+        self._A, self._device, self._adjoint = A, device, adjoint
         self.handle = handle or _lib.Handle(device)
         self.handle.set_basis(A.space.list)
-        s = A.scat_list
+        s = adjoint_list(A.scat_list) if adjoint else A.scat_list
         self.handle.set_scatter(s.amp.astype(np.complex128), s.in_, s.out, s.pm)
 
     @property
@@ -106,7 +114,13 @@ class B200LinearMap:
         return out
 
     def adjoint(self):
-        return self        # the map of a Hermitian-completed operator is self-adjoint
+        """The adjoint map (AdjointLinearMap, linear_map.jl:48-55, 120-139; the GPU kernel
+        ka_adjoint_linearmap_kernel!, gpu_interface.jl:170-205): the map of a Hermitian-completed
+        operator is itself; otherwise a device map over the adjoint terms (conjugated amplitudes,
+        creation and annihilation masks swapped), on its own handle."""
+        if self._A.hermitian:
+            return self
+        return B200LinearMap(self._A, self._device, adjoint=not self._adjoint)
 
     def release(self):
         self.handle.close()

@@ -145,3 +145,32 @@ def test_step_inner_prod_matches_oracle(h, g):
         got = momed.ED_step_inner_prod([core.MBS64Vector(v, space) for v in f],
                                        [core.MBS64Vector(v, space) for v in i], orb, handle=h)
         assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(want))
+
+
+def test_adjoint_map_of_non_hermitian_operator(h):
+    """A non-Hermitian operator (the upper two-body list taken as it is): the device map and its
+    adjoint satisfy <y, A x> = <A^H y, x>, and A^H y matches the oracle map of the adjoint terms."""
+    para, _ = mesh_para(3, 5, 0)
+    op = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=False)
+    ref, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    space = core.HilbertSubspace(ref[8], 15)
+    M = momed.create_gpu_linearmap(momed.LinearMap(op, space))
+    Madj = M.adjoint()
+    try:
+        assert Madj is not M
+        rng = np.random.default_rng(4)
+        x = rng.normal(size=len(space)) + 1j * rng.normal(size=len(space))
+        y = rng.normal(size=len(space)) + 1j * rng.normal(size=len(space))
+        ax, ay = M(x), Madj(y)
+        assert relc(np.vdot(y, ax), np.vdot(ay, x)) < 1e-12
+        from momed.methods import adjoint_list
+        assert np.max(np.abs(ay - O.matvec(ref[8], as_oracle(adjoint_list(op.scats)), y))) < 1e-12 * np.max(np.abs(ay))
+        assert np.max(np.abs(ax - O.matvec(ref[8], as_oracle(op.scats), x))) < 1e-12 * np.max(np.abs(ax))
+        # the adjoint of a Hermitian-completed operator is the map itself
+        H = momed.create_gpu_linearmap(momed.LinearMap(momed.MBOperator(
+            momed.ED_scatterlist_twobody(para), upper_hermitian=True), space))
+        assert H.adjoint() is H
+        H.release()
+    finally:
+        Madj.release()
+        M.release()
