@@ -74,7 +74,8 @@ def parse():
     ap.add_argument("--sparse-batch", type=int, default=1,
                     help="also time the headline sweep on the sparse method (1) or not (0)")
     ap.add_argument("--method", default="map", choices=["map", "sparse"],
-                    help="plain workloads: matrix-free map, or the sparse method (device-built CSR + SpMV)")
+                    help="plain workloads (and --profile-only of the sweep): matrix-free map, or the sparse "
+                         "method (device-built CSR + SpMV)")
     ap.add_argument("--serve-requests", type=int, default=80)
     ap.add_argument("--serve-meshes", default="3x5,3x9,3x10", help="subset of 3x5,3x9,3x10,4x9")
     ap.add_argument("--serve-slots", type=int, default=4)
@@ -623,7 +624,13 @@ def main():
         return vals, res, info
 
     if args.profile_only:
-        step_device(order[0])
+        if args.method == "sparse":            # one step of the sweep on the sparse method
+            h.select_sector(order[0], len(sectors[order[0]][1]))
+            h.build_sparse()
+            h.batch_solve(u, NEV, krylovdim=KRYLOV, tol=1e-12, precision=_lib.PREC_MIXED)
+            h.release_sparse()
+        else:
+            step_device(order[0])
         return
 
     for i in range(W):
