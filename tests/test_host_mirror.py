@@ -188,3 +188,41 @@ def test_connection_gaugefixing_host():
     momed.ED_connection_gaugefixing(vs, [2, 5])
     d = np.linalg.det(np.array([[w.vec[i - 1] for w in vs] for i in (2, 5)]))
     assert abs(d.imag) < 1e-12 and d.real > 0
+
+
+def test_analysis_input_checks_on_host():
+    """ED_step_inner_prod refuses mismatched subspaces, vector counts and orbital-overlap lengths
+    before touching a device (the reference's @assert lines, manybody_quantum_geometry.jl:52-53,
+    67-71)."""
+    import momed
+    from momed import core
+    s1 = core.HilbertSubspace(np.array([3, 5, 6], np.uint64), 3)
+    s2 = core.HilbertSubspace(np.array([3, 5], np.uint64), 3)
+    v1 = core.MBS64Vector(np.ones(3, complex), s1)
+    v2 = core.MBS64Vector(np.ones(2, complex), s2)
+    with pytest.raises(AssertionError):
+        momed.ED_step_inner_prod(v1, v2, np.ones(3))
+    with pytest.raises(AssertionError):
+        momed.ED_step_inner_prod(v1, v1, np.ones(4))
+    with pytest.raises(AssertionError):
+        momed.ED_step_inner_prod([v1, v1], [v1], np.ones(3))
+    with pytest.raises(AssertionError):
+        momed.ED_connection_gaugefixing([v1, v1], [1])
+
+
+def test_edsolve_method_checks_on_host():
+    """EDsolve's argument checks (MomentumED.jl:381-387) and the methods this backend leaves to
+    the reference (dense, CPU) fail before any device work."""
+    import momed
+    from momed import core
+    para, _ = mesh_para(3, 5, 0)
+    op = momed.MBOperator(momed.ED_scatterlist_onebody(para), upper_hermitian=True)
+    space = core.HilbertSubspace(np.array([31], np.uint64), 15)
+    with pytest.raises(AssertionError):
+        momed.EDsolve(space, op, N=1, method="lanczos")
+    with pytest.raises(AssertionError):
+        momed.EDsolve(space, op, N=0)
+    with pytest.raises(NotImplementedError):
+        momed.EDsolve(space, op, N=1, method="dense", device="gpu")
+    with pytest.raises(NotImplementedError):
+        momed.EDsolve(space, op, N=1, method="sparse", device="cpu")
