@@ -1,9 +1,9 @@
 """Analysis of eigenvectors on the device.
 
-  - ``ED_bracket`` ........ EDCore/src/multiplication.jl:226-245 (mul_add_bracket 153-173,
-                            mul_add_bracket_scatlist 180-190): <bra| op |ket>, the bra and the
-                            ket on their own subspaces (targets outside the bra space dropped
-                            as index_fit drops them)
+  - ``ED_bracket`` ........ EDCore/src/multiplication.jl:226-245 (mul_add_bracket 153-190,
+                            mul_add_bracket_scatlist 195-222): <bra| op |ket> and
+                            <bra| op2 op1 |ket>, the bra and the ket on their own subspaces
+                            (targets outside the bra space dropped as index_fit drops them)
 
   - ``PES_1rdm`` .......... MomentumED/src/analysis/particle_reduced_density_matrix.jl:4-33:
                             <psi| c+_i c_j |psi> over the subspace's orbitals
@@ -15,7 +15,9 @@
 The bracket runs as one fused map-and-dot kernel (``momed_bracket``): the map's rows run over
 the bra space and its targets are looked up in the ket space, and conj(bra) is folded in per
 row, so H ket is never written.  The two-operator bracket <bra| op2 op1 |ket> of the reference
-scatters through intermediate states outside any subspace and is not provided.
+scatters through intermediate states outside any subspace: they are collected on the host as
+the forward images of the ket space, op1 |ket> is mapped on their union with it, and op2 is
+bracketed against that.
 """
 from __future__ import annotations
 
@@ -25,16 +27,44 @@ from . import _lib
 from .core import MBOperator, MBS64Vector, hermitian_complete
 
 
-def ED_bracket(bra: MBS64Vector, op: MBOperator, ket: MBS64Vector, *, handle: _lib.Handle | None = None) -> complex:
-    """<bra| op |ket> (complex).  An upper_hermitian operator contributes its conjugate terms too."""
-    lst = hermitian_complete(op)
+def forward_images(states: np.ndarray, lst) -> np.ndarray:
+    """Sorted distinct states that one term of lst reaches from any of states (scat * mbs_in,
+    EDCore/src/multiplication.jl:20-34): in within the state, out empty after removing in."""
+    states = np.asarray(states, np.uint64)
+    imgs = []
+    for i_m, o_m in {(int(i), int(o)) for i, o in zip(lst.in_, lst.out)}:
+        im, om = np.uint64(i_m), np.uint64(o_m)
+        mid = states[(states & im) == im] & ~im
+        imgs.append(mid[(mid & om) == 0] | om)
+    return np.unique(np.concatenate(imgs)) if imgs else np.zeros(0, np.uint64)
+
+
+def ED_bracket(bra: MBS64Vector, op: MBOperator, op1_or_ket, ket: MBS64Vector | None = None, *,
+               handle: _lib.Handle | None = None) -> complex:
+    """<bra| op |ket>, or <bra| op2 op1 |ket> called as ED_bracket(bra, op2, op1, ket) (complex).
+    Upper_hermitian operators contribute their conjugate terms too.  The two-operator form
+    passes through every intermediate state op1 reaches: the ket is mapped by op1 on the union
+    of the ket space and those states (found on the host), then bracketed with op2."""
     h = handle or _lib.Handle(0)
     try:
-        h.set_basis(ket.space.list)
-        h.set_scatter(lst.amp.astype(np.complex128), lst.in_, lst.out, lst.pm)
-        same = len(bra.space.list) == len(ket.space.list) and np.array_equal(bra.space.list, ket.space.list)
-        return h.bracket(np.asarray(bra.vec, np.complex128), np.asarray(ket.vec, np.complex128),
-                         None if same else bra.space.list)
+        if ket is None:
+            ket = op1_or_ket
+            lst = hermitian_complete(op)
+            h.set_basis(ket.space.list)
+            h.set_scatter(lst.amp.astype(np.complex128), lst.in_, lst.out, lst.pm)
+            kvec = np.asarray(ket.vec, np.complex128)
+            kspace = ket.space.list
+        else:
+            l1, l2 = hermitian_complete(op1_or_ket), hermitian_complete(op)
+            kspace = np.union1d(forward_images(ket.space.list, l1), ket.space.list).astype(np.uint64)
+            x = np.zeros(len(kspace), np.complex128)
+            x[np.searchsorted(kspace, ket.space.list)] = ket.vec
+            h.set_basis(kspace)
+            h.set_scatter(l1.amp.astype(np.complex128), l1.in_, l1.out, l1.pm)
+            kvec = h.matvec(x)                                   # op1 |ket> on the union
+            h.set_scatter(l2.amp.astype(np.complex128), l2.in_, l2.out, l2.pm)
+        same = len(bra.space.list) == len(kspace) and np.array_equal(bra.space.list, kspace)
+        return h.bracket(np.asarray(bra.vec, np.complex128), kvec, None if same else bra.space.list)
     finally:
         if handle is None:
             h.close()

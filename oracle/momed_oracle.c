@@ -1109,6 +1109,46 @@ OR_API void or_step_inner_prod(const uint64_t* basis, int64_t N, const double* p
     }
 }
 
+/* <bra| op2 op1 |ket> (mul_add_bracket with two Scatters, EDCore/src/multiplication.jl:174-190,
+ * summed over both lists, 215-222): amp, out = scat2 * (scat1 * ket state) with the intermediate
+ * state unrestricted; the final state must lie in the bra space. */
+static int scat_fwd(const or_scat* sc, uint64_t st, uint64_t* out, double* ar, double* ai) {
+    if ((st & sc->in) != sc->in) return 0;
+    if (sc->in == sc->out) { *out = st; *ar = sc->re; *ai = sc->im; return 1; }
+    uint64_t mid = st & ~sc->in;
+    if ((mid & sc->out) != 0) return 0;
+    *out = mid | sc->out;
+    int sign = 1 - 2 * (__builtin_popcountll(mid & sc->pm) & 1);
+    *ar = sign * sc->re; *ai = sign * sc->im;
+    return 1;
+}
+
+OR_API void or_bracket2(const uint64_t* bra_basis, int64_t nbra, const double* bra, const uint64_t* ket_basis,
+                        int64_t nket, const double* ket, const or_scat* l2, int64_t n2, const or_scat* l1,
+                        int64_t n1, double* out) {
+    double sr = 0.0, si = 0.0;
+    for (int64_t a = 0; a < n2; ++a)
+        for (int64_t b = 0; b < n1; ++b)
+            for (int64_t j = 0; j < nket; ++j) {
+                uint64_t m, o;
+                double r1, i1, r2, i2;
+                if (!scat_fwd(&l1[b], ket_basis[j], &m, &r1, &i1)) continue;
+                if (!scat_fwd(&l2[a], m, &o, &r2, &i2)) continue;
+                double ar, ai;
+                cmul(r2, i2, r1, i1, &ar, &ai);
+                if (ar == 0.0 && ai == 0.0) continue;
+                int64_t i = searchsortedfirst(bra_basis, nbra, o);
+                if (i >= nbra || bra_basis[i] != o) continue;
+                double pr, pi, qr, qi;
+                cmul(ar, ai, ket[2 * j], ket[2 * j + 1], &pr, &pi);
+                cmul(bra[2 * i], -bra[2 * i + 1], pr, pi, &qr, &qi);
+                sr += qr;
+                si += qi;
+            }
+    out[0] = sr;
+    out[1] = si;
+}
+
 /* Exact nonzero count of the gather (row, term) hits, the nnz of the roofline formula. */
 OR_API int64_t or_count_hits(const uint64_t* basis, int64_t N, const or_scat* list, int64_t nscat, int nthreads) {
 #ifdef _OPENMP

@@ -113,6 +113,8 @@ def lib():
         L.or_rdm1.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int, C.c_void_p]
         L.or_step_inner_prod.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                          C.c_void_p]
+        L.or_bracket2.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                  C.c_int64, C.c_void_p, C.c_int64, C.c_void_p]
         L.or_sparse_csc.restype = C.c_int64
         L.or_sparse_csc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.c_int64]
@@ -421,6 +423,20 @@ def step_inner_prod(basis, psi_f, psi_i, orb) -> np.ndarray:
     out = np.zeros((g, g), np.complex128)
     lib().or_step_inner_prod(_ptr(bb), len(bb), _ptr(f), _ptr(i), g, _ptr(o), len(o), _ptr(out))
     return out
+
+
+def bracket2(bra_basis, bra, ket_basis, ket, list2, list1) -> complex:
+    """<bra| op2 op1 |ket> over two completed term lists (multiplication.jl:174-190, 215-222)."""
+    bb = np.ascontiguousarray(bra_basis, np.uint64)
+    kb = np.ascontiguousarray(ket_basis, np.uint64)
+    bv = np.ascontiguousarray(bra, np.complex128)
+    kv = np.ascontiguousarray(ket, np.complex128)
+    l2 = np.ascontiguousarray(list2, SCAT_DTYPE)
+    l1 = np.ascontiguousarray(list1, SCAT_DTYPE)
+    out = np.zeros(2)
+    lib().or_bracket2(_ptr(bb), len(bb), _ptr(bv), _ptr(kb), len(kb), _ptr(kv), _ptr(l2), len(l2), _ptr(l1),
+                      len(l1), _ptr(out))
+    return complex(out[0], out[1])
 
 
 def sparse_csc(basis: np.ndarray, full_list: np.ndarray):

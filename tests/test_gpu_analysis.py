@@ -174,3 +174,39 @@ def test_adjoint_map_of_non_hermitian_operator(h):
     finally:
         Madj.release()
         M.release()
+
+
+def test_two_operator_bracket(h):
+    """<bra| op2 op1 |ket> (multiplication.jl:174-190, 215-222) through unrestricted intermediate
+    states: the density-density correlation <psi| rho_-q rho_q |psi> (intermediate sector K + q)
+    and <y| H H |x> = <H y, H x>, against the oracle."""
+    a, b = 3, 5
+    kl = O.mesh_klist(a, b)
+    q = (1, 2)
+
+    def rho(qx, qy):
+        amp, out, inn = [], [], []
+        for k in range(a * b):
+            kq = ((kl[0, k] + qx) % a) + a * ((kl[1, k] + qy) % b)
+            amp.append(1.0)
+            out.append(1 << int(kq))
+            inn.append(1 << k)
+        return momed.MBOperator(core.ScatterList(np.array(amp, complex), np.array(out, np.uint64),
+                                                 np.array(inn, np.uint64)), upper_hermitian=False)
+
+    r_q, r_mq = rho(*q), rho(-q[0], -q[1])
+    ref, _ = O.momentum_subspaces(kl, (a, b), (5,))
+    space = core.HilbertSubspace(ref[2], 15)
+    rng = np.random.default_rng(7)
+    psi = rng.normal(size=len(space)) + 1j * rng.normal(size=len(space))
+    v = core.MBS64Vector(psi, space)
+    got = momed.ED_bracket(v, r_mq, r_q, v, handle=h)
+    want = O.bracket2(ref[2], psi, ref[2], psi, as_oracle(r_mq.scats), as_oracle(r_q.scats))
+    assert abs(want) > 1e-6 and relc(got, want) < 1e-12
+    para, _ = mesh_para(3, 5, 0)
+    H = momed.MBOperator(momed.ED_scatterlist_onebody(para), momed.ED_scatterlist_twobody(para),
+                         upper_hermitian=True)
+    full = as_oracle(core.hermitian_complete(H))
+    y = core.MBS64Vector(rng.normal(size=len(space)) + 0.5j, space)
+    got2 = momed.ED_bracket(y, H, H, v, handle=h)
+    assert relc(got2, np.vdot(O.matvec(ref[2], full, y.vec), O.matvec(ref[2], full, psi))) < 1e-12
