@@ -24,7 +24,8 @@
 // streams coalesced, the x gathers in flight together), shuffle reduction, no atomics.  It
 // streams 4 + s bytes per entry from HBM (column, value) and gathers x, which stays in L2 for
 // sectors up to a few million states.
-#include <numeric>
+#include <algorithm>
+#include <string>
 
 #include "candidates.cuh"
 
