@@ -225,7 +225,7 @@ k_block_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ co
     float ur[RPL];
 #pragma unroll
     for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? __ldg(u + r0 + q) : 0.f;
-    auto entry = [&](int64_t p, float2* acc) {
+    auto entry = [&](int64_t p, float2* acc, float2* accb) {
         const int c = __ldg(col + p);
         const float2 a = __ldg(pa + p);
         float2 b = make_float2(0.f, 0.f);
@@ -244,29 +244,35 @@ k_block_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ co
             for (int q = 0; q < RPL; ++q) xv[q] = __ldg(xp + q);
         }
 #pragma unroll
-        for (int q = 0; q < RPL; ++q) {
-            float cx = a.x, cy = a.y;
+        for (int q = 0; q < RPL; ++q) {     // A and B parts apart; B is scaled by u once per row
+            acc[q].x += a.x * xv[q].x - a.y * xv[q].y;
+            acc[q].y += a.x * xv[q].y + a.y * xv[q].x;
             if (HAS_B) {
-                cx += ur[q] * b.x;
-                cy += ur[q] * b.y;
+                accb[q].x += b.x * xv[q].x - b.y * xv[q].y;
+                accb[q].y += b.x * xv[q].y + b.y * xv[q].x;
             }
-            acc[q].x += cx * xv[q].x - cy * xv[q].y;
-            acc[q].y += cx * xv[q].y + cy * xv[q].x;
         }
     };
     for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
         const int64_t b0 = __ldg(row_ptr + row), e = __ldg(row_ptr + row + 1);
-        float2 acc[RPL];
-#pragma unroll
-        for (int q = 0; q < RPL; ++q) acc[q] = make_float2(0.f, 0.f);
-        int64_t p = b0 + hslot;
-        for (; p + HPI < e; p += 2 * HPI) {
-            entry(p, acc);
-            entry(p + HPI, acc);
-        }
-        if (p < e) entry(p, acc);
+        float2 acc[RPL], accb[RPL];
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
+            acc[q] = make_float2(0.f, 0.f);
+            accb[q] = make_float2(0.f, 0.f);
+        }
+        int64_t p = b0 + hslot;
+        for (; p + HPI < e; p += 2 * HPI) {
+            entry(p, acc, accb);
+            entry(p + HPI, acc, accb);
+        }
+        if (p < e) entry(p, acc, accb);
+#pragma unroll
+        for (int q = 0; q < RPL; ++q) {
+            if (HAS_B) {
+                acc[q].x += ur[q] * accb[q].x;
+                acc[q].y += ur[q] * accb[q].y;
+            }
 #pragma unroll
             for (int o = LPH; o < 32; o <<= 1) {
                 acc[q].x += __shfl_xor_sync(kFull, acc[q].x, o);
