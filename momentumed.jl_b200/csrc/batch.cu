@@ -1272,11 +1272,13 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                 LR.launches = 0;
             }
             if (cycles > 0) {
-                // exact W = H X with the FP64 map, exact residuals, final acceptance
-                for (int i = 0; i < k1; ++i)
+                // exact W = H X with the FP64 map for the nev wanted vectors (the acceptance reads
+                // their residuals; the other anchors enter only through the Ritz values' gaps and
+                // keep W' from the Lanczos relation), exact residuals, final acceptance
+                for (int i = 0; i < nev; ++i)
                     BlockMv<double2>::run(h, Xb.p + (size_t)i * stride, Wb.p + (size_t)i * stride, ud64.p, NB);
-                matvecs += (int64_t)k1 * nu;
-                matvecs64 += (int64_t)k1 * nu;
+                matvecs += (int64_t)nev * nu;
+                matvecs64 += (int64_t)nev * nu;
                 residuals();
                 for (int q = 0; q < nu; ++q)
                     if (!broken[q] && !last_t[q].empty()) accept(q, last_t[q], 1.0);
