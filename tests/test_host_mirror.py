@@ -226,3 +226,29 @@ def test_edsolve_method_checks_on_host():
         momed.EDsolve(space, op, N=1, method="dense", device="gpu")
     with pytest.raises(NotImplementedError):
         momed.EDsolve(space, op, N=1, method="sparse", device="cpu")
+
+
+def test_forward_images_host():
+    """The intermediate states of the two-operator bracket: every state one term reaches from the
+    ket space (scat * mbs_in, multiplication.jl:20-34), against a brute-force application."""
+    from momed.analysis import forward_images
+    from momed import core
+    para, _ = mesh_para(3, 5, 0)
+    op = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=True)
+    lst = core.hermitian_complete(op)
+    sectors, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    states = sectors[1]
+    want = set()
+    for s in (int(v) for v in states):
+        for i_m, o_m in zip(lst.in_.tolist(), lst.out.tolist()):
+            if s & i_m != i_m:
+                continue
+            mid = s & ~i_m
+            if mid & o_m:
+                continue
+            want.add(mid | o_m)
+    got = forward_images(states, lst)
+    assert list(got) == sorted(want)
+    assert np.all(np.diff(got.astype(np.float64)) > 0)
+    # a momentum-conserving operator keeps the sector: the images are the sector's own states
+    assert set(got.tolist()) <= set(int(v) for v in states)
