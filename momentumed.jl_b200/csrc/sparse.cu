@@ -24,6 +24,12 @@
 // streams coalesced, the x gathers in flight together), shuffle reduction, no atomics.  It
 // streams 4 + s bytes per entry from HBM (column, value) and gathers x, which stays in L2 for
 // sectors up to a few million states.
+//
+// For H(u) = A + u B the fill pass also keeps each entry's A and B parts in c64; the batched
+// solver's block SpMV reads them for its FP32 maps (one u per right-hand side), accumulating
+// the A and B products apart and scaling the B sum by u once per row as the matrix-free block
+// map does.  A host matrix (create_gpu_matrix of the reference's host CSC) can be uploaded
+// instead of built (upload_sparse), after validation of its row pointers and columns.
 #include <algorithm>
 #include <string>
 
