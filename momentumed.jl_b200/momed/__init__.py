@@ -7,7 +7,7 @@ MBS64Vector, EDsolve) and every compute step runs in libmomed_b200.so (CUDA,
 sm_100a) through its C ABI.  There is no CPU fallback.
 """
 from ._lib import Handle, MomedError, NotConverged, Server, version
-from .analysis import ED_bracket, ED_connection_gaugefixing, ED_step_inner_prod, PES_1rdm
+from .analysis import ED_bracket, ED_bracket_threaded, ED_connection_gaugefixing, ED_step_inner_prod, PES_1rdm
 from .core import (MBS64, HilbertSubspace, MBOperator, MBS64Vector, Scatter, ScatterList, hermitian_complete,
                    index_fit, make_mask64, occ_list, parity_mask, scat_occ_number, sort_merge_scatlist)
 from .methods import (DEFAULT_GPU, GPU_AVAILABLE, EDsolve, LinearMap, activate_b200, activate_gpu_device,
@@ -18,7 +18,7 @@ from .preparation import (ED_momentum_subspaces, ED_scatterlist_onebody, ED_scat
                           group_momentum_pairs, momentum_residue)
 
 __all__ = [
-    "Handle", "MomedError", "NotConverged", "Server", "version", "ED_bracket", "PES_1rdm",
+    "Handle", "MomedError", "NotConverged", "Server", "version", "ED_bracket", "ED_bracket_threaded", "PES_1rdm",
     "ED_step_inner_prod", "ED_connection_gaugefixing",
     "MBS64", "HilbertSubspace", "MBOperator", "MBS64Vector", "Scatter", "ScatterList", "hermitian_complete",
     "index_fit", "make_mask64", "occ_list", "parity_mask", "scat_occ_number", "sort_merge_scatlist",

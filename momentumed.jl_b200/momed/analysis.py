@@ -27,6 +27,13 @@ from . import _lib
 from .core import MBOperator, MBS64Vector, hermitian_complete
 
 
+def ED_bracket_threaded(bra: MBS64Vector, op: MBOperator, op1_or_ket, ket: MBS64Vector | None = None, *,
+                        handle: _lib.Handle | None = None) -> complex:
+    """ED_bracket_threaded (multiplication.jl:247-286), the reference's multithreaded form: the
+    device bracket is parallel already, so it is ED_bracket."""
+    return ED_bracket(bra, op, op1_or_ket, ket, handle=handle)
+
+
 def forward_images(states: np.ndarray, lst) -> np.ndarray:
     """Sorted distinct states that one term of lst reaches from any of states (scat * mbs_in,
     EDCore/src/multiplication.jl:20-34): in within the state, out empty after removing in."""
