@@ -213,3 +213,20 @@ def test_rdm1_restatement_properties():
     assert abs(np.trace(R) - 5) < 1e-12
     assert np.allclose(np.diag(R).real, (np.abs(x) ** 2) @ occ)
     assert np.max(np.abs(R - np.diag(np.diag(R)))) == 0.0
+
+
+def test_step_inner_prod_restatement_matches_numpy():
+    """ED_step_inner_prod restated (manybody_quantum_geometry.jl:48-94) against a direct numpy
+    evaluation of sum_x conj(f[j][x]) i[k][x] prod_{occupied o} orb[o]."""
+    sectors, _ = O.momentum_subspaces(O.mesh_klist(3, 5), (3, 5), (5,))
+    b = sectors[3]
+    rng = np.random.default_rng(5)
+    g = 2
+    f = rng.normal(size=(g, len(b))) + 1j * rng.normal(size=(g, len(b)))
+    i = rng.normal(size=(g, len(b))) + 1j * rng.normal(size=(g, len(b)))
+    orb = np.exp(1j * rng.uniform(0, 2 * np.pi, 15))
+    occ = np.array([[(int(s) >> o) & 1 for o in range(15)] for s in b], bool)
+    prod = np.array([np.prod(orb[row]) for row in occ])
+    want = np.einsum("jx,kx,x->jk", f.conj(), i, prod)
+    got = O.step_inner_prod(b, f, i, orb)
+    assert np.max(np.abs(got - want)) < 1e-12 * np.max(np.abs(want))
