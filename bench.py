@@ -208,65 +208,98 @@ def barrier(world: int):
 
 
 # ----------------------------------------------------------------------------- CPU arm
-def cpu_reference_solve(basis, pair, u0, nthreads):
-    """The reference's CPU path restated (oracle): gather map over the full term list + FP64 Lanczos."""
+def _oracle():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
+    return O
+
+
+# maps in one bounded sample of the reference arm (the first Krylov cycle of a solve, cut short)
+REF_SAMPLE_MAPS = 12
+
+
+def cpu_reference_solve(basis, pair, u0, nthreads, maxiter=100, krylovdim=None):
+    """The reference's CPU path restated (oracle): gather map over the full term list + FP64 Lanczos."""
+    O = _oracle()
     amp_a, amp_b, in_, out, pm = pair
     full = np.zeros(len(amp_a), O.SCAT_DTYPE)
     amp = amp_a + u0 * amp_b
     full["re"], full["im"], full["out"], full["in"], full["pm"] = amp.real, amp.imag, out, in_, pm
     t0 = time.perf_counter()
-    vals, _, _, info = O.eigsolve(basis, full, NEV, krylovdim=KRYLOV, tol=1e-12, seed=1, nthreads=nthreads,
-                                  want_vectors=True)
+    vals, _, _, info = O.eigsolve(basis, full, NEV, krylovdim=krylovdim or KRYLOV, tol=1e-12, maxiter=maxiter,
+                                  seed=1, nthreads=nthreads, want_vectors=True)
     return time.perf_counter() - t0, vals, info
 
 
+def reference_workload():
+    """Sector bases and the operator pair of the sweep, built by the oracle alone (the reference's
+    host algorithms restated in C): no code of this package runs in the reference arm."""
+    O = _oracle()
+    a, b = MESH
+    bases, _ = O.momentum_subspaces(O.mesh_klist(a, b), (a, b), (NE,))
+    S = O.Synth(a, b, SEED)
+    one = O.hermitian_complete(O.sort_merge(S.onebody()))
+    two = O.hermitian_complete(O.sort_merge(S.twobody()))
+    # H(u) = H0 + u V on the union of the two completed term lists (one-body terms are diagonal)
+    keys = np.concatenate([one[["out", "in"]], two[["out", "in"]]])
+    uk, inv = np.unique(keys, return_inverse=True)
+    amp_a = np.zeros(len(uk), np.complex128)
+    amp_b = np.zeros(len(uk), np.complex128)
+    np.add.at(amp_a, inv[:len(one)], one["re"] + 1j * one["im"])
+    np.add.at(amp_b, inv[len(one):], two["re"] + 1j * two["im"])
+    pm = np.zeros(len(uk), np.uint64)
+    pm[inv[:len(one)]] = one["pm"]
+    pm[inv[len(one):]] = two["pm"]
+    u = 0.5 + 1.5 * np.arange(NU) / (NU - 1)
+    return bases, (amp_a, amp_b, uk["in"].copy(), uk["out"].copy(), pm), u
+
+
 def run_reference(args, rank, world):
-    """--impl reference: the reference CPU path (oracle restatement, all host threads) on this workload."""
+    """--impl reference: the reference's CPU path (the oracle's C restatement of the CPU map
+    linear_map.jl:100-118 and the FP64 Lanczos, all host threads) on this workload.  Rank 0 alone
+    runs.  A full solve takes a minute or more on the host, so each step is a bounded sample: the
+    first REF_SAMPLE_MAPS Lanczos steps (maps with full reorthogonalisation) of the FP64 solve of
+    the step's (sector, U0) pair, the sectors and U0 values in the order of the GPU arm's steps.
+    solves/s = the sampled map rate / the maps of one full solve, counted by one complete solve of
+    the first timed pair before the steps (its own rate is reported beside)."""
     if rank != 0:
         return
-    import momed
-    para, pair, u = workload_operators()
-    h = momed.Handle(0) if _has_gpu() else None
-    if h is not None:
-        sectors = h.enumerate_basis(para.k_list, para.Gk, 1, 1, (NE,))
-    else:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import oracle as O
-        b, ks = O.momentum_subspaces(para.k_list, para.Gk, (NE,))
-        sectors = list(zip(ks, b))
+    bases, pair, u = reference_workload()
+    nsec = len(bases)
     nthreads = os.cpu_count() or 1
-    times = []
-    budget = 150.0
-    t_start = time.perf_counter()
-    for k in range(max(args.steps, 1)):
-        basis = sectors[k % len(sectors)][1]
-        dt, vals, info = cpu_reference_solve(basis, pair, float(u[k % NU]), nthreads)
+    W, K = max(args.warmup, 0), max(args.steps, 1)
+    order = sector_order(0, 1, nsec, W + K)
+    full_t, full_vals, full_info = cpu_reference_solve(bases[order[W]], pair, float(u[W % NU]), nthreads)
+    mv_full = full_info["matvecs"]
+    for i in range(W):
+        cpu_reference_solve(bases[order[i]], pair, float(u[i % NU]), nthreads, maxiter=0, krylovdim=REF_SAMPLE_MAPS)
+    times, mvs = [], []
+    for i in range(K):
+        dt, _, info = cpu_reference_solve(bases[order[W + i]], pair, float(u[(W + i) % NU]), nthreads, maxiter=0,
+                                          krylovdim=REF_SAMPLE_MAPS)
         times.append(dt)
-        if time.perf_counter() - t_start > budget:
-            break
-    value = len(times) / sum(times)
+        mvs.append(info["matvecs"])
+    mv_rate = sum(mvs) / sum(times)
+    value = mv_rate / mv_full
     line = {
         "impl": "reference", "metric": METRIC, "value": value,
-        "unit": "solves/s", "n_gpus": 0, "steps": len(times), "warmup": 0,
-        "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": True, "scaling": "weak",
+        "unit": "solves/s", "n_gpus": 0, "steps": K, "warmup": W,
+        "ms_per_step": 1e3 * sum(times) / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": workload_name(), "solver": "reference CPU map + FP64 Lanczos (oracle restatement), "
-                                                   "one (sector, U0) solve per step"},
+        "config": {"workload": workload_name(),
+                   "solver": "reference CPU map + FP64 Lanczos (oracle restatement), one (sector, U0) pair per "
+                             "step in the GPU arm's order",
+                   "step_sample": f"first {REF_SAMPLE_MAPS} Lanczos steps of the pair's FP64 solve (maps with "
+                                  f"full reorthogonalisation); solves/s = map rate / {mv_full} maps per full solve",
+                   "full_solve": {"seconds": full_t, "matvecs": mv_full, "solves_per_s": 1.0 / full_t,
+                                  "converged": full_info["converged"]}},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads, "kind": "port",
-                         "sample": f"{len(times)} full (sector, U0) solves, {len(sectors[0][1])}-state sector"},
+                         "sample": f"{K} samples of {REF_SAMPLE_MAPS} Lanczos steps ({sum(mvs)} maps) of (sector, U0) solves of "
+                                   f"{len(bases[order[W]])}-state sectors, scaled by one full solve's "
+                                   f"{mv_full} maps"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-def _has_gpu():
-    try:
-        import torch
-        return torch.cuda.is_available()
-    except Exception:
-        return False
 
 
 # ----------------------------------------------------------------------------- serving
@@ -794,13 +827,19 @@ def main():
 
     # ---------------------------------------------------------------- CPU baseline (rank 0, N = 1)
     cpu = None
+    eig_vs_oracle = None
     if rank == 0 and world == 1 and not args.no_cpu:
         basis = sectors[order[W]][1]
         nthreads = os.cpu_count() or 1
-        dt, _, _ = cpu_reference_solve(basis, pair, float(u[0]), nthreads)
+        dt, ovals, _ = cpu_reference_solve(basis, pair, float(u[0]), nthreads)
         cpu = {"value": 1.0 / dt, "unit": "solves/s", "cores": nthreads, "kind": "port",
                "sample": f"1 full FP64 solve (reference CPU map + Lanczos) of one (sector, U0) pair, "
                          f"{len(basis)} states, U0={u[0]:.3f}"}
+        # the batched mixed-precision result of the same (sector, U0) against the FP64 oracle
+        bv = np.asarray(all_vals[0][1])[0]
+        eig_vs_oracle = {"max_rel_err": float(np.max(np.abs(bv - ovals) / np.abs(ovals))),
+                         "per_eigenvalue": [float(v) for v in np.abs(bv - ovals) / np.abs(ovals)],
+                         "pair": f"sector {all_vals[0][0]}, U0={u[0]:.3f}, nev {NEV}"}
 
     serving = None
     if rank == 0 and world == 1 and not args.no_serve and args.serve_requests > 0:
@@ -840,6 +879,7 @@ def main():
                          "launches": n_mv, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "cpu_baseline": cpu,
+            "eig_err_vs_fp64_oracle": eig_vs_oracle,
             "serving": serving,
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(np.mean(h2d)),
                     "d2h_bytes_per_step": int(np.mean(d2h))},

@@ -81,7 +81,7 @@ MOMED_API int  momed_set_stream(momed_handle* h, void* cuda_stream);      /* opt
 MOMED_API int  momed_set_hbm_budget(momed_handle* h, int64_t bytes);      /* admission limit for this handle (0 = free memory) */
 
 /* Kernel (a): basis enumeration per momentum sector.
- * Replaces ED_momentum_subspaces (momentum_decomposition.jl:339-413) without selection_rule.
+ * Replaces ED_momentum_subspaces (momentum_decomposition.jl:188-273) without selection_rule.
  * mask (sorted 1-based orbitals) may be NULL (mlen < 0).  momentum_list (nmom * dim) restricts
  * the sectors when nmom >= 0; nmom < 0 enumerates every momentum in the reference order.
  * The result stays on the device; fetch it with momed_enumeration_copy. */
@@ -100,7 +100,7 @@ MOMED_API int  momed_select_sector(momed_handle* h, int64_t s);
  * pool, or services that reserve all HBM up front).  No counterpart in the reference, whose
  * enumeration runs on the host.  Runs on the current device and the given stream (NULL: the
  * default stream) and returns after the stream has finished it.  Working space is a static
- * 148,608-byte device array per GPU, kept until process exit; the first call on a device
+ * 148,864-byte device array per GPU, kept until process exit; the first call on a device
  * looks its address up and should come before any stream capture; calls that overlap on the
  * GPU race on it.  Limits: momentum box (product of Gk, or of the momentum ranges where
  * Gk == 0) <= 4096 entries.  *n_states receives the sector size; when it exceeds

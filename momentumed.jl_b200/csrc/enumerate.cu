@@ -1,6 +1,6 @@
 // Kernel (a): per-momentum-sector basis enumeration.
 //
-// Reference: ED_momentum_subspaces (MomentumED/src/preparation/momentum_decomposition.jl:339-413)
+// Reference: ED_momentum_subspaces (MomentumED/src/preparation/momentum_decomposition.jl:188-273)
 // recurses over the conserved components, last component outermost and in the
 // highest bits (accumulated_mbs * mbs_smaller, EDCore manybodystate_basis.jl:81-83),
 // each component walked in colex order (EDCore colex_mbslist.jl), and pushes
@@ -529,7 +529,7 @@ void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each
 // library only the output buffer, and services that reserve all of HBM up front for their
 // solve slots and allow no allocation afterwards.  The caller passes the output buffer; the
 // working space (binomial table, momentum-to-sector table, per-block counts and offsets,
-// error counters and the state count) lives in the static array below, 148,608 bytes that
+// error counters and the state count) lives in the static array below, 148,864 bytes that
 // every GPU that loads the library keeps until the process exits.
 //
 // The first call on a device looks the array's device address up (cudaGetSymbolAddress,
@@ -547,7 +547,9 @@ constexpr size_t kNoAllocSecOff = 34048;                                        
 constexpr size_t kNoAllocCntOff = kNoAllocSecOff + 4 * kNoAllocMaxBox;            // int32  [kNoAllocMaxBlocks]
 constexpr size_t kNoAllocOffOff = kNoAllocCntOff + 4 * kNoAllocMaxBlocks;         // int64  [kNoAllocMaxBlocks]
 constexpr size_t kNoAllocErrOff = kNoAllocOffOff + 8 * kNoAllocMaxBlocks;         // uint64 [8] errors, [8] total
-constexpr size_t kNoAllocBytes = kNoAllocErrOff + 16 * 8;                         // 148,608 bytes
+constexpr size_t kNoAllocBytes = kNoAllocErrOff + 16 * 8;                         // 148,864 bytes
+static_assert(kNoAllocBytes == 148864, "the documented size of the no-allocation scratch array");
+static_assert(kNoAllocSecOff >= 65 * 65 * 8 && kNoAllocSecOff % 256 == 0, "binomial table overlaps the sector table");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -701,6 +703,9 @@ extern "C" MOMED_API int momed_enumerate_sector_noalloc(const momed_para* p, con
             note_launches(2);
             MOMED_CUDA_TRY(cudaMemcpyAsync(res, d_err, sizeof(res), cudaMemcpyDeviceToHost, st));
             MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+            MOMED_REQUIRE(res[0] == 0, MOMED_ECUDA, "basis enumeration count pass skipped out-of-range accesses");
+        } else {
+            MOMED_CUDA_TRY(cudaStreamSynchronize(st));   // the table uploads above, before returning
         }
         const int64_t n = (int64_t)res[8];
         *n_states = n;

@@ -11,6 +11,7 @@
 module MomentumEDB200Ext
 
 using MomentumED
+using MomentumED: EDPara, HilbertSubspace, MBS64
 using MomentumED.Methods: GPU_AVAILABLE, DEFAULT_GPU, LinearMap, AbstractGPULinearMap
 import MomentumED.Methods: create_gpu_linearmap, krylov_map_solve, release_gpu_memory
 import MomentumED.Methods: create_gpu_matrix, krylov_matrix_solve
@@ -28,6 +29,15 @@ struct MomedSolveOpts
     seed::UInt64
     want_vectors::Int32
     vecs_on_device::Int32
+end
+
+struct MomedPara
+    dim::Int32
+    Nk::Int32
+    Nc_mix::Int32
+    Nc_conserve::Int32
+    k_list::Ptr{Int64}
+    Gk::Ptr{Int64}
 end
 
 mutable struct MomedInfo
@@ -113,13 +123,26 @@ function krylov_map_solve(H::B200LinearMap{bits, F}, N_eigen::Int64; ishermitian
     vals = zeros(Float64, nev)
     resid = zeros(Float64, nev)
     vecs = zeros(ComplexF64, m, nev)            # column i = eigenvector i (layout [nev][N] in C)
-    v0 = vec0 === nothing ? C_NULL : pointer(ComplexF64.(vec0))
     info = MomedInfo()
-    check(H.handle, ccall((:momed_eigsolve, libmomed), Cint,
-                          (Ptr{Cvoid}, Ref{MomedSolveOpts}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{ComplexF64},
-                           Ref{MomedInfo}),
-                          H.handle, opts, v0, vals, resid, vecs, info))
+    eigsolve_call(H.handle, opts, vec0, vals, resid, vecs, info)
     return vals, [Vector{Complex{F}}(vecs[:, i]) for i in 1:nev], info
+end
+
+# momed_eigsolve with the start vector converted to a ComplexF64 buffer that stays rooted for the
+# whole call (the conversion makes a new array: it must be bound to a live variable, not passed as
+# a temporary's pointer, or the collector may free it while the library reads it).
+function eigsolve_call(h::Ptr{Cvoid}, opts::MomedSolveOpts, vec0, vals::Vector{Float64},
+                       resid::Vector{Float64}, vecs::Matrix{ComplexF64}, info::MomedInfo)
+    v0buf = vec0 === nothing ? ComplexF64[] : Vector{ComplexF64}(vec0)
+    vec0 === nothing || length(v0buf) == size(vecs, 1) || error("vec0 has length $(length(v0buf)), expected $(size(vecs, 1))")
+    GC.@preserve v0buf begin
+        v0 = vec0 === nothing ? Ptr{ComplexF64}(C_NULL) : pointer(v0buf)
+        check(h, ccall((:momed_eigsolve, libmomed), Cint,
+                       (Ptr{Cvoid}, Ref{MomedSolveOpts}, Ptr{ComplexF64}, Ptr{Float64}, Ptr{Float64}, Ptr{ComplexF64},
+                        Ref{MomedInfo}),
+                       h, opts, v0, vals, resid, vecs, info))
+    end
+    return nothing
 end
 
 # Sparse method hooks (EDsolve(...; method=:sparse, device=:gpu), MomentumEDCUDAExt.jl:145-200).
@@ -157,13 +180,67 @@ function krylov_matrix_solve(H::B200SparseMatrix{F}, N_eigen::Int64; ishermitian
     vals = zeros(Float64, nev)
     resid = zeros(Float64, nev)
     vecs = zeros(ComplexF64, H.n, nev)
-    v0 = vec0 === nothing ? C_NULL : pointer(ComplexF64.(vec0))
     info = MomedInfo()
-    check(H.handle, ccall((:momed_eigsolve, libmomed), Cint,
-                          (Ptr{Cvoid}, Ref{MomedSolveOpts}, Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{ComplexF64},
-                           Ref{MomedInfo}),
-                          H.handle, opts, v0, vals, resid, vecs, info))
+    eigsolve_call(H.handle, opts, vec0, vals, resid, vecs, info)
     return vals, [Vector{Complex{F}}(vecs[:, i]) for i in 1:nev], info
+end
+
+# ED_momentum_subspaces on the device (kernel (a)): the reference enumerates on host threads
+# (MomentumED/src/preparation/momentum_decomposition.jl:188-273).  Selected with a trailing
+# Val(:b200), so the reference's own methods stay as they are:
+#     subspaces, subspace_k = ED_momentum_subspaces(para, (Ne,), Val(:b200))
+# Same keywords, same result (sectors in the reference order, empty ones dropped, each list
+# sorted); a selection_rule other than the default is applied on the host to each sector.
+function MomentumED.ED_momentum_subspaces(para::EDPara{dim}, N_each_component, ::Val{:b200};
+        momentum_restriction::Bool = false, momentum_list::Vector{NTuple{dim, Int64}} = NTuple{dim, Int64}[],
+        mask::Union{Nothing, Vector{Int64}} = nothing,
+        selection_rule::Function = Returns(true)) where {dim}
+    Ns = N_each_component isa Integer ? Int64[N_each_component] : Int64[n for n in N_each_component]
+    @assert length(Ns) == para.Nc_conserve "The length of number_list must be equal to the number of conserved components $(para.Nc_conserve)"
+    bits = para.Nk * para.Nc
+    momentum_restriction && isempty(momentum_list) &&
+        return HilbertSubspace{bits}[], NTuple{dim, Int64}[]
+    klist = Matrix{Int64}(para.k_list)                 # dim x Nk, column-major: k_list[d + dim*i]
+    Gk = Int64[para.Gk...]
+    maskv = mask === nothing ? Int64[] : sort(mask)
+    moms = momentum_restriction ? Int64[m[d] for m in momentum_list for d in 1:dim] : Int64[]
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(C_NULL, ccall((:momed_create, libmomed), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, h))
+    try
+        nsec, ntot = Ref{Int64}(0), Ref{Int64}(0)
+        GC.@preserve klist Gk maskv moms Ns begin
+            p = MomedPara(Int32(dim), Int32(para.Nk), Int32(para.Nc_mix), Int32(para.Nc_conserve),
+                          pointer(klist), pointer(Gk))
+            check(h[], ccall((:momed_enumerate_basis, libmomed), Cint,
+                             (Ptr{Cvoid}, Ref{MomedPara}, Ptr{Int64}, Int32, Ptr{Int64}, Int32, Ptr{Int64}, Int32,
+                              Ref{Int64}, Ref{Int64}),
+                             h[], p, Ns, Int32(length(Ns)),
+                             mask === nothing ? Ptr{Int64}(C_NULL) : pointer(maskv),
+                             Int32(mask === nothing ? -1 : length(maskv)),
+                             momentum_restriction ? pointer(moms) : Ptr{Int64}(C_NULL),
+                             Int32(momentum_restriction ? length(momentum_list) : -1), nsec, ntot))
+        end
+        sector_k = Vector{Int64}(undef, max(nsec[] * dim, 1))
+        sizes = Vector{Int64}(undef, max(nsec[], 1))
+        basis = Vector{UInt64}(undef, max(ntot[], 1))
+        check(h[], ccall((:momed_enumeration_copy, libmomed), Cint,
+                         (Ptr{Cvoid}, Ptr{Int64}, Ptr{Int64}, Ptr{UInt64}, Int32),
+                         h[], sector_k, sizes, basis, Int32(0)))
+        subspaces = HilbertSubspace{bits}[]
+        subspace_k = NTuple{dim, Int64}[]
+        off = 0
+        for s in 1:nsec[]
+            list = MBS64{bits}[MBS64{bits}(basis[off + i]) for i in 1:sizes[s]]
+            off += sizes[s]
+            selection_rule === Returns(true) || filter!(selection_rule, list)
+            isempty(list) && continue
+            push!(subspaces, HilbertSubspace(list))
+            push!(subspace_k, ntuple(d -> sector_k[(s - 1) * dim + d], Val(dim)))
+        end
+        return subspaces, subspace_k
+    finally
+        ccall((:momed_destroy, libmomed), Cint, (Ptr{Cvoid},), h[])
+    end
 end
 
 # release_gpu_memory hook: device buffers belong to handles (freed by their finalizers).

@@ -220,11 +220,17 @@ def release_gpu_memory(device: str = "b200", level: int = 2):
     return None
 
 
-def EDsolve(subspace: HilbertSubspace, Hamiltonian: MBOperator, *, N: int, method: str = "map",
+def EDsolve(subspace: HilbertSubspace, *Hamiltonian, N: int, method: str | None = None,
             device: str = "gpu", showtime: bool = False, ishermitian: bool = True, element_type=None,
             index_type=np.int32, map_warning_dim: int = 20000, method_info: bool = True, **krylovkit_kwargs):
-    """Lowest N eigenpairs of ``Hamiltonian`` in ``subspace`` (MomentumED.jl:375-480, :map or :sparse
-    on the GPU).
+    """Lowest N eigenpairs of the Hamiltonian in ``subspace`` on the GPU.
+
+    Two forms, as in the reference: ``EDsolve(subspace, H::MBOperator; N, method=:map)``
+    (MomentumED.jl:375-480; :map or :sparse) and ``EDsolve(subspace, scat_lists...; N,
+    method=:sparse)`` (MomentumED.jl:217-372) with one or more scatter lists, whose matrix is built
+    on the device from their sum (upper-Hermitian lists when ``ishermitian``).  The list form has
+    no matrix-free method (the reference refuses :map there too), and this backend has no dense
+    method, so small sectors also run on the device's sparse method.
 
     Returns ``(energies, vectors)`` with ``vectors`` a list of ``MBS64Vector``.
     ``krylovkit_kwargs`` accepts krylovdim, tol, maxiter, vec0, seed and precision ("fp64"/"mixed").
@@ -232,6 +238,17 @@ def EDsolve(subspace: HilbertSubspace, Hamiltonian: MBOperator, *, N: int, metho
     import time
     import warnings
 
+    if len(Hamiltonian) == 1 and isinstance(Hamiltonian[0], MBOperator):
+        Hamiltonian = Hamiltonian[0]
+        method = "map" if method is None else method
+    else:
+        if not Hamiltonian or not all(isinstance(h, ScatterList) for h in Hamiltonian):
+            raise TypeError("EDsolve takes one MBOperator or one or more scatter lists")
+        method = "sparse" if method is None else method
+        if method == "map":
+            raise ValueError("Linear map methods are only supported when input Hamitonian is MBOperator instead of "
+                             "Vector{Scatter}.")
+        Hamiltonian = MBOperator(*Hamiltonian, upper_hermitian=ishermitian)
     if N < 1:
         raise AssertionError("N should be at least 1.")
     if len(subspace) > np.iinfo(index_type).max:

@@ -2,7 +2,7 @@
 
   - ``EDPara`` ........................ MomentumED/src/preparation/init_parameter.jl:62-146
   - ``momentum_residue`` / ``MBS_totalmomentum`` .. init_parameter.jl:148-152, momentum_decomposition.jl:49-77
-  - ``ED_momentum_subspaces`` ......... momentum_decomposition.jl:339-423 (device kernel (a))
+  - ``ED_momentum_subspaces`` ......... momentum_decomposition.jl:188-273 (device kernel (a))
   - ``group_momentum_pairs`` .......... scat_list.jl:174-200
   - ``ED_scatterlist_onebody/twobody`` . scat_list.jl:78-142, 425-572
 

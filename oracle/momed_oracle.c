@@ -506,6 +506,25 @@ typedef void (*or_h2_fn)(void* ctx, int64_t kf1, int64_t kf2, int64_t ki2, int64
 typedef void (*or_h1c_fn)(void* ctx, const double* k, int64_t cf, int64_t ci, double* re, double* im);
 typedef void (*or_h2c_fn)(void* ctx, const double* kf1, const double* kf2, const double* ki2, const double* ki1,
                           int64_t cf1, int64_t cf2, int64_t ci2, int64_t ci1, double* re, double* im);
+/* Rational-coordinate mode (scat_list.jl:5-16, the default when kshift is nothing, an integer
+ * or a rational): each coordinate is passed as an exact fraction, k[2d] / k[2d + 1] for
+ * direction d (not reduced), k/Gk + shift/Gk where Gk != 0 and k + shift where Gk == 0; the
+ * shift of conserved component c is rshift[2(d + dim c)] / rshift[2(d + dim c) + 1]. */
+typedef void (*or_h1r_fn)(void* ctx, const int64_t* k, int64_t cf, int64_t ci, double* re, double* im);
+typedef void (*or_h2r_fn)(void* ctx, const int64_t* kf1, const int64_t* kf2, const int64_t* ki2, const int64_t* ki1,
+                          int64_t cf1, int64_t cf2, int64_t ci2, int64_t ci1, double* re, double* im);
+
+/* exact coordinate of momentum index k (1-based) of conserved component cc (1-based) */
+static void rational_coord(const or_para* p, const int64_t* rshift, int k, int cc, int64_t* out) {
+    for (int d = 0; d < p->dim; ++d) {
+        int64_t kv = p->k_list[d + p->dim * (k - 1)];
+        int64_t sn = rshift ? rshift[2 * (d + p->dim * (cc - 1))] : 0;
+        int64_t sd = rshift ? rshift[2 * (d + p->dim * (cc - 1)) + 1] : 1;
+        int64_t g = p->Gk[d] != 0 ? p->Gk[d] : 1;
+        out[2 * d] = kv * sd + sn;
+        out[2 * d + 1] = g * sd;
+    }
+}
 
 static int64_t push_scat(or_scat* out, int64_t cap, int64_t n, const or_scat* s) {
     if (out && n < cap) out[n] = *s;
@@ -515,8 +534,8 @@ static int64_t push_scat(or_scat* out, int64_t cap, int64_t n, const or_scat* s)
 /* scat_list.jl:78-142 (index mode at 126-138, coordinate mode at 92-118).
  * prec 32 rounds H_one's value to Complex{Float32}.  Returns the sorted-merged count,
  * the merged list in out (capacity cap); when out == NULL it returns the raw term count. */
-static int64_t onebody_common(const or_para* p, or_h1_fn f, or_h1c_fn fc, void* ctx,
-                              const double* shift /* [dim*Ncc] or NULL */, int prec,
+static int64_t onebody_common(const or_para* p, or_h1_fn f, or_h1c_fn fc, or_h1r_fn fr, void* ctx,
+                              const double* shift /* [dim*Ncc] or NULL */, const int64_t* rshift, int prec,
                               or_scat* out, int64_t cap) {
     int Nk = p->Nk, Ncm = p->Nc_mix, Ncc = p->Nc_conserve, dim = p->dim;
     int64_t n = 0;
@@ -530,7 +549,11 @@ static int64_t onebody_common(const or_para* p, or_h1_fn f, or_h1c_fn fc, void* 
                     int i_out = k + Nk * (cf - 1), i_in = k + Nk * (ci - 1);
                     if (i_in >= i_out) {
                         double re = 0, im = 0;
-                        if (fc) {
+                        if (fr) {
+                            int64_t kr[16];
+                            rational_coord(p, rshift, k, cc, kr);
+                            fr(ctx, kr, cf, ci, &re, &im);
+                        } else if (fc) {
                             double kc[8];
                             for (int d = 0; d < dim; ++d) {
                                 double kv = (double)p->k_list[d + dim * (k - 1)];
@@ -560,11 +583,15 @@ static int64_t onebody_common(const or_para* p, or_h1_fn f, or_h1c_fn fc, void* 
     return m;
 }
 OR_API int64_t or_scatterlist_onebody(const or_para* p, or_h1_fn f, void* ctx, int prec, or_scat* out, int64_t cap) {
-    return onebody_common(p, f, NULL, ctx, NULL, prec, out, cap);
+    return onebody_common(p, f, NULL, NULL, ctx, NULL, NULL, prec, out, cap);
 }
 OR_API int64_t or_scatterlist_onebody_coord(const or_para* p, or_h1c_fn f, void* ctx, const double* shift,
                                             int prec, or_scat* out, int64_t cap) {
-    return onebody_common(p, NULL, f, ctx, shift, prec, out, cap);
+    return onebody_common(p, NULL, f, NULL, ctx, shift, NULL, prec, out, cap);
+}
+OR_API int64_t or_scatterlist_onebody_rational(const or_para* p, or_h1r_fn f, void* ctx, const int64_t* rshift,
+                                               int prec, or_scat* out, int64_t cap) {
+    return onebody_common(p, NULL, NULL, f, ctx, NULL, rshift, prec, out, cap);
 }
 
 /* group_momentum_pairs: scat_list.jl:174-200.  Pairs (i, j), i >= j, 1-based, keyed by
@@ -572,8 +599,8 @@ OR_API int64_t or_scatterlist_onebody_coord(const or_para* p, or_h1c_fn f, void*
  * (each (in, out) key is produced once), so groups are walked in first-appearance order. */
 typedef struct { int i, j; int64_t K[8]; } pair_t;
 
-static int64_t twobody_common(const or_para* p, or_h2_fn f, or_h2c_fn fc, void* ctx,
-                              const double* shift, int prec, or_scat* out, int64_t cap) {
+static int64_t twobody_common(const or_para* p, or_h2_fn f, or_h2c_fn fc, or_h2r_fn fr, void* ctx,
+                              const double* shift, const int64_t* rshift, int prec, or_scat* out, int64_t cap) {
     int Nk = p->Nk, Nc = p->Nc_mix * p->Nc_conserve, Ncm = p->Nc_mix, dim = p->dim;
     int all_nonzero = 1;
     for (int d = 0; d < dim; ++d) if (p->Gk[d] == 0) all_nonzero = 0;
@@ -623,7 +650,14 @@ static int64_t twobody_common(const or_para* p, or_h2_fn f, or_h2c_fn fc, void* 
                     int fmin = f1 < f2 ? f1 : f2, fmax = f1 < f2 ? f2 : f1;
                     if (!(imin > fmin || (imin == fmin && imax >= fmax))) continue;   /* minmax >= */
                     double dr, di, er, ei;
-                    if (fc) {
+                    if (fr) {
+                        int ks[4] = {kf1, kf2, ki2, ki1};
+                        int cs[4] = {(cf1 - 1) / Ncm + 1, (cf2 - 1) / Ncm + 1, (ci2 - 1) / Ncm + 1, (ci1 - 1) / Ncm + 1};
+                        int64_t kr[4][16];
+                        for (int q = 0; q < 4; ++q) rational_coord(p, rshift, ks[q], cs[q], kr[q]);
+                        fr(ctx, kr[0], kr[1], kr[2], kr[3], cf1, cf2, ci2, ci1, &dr, &di);
+                        fr(ctx, kr[0], kr[1], kr[3], kr[2], cf1, cf2, ci1, ci2, &er, &ei);
+                    } else if (fc) {
                         int ks[4] = {kf1, kf2, ki2, ki1};
                         int cs[4] = {(cf1 - 1) / Ncm + 1, (cf2 - 1) / Ncm + 1, (ci2 - 1) / Ncm + 1, (ci1 - 1) / Ncm + 1};
                         for (int q = 0; q < 4; ++q)
@@ -668,11 +702,15 @@ static int64_t twobody_common(const or_para* p, or_h2_fn f, or_h2c_fn fc, void* 
     return m;
 }
 OR_API int64_t or_scatterlist_twobody(const or_para* p, or_h2_fn f, void* ctx, int prec, or_scat* out, int64_t cap) {
-    return twobody_common(p, f, NULL, ctx, NULL, prec, out, cap);
+    return twobody_common(p, f, NULL, NULL, ctx, NULL, NULL, prec, out, cap);
 }
 OR_API int64_t or_scatterlist_twobody_coord(const or_para* p, or_h2c_fn f, void* ctx, const double* shift,
                                             int prec, or_scat* out, int64_t cap) {
-    return twobody_common(p, NULL, f, ctx, shift, prec, out, cap);
+    return twobody_common(p, NULL, f, NULL, ctx, shift, NULL, prec, out, cap);
+}
+OR_API int64_t or_scatterlist_twobody_rational(const or_para* p, or_h2r_fn f, void* ctx, const int64_t* rshift,
+                                               int prec, or_scat* out, int64_t cap) {
+    return twobody_common(p, NULL, NULL, f, ctx, NULL, rshift, prec, out, cap);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -767,10 +805,10 @@ OR_API void or_mesh_klist(int a, int b, int64_t* k_list) {
     for (int i = 0; i < a * b; ++i) { k_list[2 * i] = i % a; k_list[2 * i + 1] = i / a; }
 }
 OR_API int64_t or_synth_onebody(const or_para* p, or_synth* S, int prec, or_scat* out, int64_t cap) {
-    return onebody_common(p, or_synth_h1, NULL, S, NULL, prec, out, cap);
+    return onebody_common(p, or_synth_h1, NULL, NULL, S, NULL, NULL, prec, out, cap);
 }
 OR_API int64_t or_synth_twobody(const or_para* p, or_synth* S, int prec, or_scat* out, int64_t cap) {
-    return twobody_common(p, or_synth_h2, NULL, S, NULL, prec, out, cap);
+    return twobody_common(p, or_synth_h2, NULL, NULL, S, NULL, NULL, prec, out, cap);
 }
 
 /* scat * mbs_in (EDCore/src/multiplication.jl:19-33): returns 1 and writes (amp, out state)

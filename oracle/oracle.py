@@ -14,6 +14,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 import subprocess
+from fractions import Fraction
 
 import numpy as np
 
@@ -48,6 +49,17 @@ H1_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_int64, C.c_int64,
 H2_FN = C.CFUNCTYPE(None, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
                     C.c_int64, C.c_int64, C.c_int64, C.c_int64,
                     C.POINTER(C.c_double), C.POINTER(C.c_double))
+
+H1C_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.c_int64, C.c_int64,
+                     C.POINTER(C.c_double), C.POINTER(C.c_double))
+H2C_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                     C.POINTER(C.c_double), C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                     C.POINTER(C.c_double), C.POINTER(C.c_double))
+H1R_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_int64), C.c_int64, C.c_int64,
+                     C.POINTER(C.c_double), C.POINTER(C.c_double))
+H2R_FN = C.CFUNCTYPE(None, C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64),
+                     C.POINTER(C.c_int64), C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                     C.POINTER(C.c_double), C.POINTER(C.c_double))
 
 _lib = None
 
@@ -97,6 +109,18 @@ def lib():
         L.or_scatterlist_onebody.argtypes = [C.POINTER(_Para), H1_FN, C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
         L.or_scatterlist_twobody.restype = C.c_int64
         L.or_scatterlist_twobody.argtypes = [C.POINTER(_Para), H2_FN, C.c_void_p, C.c_int, C.c_void_p, C.c_int64]
+        L.or_scatterlist_onebody_coord.restype = C.c_int64
+        L.or_scatterlist_onebody_coord.argtypes = [C.POINTER(_Para), H1C_FN, C.c_void_p, C.c_void_p, C.c_int,
+                                                   C.c_void_p, C.c_int64]
+        L.or_scatterlist_twobody_coord.restype = C.c_int64
+        L.or_scatterlist_twobody_coord.argtypes = [C.POINTER(_Para), H2C_FN, C.c_void_p, C.c_void_p, C.c_int,
+                                                   C.c_void_p, C.c_int64]
+        L.or_scatterlist_onebody_rational.restype = C.c_int64
+        L.or_scatterlist_onebody_rational.argtypes = [C.POINTER(_Para), H1R_FN, C.c_void_p, C.c_void_p, C.c_int,
+                                                      C.c_void_p, C.c_int64]
+        L.or_scatterlist_twobody_rational.restype = C.c_int64
+        L.or_scatterlist_twobody_rational.argtypes = [C.POINTER(_Para), H2R_FN, C.c_void_p, C.c_void_p, C.c_int,
+                                                      C.c_void_p, C.c_int64]
         L.or_synth_init.argtypes = [C.POINTER(_Synth), C.c_int, C.c_int, C.c_uint64]
         L.or_synth_free.argtypes = [C.POINTER(_Synth)]
         L.or_synth_onebody.restype = C.c_int64
@@ -352,6 +376,98 @@ def scatterlist_twobody(k_list, Gk, H_two, Nc_mix=1, Nc_conserve=1, prec=64) -> 
 
 
 # --------------------------------------------------------------------------- matvec / eig
+def shift_matrix(kshift, Ncc: int, dim: int):
+    """kshift -> shifts[d][c] (scat_list.jl:29-50): None -> zeros, a tuple -> the same shift for
+    every conserved component, a list of Ncc tuples -> one per component, a dim x Ncc array."""
+    if kshift is None:
+        return [[0] * Ncc for _ in range(dim)]
+    if isinstance(kshift, tuple):
+        return [[kshift[d] for _ in range(Ncc)] for d in range(dim)]
+    if isinstance(kshift, list):
+        assert len(kshift) == Ncc, "length of kshift isn't equal to para.Nc_conserve."
+        return [[kshift[c][d] for c in range(Ncc)] for d in range(dim)]
+    a = np.asarray(kshift)
+    assert a.shape == (dim, Ncc), "size of kshift isn't equal to para.Nc_conserve."
+    return [[a[d, c].item() for c in range(Ncc)] for d in range(dim)]
+
+
+def _exact(shifts) -> bool:
+    """scat_list.jl:453-457: integer and rational shifts keep coordinates exact (Rational), any
+    float makes them Float64."""
+    return all(isinstance(v, (int, np.integer, Fraction)) for row in shifts for v in row)
+
+
+def _coord_call(k_list, Gk, Nc_mix, Nc_conserve, kshift, prec, onebody, fn):
+    p = _para(k_list, Gk, Nc_mix, Nc_conserve)
+    dim = p.dim
+    shifts = shift_matrix(kshift, Nc_conserve, dim)
+    L = lib()
+    if _exact(shifts):
+        rs = np.zeros(2 * dim * Nc_conserve, np.int64)
+        for d in range(dim):
+            for c in range(Nc_conserve):
+                f = Fraction(shifts[d][c])
+                rs[2 * (d + dim * c)], rs[2 * (d + dim * c) + 1] = f.numerator, f.denominator
+
+        def co(k):
+            return tuple(Fraction(int(k[2 * d]), int(k[2 * d + 1])) for d in range(dim))
+
+        if onebody:
+            @H1R_FN
+            def cb(ctx, k, cf, ci, re, im):
+                v = complex(fn(co(k), cf, ci))
+                re[0], im[0] = v.real, v.imag
+            build = L.or_scatterlist_onebody_rational
+        else:
+            @H2R_FN
+            def cb(ctx, a, b, c, d, cf1, cf2, ci2, ci1, re, im):
+                v = complex(fn(co(a), co(b), co(c), co(d), cf1, cf2, ci2, ci1))
+                re[0], im[0] = v.real, v.imag
+            build = L.or_scatterlist_twobody_rational
+        sh = rs
+    else:
+        sh = np.zeros(dim * Nc_conserve, np.float64)
+        for d in range(dim):
+            for c in range(Nc_conserve):
+                sh[d + dim * c] = float(shifts[d][c])
+
+        def co(k):
+            return tuple(float(k[d]) for d in range(dim))
+
+        if onebody:
+            @H1C_FN
+            def cb(ctx, k, cf, ci, re, im):
+                v = complex(fn(co(k), cf, ci))
+                re[0], im[0] = v.real, v.imag
+            build = L.or_scatterlist_onebody_coord
+        else:
+            @H2C_FN
+            def cb(ctx, a, b, c, d, cf1, cf2, ci2, ci1, re, im):
+                v = complex(fn(co(a), co(b), co(c), co(d), cf1, cf2, ci2, ci1))
+                re[0], im[0] = v.real, v.imag
+            build = L.or_scatterlist_twobody_coord
+        sh = sh
+    n = build(C.byref(p), cb, None, _ptr(sh), prec, None, 0)
+    out = np.zeros(max(n, 1), SCAT_DTYPE)
+    m = build(C.byref(p), cb, None, _ptr(sh), prec, _ptr(out), len(out))
+    if m < 0:
+        raise RuntimeError("builder failed")
+    return out[:m].copy()
+
+
+def scatterlist_onebody_coord(k_list, Gk, H_one, Nc_mix=1, Nc_conserve=1, kshift=None, prec=64) -> np.ndarray:
+    """ED_scatterlist_onebody with a coordinate-mode callable H_one(k::tuple, cf, ci)
+    (scat_list.jl:78-142): k is k/Gk (+ the component's kshift/Gk) as Fractions for integer or
+    rational shifts (the default) and as floats otherwise."""
+    return _coord_call(k_list, Gk, Nc_mix, Nc_conserve, kshift, prec, True, H_one)
+
+
+def scatterlist_twobody_coord(k_list, Gk, H_two, Nc_mix=1, Nc_conserve=1, kshift=None, prec=64) -> np.ndarray:
+    """ED_scatterlist_twobody with a coordinate-mode callable H_two(kf1, kf2, ki2, ki1, cf1, cf2, ci2, ci1)
+    (scat_list.jl:442-514), coordinates as in scatterlist_onebody_coord."""
+    return _coord_call(k_list, Gk, Nc_mix, Nc_conserve, kshift, prec, False, H_two)
+
+
 def matvec(basis: np.ndarray, full_list: np.ndarray, x: np.ndarray, nthreads: int = 0) -> np.ndarray:
     """Reference CPU map y = H x over the Hermitian-completed list (complex128 or complex64)."""
     basis = np.ascontiguousarray(basis, np.uint64)
