@@ -435,6 +435,13 @@ def mv_bytes(N: int, nnz: int, nscat: int, s: int) -> float:
     return N * (8 + 2 * s) + nnz * s + nscat * (s + 24)
 
 
+def block_size(nev: int, N: int) -> int:
+    """Block size the eigensolver picks for nev pairs on N states (0: single-vector Lanczos)."""
+    if nev < 2 or N < 16384:
+        return 0
+    return 4 if nev <= 4 else (8 if nev <= 10 else 16)
+
+
 def sp_bytes(N: int, nnz_sp: int, s: int) -> float:
     """Algorithmic HBM bytes of one CSR SpMV: the column and value of every stored entry, the row
     pointers, and x and y once each (x, at most a few tens of MB here, serves its gathers from L2)."""
@@ -501,7 +508,13 @@ def run_plain_workload(args, rank, world, local):
     barrier(world)
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(K)]
     n_mv, ms_mv = h.profile_read(_lib.KERNEL_SPMV_C128 if sparse else _lib.KERNEL_MATVEC_C128)
+    n_bmv, ms_bmv = h.profile_read(_lib.KERNEL_BLOCK_MATVEC_C128)
     h.profile(False)
+    # nev >= 2 on large sectors runs the block solver (block_size_for in block_lanczos.cu): its maps
+    # are block maps of B right-hand sides, the single-vector launches only the final residual maps
+    bsz = block_size(nev, len(sectors[order[W]][1])) if not sparse else 0
+    if bsz and n_bmv > 0:
+        n_mv, ms_mv = n_bmv, ms_bmv
     launches = _lib.kernel_launches() - launches0
     elapsed = all_max(sum(step_ms) / 1e3, world)
     value = all_sum(K, world) / elapsed
@@ -517,6 +530,9 @@ def run_plain_workload(args, rank, world, local):
             build_ms.append((time.perf_counter() - t0) * 1e3)
             nb.append(sp_bytes(len(sectors[sidx][1]), nsp, 16))
             nnz_mean.append(nsp)
+        elif bsz:
+            nb.append(block_bytes(len(sectors[sidx][1]), st["nnz"], len(pair[0]), bsz, 16))
+            nnz_mean.append(st["nnz"])
         else:
             nb.append(mv_bytes(len(sectors[sidx][1]), st["nnz"], len(pair[0]), 16))
             nnz_mean.append(st["nnz"])
@@ -580,6 +596,9 @@ def run_plain_workload(args, rank, world, local):
                                 "matrix_bytes_per_entry": 28,
                                 "algorithmic_bytes": "column + c128 value per entry, row pointers, x and y once "
                                                      "(x gathers served from L2)"}}
+        elif bsz:
+            kernel = f"block map c128 x{bsz} (k_block_matvec_v<double, {bsz}>, block Lanczos)"
+            extra = {"block_lanczos": {"block": bsz, "maps_per_launch": bsz}}
         else:
             kernel = "map c128 (k_matvec<double>)"
             extra = {}

@@ -138,6 +138,15 @@ MOMED_API int  momed_matvec(momed_handle* h, const void* x, void* y, int32_t pre
 MOMED_API int  momed_eigsolve(momed_handle* h, const momed_solve_opts* opts, const double* vec0,
                     double* vals, double* resid, void* vecs, momed_info* info);
 
+/* Eigenpairs of a NON-Hermitian operator (a term list set as it is, without Hermitian
+ * completion): krylov_map_solve(H, N; ishermitian = false) (MomentumEDCUDAExt.jl:159-179) ->
+ * KrylovKit eigsolve(:SR; ishermitian = false).  Arnoldi with Krylov-Schur restarts in FP64 on
+ * the matrix-free map.  vals [2 nev]: complex eigenvalues (re, im) ordered by real part
+ * (ascending); resid [nev] = ||H x - e x||; vecs [nev][N] c128 right eigenvectors (unit norm).
+ * opts->precision is ignored (FP64).  Returns MOMED_ENOTCONV when fewer than nev pairs met tol. */
+MOMED_API int  momed_eigsolve_general(momed_handle* h, const momed_solve_opts* opts, const double* vec0,
+                                      double* vals, double* resid, void* vecs, momed_info* info);
+
 /* Batched solve of H(u) = A + u B (momed_set_scatter_pair) for nu values of u at once on the
  * working basis: block matvec over all u, one Lanczos per u.  vals [nu][nev], resid [nu][nev];
  * vecs [nu][nev][N] c128 host (may be NULL).  Mixed precision is opts->precision.  With a

@@ -506,6 +506,15 @@ int momed_eigsolve(momed_handle* h, const momed_solve_opts* opts, const double* 
     });
 }
 
+int momed_eigsolve_general(momed_handle* h, const momed_solve_opts* opts, const double* vec0, double* vals,
+                           double* resid, void* vecs, momed_info* info) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(opts && vals, MOMED_EINVAL, "opts and vals are required");
+        return momed_eigsolve_general_impl(h, opts, vec0, vals, resid, vecs, info);
+    });
+}
+
 int momed_batch_solve(momed_handle* h, const momed_solve_opts* opts, const double* u, int32_t nu, double* vals,
                       double* resid, double* vecs, momed_info* info) {
     if (!h) return MOMED_EINVAL;

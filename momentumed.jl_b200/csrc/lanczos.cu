@@ -382,6 +382,13 @@ void rayleigh_ritz_fp64(momed_handle* h, double2* X, double2* W, double2* scratc
 
 }  // namespace momed
 
+namespace momed {
+int block_size_for(momed_handle* h, int nev, int precision);                    // block_lanczos.cu
+bool eigsolve_block(momed_handle* h, const momed_solve_opts* o, int nev, int B, const double2* start64, double2* X,
+                    std::vector<double>& theta, std::vector<double>& res, int& nconv, int& restarts, int64_t& matvecs,
+                    int64_t& matvecs64);
+}  // namespace momed
+
 using namespace momed;
 
 int momed_eigsolve_impl(momed_handle* h, const momed_solve_opts* o, const double* vec0, double* vals, double* resid,
@@ -406,7 +413,13 @@ int momed_eigsolve_impl(momed_handle* h, const momed_solve_opts* o, const double
     std::vector<double> theta, res;
     int nconv = 0, restarts = 0;
     int64_t matvecs = 0, matvecs64 = 0;
-    if (o->precision == MOMED_PREC_MIXED) {
+    // several wanted pairs on a large sector: the block solver (B vectors per map launch); a
+    // block that loses rank sends the solve back to the single-vector solver below
+    const int B = block_size_for(h, nev, o->precision);
+    const bool blocked = B > 0 && eigsolve_block(h, o, nev, B, vec0 ? start64.p : nullptr, X.p, theta, res, nconv,
+                                                 restarts, matvecs, matvecs64);
+    if (blocked) {
+    } else if (o->precision == MOMED_PREC_MIXED) {
         // phase 1: FP32 Lanczos to the FP32 floor
         const int extra = std::min<int>(4, std::max<int>(0, m - 2 - nev));
         const int k1 = nev + extra;

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <complex>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -288,6 +289,12 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
 void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each, int ncc, const int64_t* mask,
                      int mlen, const int64_t* momentum_list, int nmom);
 
+// tc_proj.cu: C = Q^H W of a c64 block basis on the tensor cores (B = 8 or 16 right-hand
+// sides, ncol basis columns in blocks [N][B]); writes partial[split][c][r] for the *nsplit
+// splits it chose (at most max_splits), to be summed over splits; *err = 1 if a wait timed out
+void launch_proj_tc_c64(const float2* Q, int ncol, int64_t N, const float2* W, int B, double2* partial,
+                        int max_splits, int* nsplit, int* err, cudaStream_t st);
+
 // y = H x in FP64 on the working basis/operator (parameter u from the handle)
 void apply_h_fp64(momed_handle* h, const double2* x, double2* y);
 
@@ -302,11 +309,17 @@ int64_t launches_total();
 // small dense symmetric eigensolver (host, FP64): A n x n row-major (destroyed),
 // eigenvalues ascending in w, eigenvectors as columns of V (row-major n x n)
 void symeig(int n, double* A, double* w, double* V);
+// small dense Hermitian eigensolver (host, FP64): A n x n row-major complex (destroyed),
+// eigenvalues ascending in w, eigenvectors as columns of Z (row-major n x n complex)
+void herm_eig(int n, std::complex<double>* A, double* w, std::complex<double>* Z);
 
 }  // namespace momed
 
 // Lanczos drivers (lanczos.cu)
 int momed_eigsolve_impl(momed_handle* h, const momed_solve_opts* o, const double* vec0, double* vals, double* resid,
                         void* vecs, momed_info* info);
+// arnoldi.cu: the non-Hermitian solver (vals [nev] complex, ordered by real part)
+int momed_eigsolve_general_impl(momed_handle* h, const momed_solve_opts* o, const double* vec0, double* vals,
+                                double* resid, void* vecs, momed_info* info);
 int momed_batch_solve_impl(momed_handle* h, const momed_solve_opts* o, const double* u, int32_t nu, double* vals,
                            double* resid, double* vecs, momed_info* info);

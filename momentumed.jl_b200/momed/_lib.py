@@ -69,6 +69,8 @@ SIGNATURES = {
     "momed_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
     "momed_eigsolve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.POINTER(Info)]),
+    "momed_eigsolve_general": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.POINTER(Info)]),
     "momed_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_int32, C.c_void_p,
                                     C.c_void_p, C.c_void_p, C.POINTER(Info)]),
     "momed_build_sparse": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
@@ -416,6 +418,27 @@ class Handle:
         return vals, vecs, resid, {"converged": info.converged, "restarts": info.restarts,
                                    "matvecs": info.matvecs, "matvecs_fp64": info.matvecs_fp64,
                                    "seconds": info.seconds}
+
+    def eigsolve_general(self, nev: int, krylovdim: int = 30, tol: float = 1e-12, maxiter: int = 100,
+                         vec0: np.ndarray | None = None, seed: int = 0, want_vectors: bool = True,
+                         raise_on_notconv: bool = False):
+        """Non-Hermitian operator (its term list set as it is): complex eigenvalues ordered by
+        real part, right eigenvectors, residuals (momed_eigsolve_general)."""
+        n = self.n
+        nev_eff = min(nev, n)
+        opts = SolveOpts(nev, krylovdim, maxiter, PREC_FP64, tol, seed, int(want_vectors), 0)
+        vals = np.zeros(2 * nev_eff)
+        resid = np.zeros(nev_eff)
+        vecs = np.zeros((nev_eff, n), np.complex128) if want_vectors else None
+        v0 = None if vec0 is None else np.ascontiguousarray(vec0, np.complex128)
+        info = Info()
+        rc = lib().momed_eigsolve_general(self._h, C.byref(opts), _p(v0), _p(vals), _p(resid), _p(vecs),
+                                          C.byref(info))
+        if rc not in (OK, ENOTCONV) or (rc == ENOTCONV and raise_on_notconv):
+            self._check(rc)
+        return (vals[0::2] + 1j * vals[1::2], vecs, resid,
+                {"converged": info.converged, "restarts": info.restarts, "matvecs": info.matvecs,
+                 "matvecs_fp64": info.matvecs_fp64, "seconds": info.seconds})
 
     def batch_solve(self, u: np.ndarray, nev: int, krylovdim: int = 30, tol: float = 1e-12, maxiter: int = 100,
                     seed: int = 0, precision: int = PREC_MIXED, want_vectors: bool = False,

@@ -14,6 +14,8 @@ are the complex conjugates of these.  Eigenvalues are identical.
 """
 from __future__ import annotations
 
+import warnings
+
 import numpy as np
 
 from . import _lib
@@ -133,10 +135,19 @@ def create_gpu_linearmap(A: LinearMap, device: str = "b200") -> B200LinearMap:
 def krylov_map_solve(H: B200LinearMap, N_eigen: int, *, ishermitian: bool = True, vec0=None,
                      krylovdim: int = 30, tol: float = 1e-12, maxiter: int = 100, seed: int = 0,
                      precision: str = "fp64", verbosity: int = 0):
-    """Lowest N_eigen eigenpairs (:SR) of the device map; returns (vals, vecs, info)."""
-    if not ishermitian:
-        raise NotImplementedError("the non-Hermitian map is not part of this backend")
+    """Lowest N_eigen eigenpairs (:SR) of the device map; returns (vals, vecs, info).
+
+    ishermitian=False (a map of a non-Hermitian operator): Arnoldi with Krylov-Schur restarts,
+    complex eigenvalues ordered by real part (KrylovKit eigsolve(:SR; ishermitian = false))."""
     m = H.size[0]
+    if not ishermitian:
+        if getattr(H, "hermitian", False):
+            warnings.warn("ishermitian=false on a Hermitian map: solved as a general matrix")
+        vals, vecs, resid, info = H.handle.eigsolve_general(min(N_eigen, m), krylovdim=krylovdim, tol=tol,
+                                                            maxiter=maxiter, vec0=vec0, seed=seed)
+        info = dict(info)
+        info["residuals"] = resid
+        return vals, [vecs[i] for i in range(len(vals))], info
     N_eigen = min(N_eigen, m)
     prec = _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64
     vals, vecs, resid, info = H.handle.eigsolve(N_eigen, krylovdim=krylovdim, tol=tol, maxiter=maxiter,

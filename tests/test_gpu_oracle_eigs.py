@@ -1,0 +1,133 @@
+"""Eigenpairs at the benchmark configurations against the FP64 oracle (committed fixtures).
+
+tests/golden/eig_oracle.json holds, per case, the oracle's FP64 Lanczos eigenvalues (nev + 2),
+its residuals and an 8-probe sketch of each eigenvector (tests/golden/make_eig_fixtures.py
+made it with the oracle alone).  The cases: the 3x9 U0 sweep of the headline (one sector at
+three U0 values, a second sector at one), a ~1.0M-state 3x10 sector with nev 6 and krylovdim
+64, and a two-component 4x5 (3+3) sector with nev 8 standing in for the 4x6 one.
+
+Each case is solved on the device by the plain FP64 single-vector Lanczos, the mixed-precision
+single-vector solver and the batched mixed-precision solver (for the 3x9 sector, over the full
+32-value U0 grid of the sweep).  Bars, per eigenvalue: relative error <= 1e-10 against the
+oracle; the device's FP64 residual ||H psi - E psi|| <= 1e-8; for each eigenvalue separated
+from its neighbours, the overlap |<psi_oracle|psi>| >= 1 - 1e-9 by the Davis-Kahan bound
+(sin angle <= (r_device + r_oracle) / gap) and, from the sketches, the measured deviation
+||R^H psi - e^{i phi} R^H psi_oracle|| / ||R^H psi_oracle|| <= 5e-5 (sin angle of the two
+vectors, estimated on 8 random unit probes).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import momed
+from momed import _lib
+from momed.core import pair_operator
+from momed.synthetic import mesh_para, u_grid
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = json.load(open(os.path.join(HERE, "golden", "eig_oracle.json")))
+
+
+def probes(N, seed):
+    rs = np.random.RandomState(seed)
+    re = rs.standard_normal((8, N))
+    im = rs.standard_normal((8, N))
+    r = re + 1j * im
+    return r / np.linalg.norm(r, axis=1, keepdims=True)
+
+
+_cache = {}
+
+
+def setup(h, c):
+    """Operator pair and the case's sector on the handle (enumerated on the device)."""
+    key = (tuple(c["mesh"]), c["seed"], c["Nc_conserve"], tuple(c["N_each"]))
+    if key not in _cache:
+        a, b = c["mesh"]
+        para, _ = mesh_para(a, b, c["seed"], Nc_conserve=c["Nc_conserve"])
+        A = momed.MBOperator(momed.ED_scatterlist_onebody(para), upper_hermitian=True)
+        B = momed.MBOperator(momed.ED_scatterlist_twobody(para), upper_hermitian=True)
+        sectors = h.enumerate_basis(para.k_list, para.Gk, 1, c["Nc_conserve"], c["N_each"])
+        _cache.clear()
+        _cache[key] = (pair_operator(A, B), sectors)
+    pair, sectors = _cache[key]
+    k, basis = sectors[c["sector"]]
+    assert list(k) == c["k"] and len(basis) == c["N"]
+    h.set_scatter_pair(*pair)
+    h.set_basis(basis)
+    h.set_param(c["u"])
+    return basis
+
+
+def check(c, vals, vecs, resid, R):
+    nev = c["nev"]
+    ref = np.asarray(c["vals"])
+    err = np.abs(vals[:nev] - ref[:nev]) / np.abs(ref[:nev])
+    assert np.max(err) <= 1e-10, (c["case"], err)
+    assert np.max(resid[:nev]) <= 1e-8, (c["case"], resid)
+    for i in range(nev):
+        others = np.delete(ref, i)
+        gap = float(np.min(np.abs(others - ref[i])))
+        if gap < 1e-6 * max(1.0, abs(ref[i])):
+            continue                                     # a degenerate pair: no single-vector overlap
+        sin_dk = (resid[i] + c["resid"][i]) / gap
+        assert np.sqrt(max(0.0, 1.0 - sin_dk ** 2)) >= 1 - 1e-9, (c["case"], i, sin_dk)
+        if vecs is not None:
+            s_ref = np.asarray(c["sketch_re"][i]) + 1j * np.asarray(c["sketch_im"][i])
+            s = R.conj() @ vecs[i]
+            ph = np.vdot(s_ref, s)
+            ph /= abs(ph)
+            dev = np.linalg.norm(s - ph * s_ref) / np.linalg.norm(s_ref)
+            assert dev <= 5e-5, (c["case"], i, dev)
+
+
+CASES = sorted(FIX)
+
+
+@pytest.fixture(scope="module")
+def h():
+    hd = momed.Handle(0)
+    yield hd
+    hd.close()
+
+
+@pytest.mark.parametrize("case", CASES)
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_single_vector_solver_vs_oracle(h, case, precision):
+    c = FIX[case]
+    basis = setup(h, c)
+    prec = _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64
+    vals, vecs, resid, info = h.eigsolve(c["nev"], krylovdim=c["krylovdim"], tol=1e-12, maxiter=300, seed=1,
+                                         precision=prec)
+    check(c, vals, vecs, resid, probes(len(basis), c["sketch_seed"]))
+
+
+def test_batched_sweep_3x9_vs_oracle(h):
+    """The headline's batched mixed solver over the whole 32-value U0 grid of one 3x9 sector,
+    checked at the three grid points the oracle solved."""
+    cs = [FIX[k] for k in CASES if k.startswith("c3_3x9_s3_")]
+    assert len(cs) == 3
+    basis = setup(h, cs[0])
+    u = u_grid(32, 0.5, 2.0)
+    vals, vecs, resid, info = h.batch_solve(u, 4, krylovdim=30, tol=1e-12, precision=_lib.PREC_MIXED,
+                                            want_vectors=True)
+    R = probes(len(basis), cs[0]["sketch_seed"])
+    for c in cs:
+        j = int(np.argmin(np.abs(u - c["u"])))
+        assert abs(u[j] - c["u"]) < 1e-15
+        check(c, vals[j], vecs[j], resid[j], R)
+
+
+@pytest.mark.parametrize("case", [k for k in CASES if not k.startswith("c3_3x9_s3_")])
+def test_batched_solver_vs_oracle(h, case):
+    c = FIX[case]
+    basis = setup(h, c)
+    vals, vecs, resid, info = h.batch_solve(np.array([c["u"], c["u"]]), c["nev"], krylovdim=max(30, c["krylovdim"]),
+                                            tol=1e-12, precision=_lib.PREC_MIXED, want_vectors=True)
+    R = probes(len(basis), c["sketch_seed"])
+    for j in range(2):
+        check(c, vals[j], vecs[j], resid[j], R)
