@@ -123,6 +123,30 @@ MOMED_API int  momed_set_scatter(momed_handle* h, const double* amp, const uint6
 MOMED_API int  momed_set_scatter_pair(momed_handle* h, const double* amp_a, const double* amp_b, const uint64_t* in,
                             const uint64_t* out, const uint64_t* parity, int64_t nscat);
 
+/* Twisted-boundary sweeps: the two-body amplitudes regenerated on the device for each kshift.
+ * With momentum coordinates, ED_scatterlist_twobody (scat_list.jl:442-497) evaluates H_two at
+ * k/Gk + kshift/Gk of each conserved component (scat_list.jl:5-50), so the reference rebuilds
+ * the list on the host for every point of a sweep.  momed_set_twobody_recipe attaches to the
+ * working operator (set by momed_set_scatter, a single operator) the structure of its two-body
+ * terms: raw[nraw][9] = (kf1, kf2, ki2, ki1) 0-based momentum indices, (cf1, cf2, ci2, ci1)
+ * 1-based components, flags (bit 0: negate; bits 1-2: 0 as is, 1 conjugate, 2 real part: the
+ * normal ordering of the Scatter constructor), grouped per upper term by upper_start[nupper + 1]
+ * in the order the terms are summed; for each entry e of the list passed to momed_set_scatter,
+ * entry_upper[e] (its upper term, -1 for a term the recipe leaves as uploaded) and
+ * entry_partner[e] (1 for the Hermitian partner, whose amplitude is the conjugate).
+ * momed_set_kshift(h, kshift[Nc_conserve][dim]) evaluates the recipe's interaction on the device
+ * for every contribution, (direct - exchange) / Nk as scat_list.jl does, and overwrites the term
+ * amplitudes (a built sparse matrix is dropped).  Recipe MOMED_RECIPE_LANDAU_COULOMB: the
+ * screened Coulomb interaction in the lowest Landau level with magnetic-translation phases
+ * (the H_two of MomentumED/test/example1_FQH_Laughlin.jl:20-89), params [Gl, D, W0, angle,
+ * nshell], 2D meshes.  FP64 on the device: amplitudes agree with the host builder to ~1e-15. */
+#define MOMED_RECIPE_LANDAU_COULOMB 1
+MOMED_API int  momed_set_twobody_recipe(momed_handle* h, const momed_para* p, int32_t recipe, const double* params,
+                                        int32_t nparams, const int32_t* raw, int64_t nraw, const int64_t* upper_start,
+                                        int64_t nupper, const int64_t* entry_upper, const int32_t* entry_partner,
+                                        int64_t nentries);
+MOMED_API int  momed_set_kshift(momed_handle* h, const double* kshift);
+
 /* Parameter u of the operator H(u) = A + u B set by momed_set_scatter_pair (default 1). */
 MOMED_API int  momed_set_param(momed_handle* h, double u);
 

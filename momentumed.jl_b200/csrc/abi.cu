@@ -164,6 +164,8 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
         up(op.ampb32, B32);
     }
     MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+    h->op_order = std::move(ord);
+    h->recipe.set = false;                 // a recipe describes the operator it was attached to
     h->op_mask_or = mask_or;
     h->op_set = true;
     h->op_validated = false;
@@ -434,6 +436,26 @@ int momed_set_scatter(momed_handle* h, const double* amp, const uint64_t* in, co
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {
         upload_operator(h, amp, nullptr, in, out, parity, nscat);
+        return MOMED_OK;
+    });
+}
+
+int momed_set_twobody_recipe(momed_handle* h, const momed_para* p, int32_t recipe, const double* params,
+                             int32_t nparams, const int32_t* raw, int64_t nraw, const int64_t* upper_start,
+                             int64_t nupper, const int64_t* entry_upper, const int32_t* entry_partner,
+                             int64_t nentries) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        set_twobody_recipe(h, p, recipe, params, nparams, raw, nraw, upper_start, nupper, entry_upper, entry_partner,
+                           nentries);
+        return MOMED_OK;
+    });
+}
+
+int momed_set_kshift(momed_handle* h, const double* kshift) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        set_kshift(h, kshift);
         return MOMED_OK;
     });
 }

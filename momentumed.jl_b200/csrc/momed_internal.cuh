@@ -161,6 +161,25 @@ struct Operator {
     OpView view() const;
 };
 
+// Device recipe of the two-body terms for twisted-boundary sweeps (recipe.cu): the raw
+// contributions of every upper term of the working operator, so that its amplitudes can be
+// regenerated on the device for any kshift (momed_set_kshift) without rebuilding the list.
+struct TwoBodyRecipe {
+    bool set = false;
+    int32_t kind = 0, dim = 0, Nk = 0, Nc_mix = 1, Ncc = 1;
+    double sys_size = 1.0;
+    double params[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    double Gk[3] = {0, 0, 0};
+    int64_t nraw = 0, nupper = 0;
+    DevBuf<double> kcoord;         // [Nk][dim] momentum coordinates k (before / Gk)
+    DevBuf<int32_t> raw;           // [nraw][9]: kf1 kf2 ki2 ki1 (0-based), cf1 cf2 ci2 ci1 (1-based), flags
+    DevBuf<int64_t> upper_start;   // [nupper + 1] contributions of each upper term, in merge order
+    DevBuf<int32_t> slot_upper;    // per device term slot: its upper term (-1: keep the amplitude)
+    DevBuf<int32_t> slot_partner;  // per device term slot: 1 for the Hermitian partner (conjugate)
+    DevBuf<double2> upper_amp;     // [nupper] scratch of the regeneration
+    DevBuf<double> shift;          // [Ncc][dim]
+};
+
 // CSR matrix of the working operator on the working basis (the sparse method, sparse.cu):
 // row_ptr[n + 1]; per entry a column, the FP64 value at u and its FP32 rounding.
 struct SparseMatrix {
@@ -209,6 +228,8 @@ struct momed_handle {
     bool index_dirty = true;
     uint64_t index_bits = 0;               // bits the index tables cover
     momed::Operator op;
+    std::vector<int64_t> op_order;         // device term slot q holds entry op_order[q] of the uploaded list
+    momed::TwoBodyRecipe recipe;           // amplitudes regenerated on the device (momed_set_kshift)
     momed::SparseMatrix sparse;           // built by momed_build_sparse; maps use it while built
     bool sparse_only = false;              // an uploaded matrix (momed_set_sparse_csr) without a basis
     bool op_set = false;
@@ -294,6 +315,12 @@ void enumerate_basis(momed_handle* h, const momed_para* p, const int64_t* N_each
 // splits it chose (at most max_splits), to be summed over splits; *err = 1 if a wait timed out
 void launch_proj_tc_c64(const float2* Q, int ncol, int64_t N, const float2* W, int B, double2* partial,
                         int max_splits, int* nsplit, int* err, cudaStream_t st);
+
+// recipe.cu: device regeneration of the two-body amplitudes for a kshift
+void set_twobody_recipe(momed_handle* h, const momed_para* p, int32_t kind, const double* params, int32_t nparams,
+                        const int32_t* raw, int64_t nraw, const int64_t* upper_start, int64_t nupper,
+                        const int64_t* entry_upper, const int32_t* entry_partner, int64_t nentries);
+void set_kshift(momed_handle* h, const double* kshift);
 
 // y = H x in FP64 on the working basis/operator (parameter u from the handle)
 void apply_h_fp64(momed_handle* h, const double2* x, double2* y);

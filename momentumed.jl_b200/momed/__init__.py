@@ -13,6 +13,7 @@ from .core import (MBS64, HilbertSubspace, MBOperator, MBS64Vector, Scatter, Sca
 from .methods import (DEFAULT_GPU, GPU_AVAILABLE, EDsolve, LinearMap, activate_b200, activate_gpu_device,
                       create_gpu_linearmap, create_gpu_matrix, krylov_map_solve, krylov_matrix_solve,
                       release_gpu_memory)
+from .recipes import KShiftOperator, LandauCoulomb, kshift_sweep
 from .preparation import (ED_momentum_subspaces, ED_scatterlist_onebody, ED_scatterlist_twobody,
                           ED_sortedScatterList_onebody, ED_sortedScatterList_twobody, EDPara, MBS_totalmomentum,
                           group_momentum_pairs, momentum_residue)
@@ -26,4 +27,5 @@ __all__ = [
     "create_gpu_linearmap", "create_gpu_matrix", "krylov_map_solve", "krylov_matrix_solve", "release_gpu_memory",
     "ED_momentum_subspaces", "ED_scatterlist_onebody", "ED_scatterlist_twobody", "ED_sortedScatterList_onebody",
     "ED_sortedScatterList_twobody", "EDPara", "MBS_totalmomentum", "group_momentum_pairs", "momentum_residue",
+    "KShiftOperator", "LandauCoulomb", "kshift_sweep",
 ]

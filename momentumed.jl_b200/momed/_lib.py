@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(PKG_ROOT, "lib", "libmomed_b200.so")
 
 OK, EINVAL, ENOMEM, ECUDA, ENOTCONV, ETIMEOUT, ESTATE, ENODEV = range(8)
 C128, C64 = 0, 1
+RECIPE_LANDAU_COULOMB = 1
 PREC_FP64, PREC_MIXED = 0, 1
 
 
@@ -69,6 +70,9 @@ SIGNATURES = {
     "momed_matvec": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32]),
     "momed_eigsolve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.POINTER(Info)]),
+    "momed_set_twobody_recipe": (C.c_int, [C.c_void_p, C.POINTER(Para), C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                           C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64]),
+    "momed_set_kshift": (C.c_int, [C.c_void_p, C.c_void_p]),
     "momed_eigsolve_general": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.POINTER(Info)]),
     "momed_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_int32, C.c_void_p,
@@ -265,6 +269,27 @@ class Handle:
             out.append((tuple(int(v) for v in ks[s * dim:(s + 1) * dim]), basis[off:off + sizes[s]]))
             off += int(sizes[s])
         return out
+
+    def set_twobody_recipe(self, para, kind: int, params, raw, upper_start, entry_upper, entry_partner):
+        """Attach the device recipe of the working operator's two-body terms (momed_set_twobody_recipe)."""
+        k_list = np.asarray(para.k_list, np.int64)
+        dim, Nk = k_list.shape
+        kl = np.ascontiguousarray(k_list.T).reshape(-1)
+        g = np.asarray(para.Gk, np.int64)
+        p = Para(dim, Nk, para.Nc_mix, para.Nc_conserve, kl.ctypes.data_as(C.POINTER(C.c_int64)),
+                 g.ctypes.data_as(C.POINTER(C.c_int64)))
+        prm = np.ascontiguousarray(params, np.float64)
+        raw = np.ascontiguousarray(raw, np.int32).reshape(-1, 9)
+        us = np.ascontiguousarray(upper_start, np.int64)
+        eu = np.ascontiguousarray(entry_upper, np.int64)
+        ep = np.ascontiguousarray(entry_partner, np.int32)
+        self._check(lib().momed_set_twobody_recipe(self._h, C.byref(p), kind, _p(prm), len(prm), _p(raw), len(raw),
+                                                   _p(us), len(us) - 1, _p(eu), _p(ep), len(eu)))
+
+    def set_kshift(self, kshift):
+        """Regenerate the recipe's amplitudes on the device at kshift [Nc_conserve][dim]."""
+        k = np.ascontiguousarray(kshift, np.float64)
+        self._check(lib().momed_set_kshift(self._h, _p(k)))
 
     def select_sector(self, s: int, n: int):
         self._check(lib().momed_select_sector(self._h, s))

@@ -17,7 +17,7 @@ from fractions import Fraction
 
 import numpy as np
 
-from .core import HilbertSubspace, MBS64, Scatter, ScatterList, sort_merge_scatlist
+from .core import HilbertSubspace, MBS64, Scatter, ScatterList, parity_mask, sort_merge_scatlist
 
 
 class EDPara:
@@ -273,3 +273,67 @@ def ED_scatterlist_twobody(para: EDPara, *, element_type=np.float64, kshift=None
 # the names the README and older releases use (scat_list.jl:573-574)
 ED_sortedScatterList_onebody = ED_scatterlist_onebody
 ED_sortedScatterList_twobody = ED_scatterlist_twobody
+
+
+# ------------------------------------------------------------------------------- device recipes
+def twobody_recipe_table(para: EDPara) -> dict:
+    """Structure of the coordinate-mode two-body list without evaluating H_two: the loop, filters
+    and normal ordering of ED_scatterlist_twobody (scat_list.jl:442-497), recording for every raw
+    term its momenta and components and what the Scatter constructor does to its amplitude (sign;
+    as is, conjugated on the upper swap, or reduced to the real part on the diagonal), grouped by
+    upper term (out, in) in the order sort_merge_scatlist sums them.
+
+    Returns dict(out, in_, pm: the upper terms (sorted by in, out); raw: int32 [nraw][9] = kf1, kf2,
+    ki2, ki1 (0-based), cf1, cf2, ci2, ci1, flags (bit 0 negate, bits 1-2: 0 as is, 1 conjugate,
+    2 real part); upper_start: int64 [nupper + 1]).  Every structurally allowed term is kept, also
+    those whose amplitude vanishes at some kshift."""
+    Nk, Nc, Ncm, bits = para.Nk, para.Nc, para.Nc_mix, para.bits
+    probe = complex(1.0, 2.0)
+    recs, keys = [], []
+    for _, pairs in group_momentum_pairs(para).items():
+        for (ki1, ki2) in pairs:
+            for (kf1, kf2) in pairs:
+                for ci1 in range(1, Nc + 1):
+                    for ci2 in range(1, Nc + 1):
+                        for cf1 in range(1, Nc + 1):
+                            for cf2 in range(1, Nc + 1):
+                                f1, f2 = kf1 + Nk * (cf1 - 1), kf2 + Nk * (cf2 - 1)
+                                i1, i2 = ki1 + Nk * (ci1 - 1), ki2 + Nk * (ci2 - 1)
+                                if i1 == i2 or f1 == f2:
+                                    continue
+                                if ki1 == ki2 and i1 < i2:
+                                    continue
+                                if kf1 == kf2 and f1 < f2:
+                                    continue
+                                if not ((min(i1, i2), max(i1, i2)) >= (min(f1, f2), max(f1, f2))):
+                                    continue
+                                s = Scatter(probe, f1, f2, i2, i1, bits=bits, upper_hermitian=True)
+                                a = complex(s.Amp)
+                                if a == probe:
+                                    fl = 0
+                                elif a == -probe:
+                                    fl = 1
+                                elif a == probe.conjugate():
+                                    fl = 2
+                                elif a == -probe.conjugate():
+                                    fl = 3
+                                elif a == 1:
+                                    fl = 4
+                                elif a == -1:
+                                    fl = 5
+                                else:
+                                    raise AssertionError(f"unexpected normal ordering {a}")
+                                recs.append((kf1 - 1, kf2 - 1, ki2 - 1, ki1 - 1, cf1, cf2, ci2, ci1, fl))
+                                keys.append((s.in_, s.out))
+    if not recs:
+        z = np.zeros(0, np.uint64)
+        return dict(out=z, in_=z.copy(), pm=z.copy(), raw=np.zeros((0, 9), np.int32),
+                    upper_start=np.zeros(1, np.int64))
+    order = sorted(range(len(recs)), key=lambda r: keys[r])        # stable: merge order within a key
+    raw = np.array([recs[r] for r in order], np.int32)
+    sk = [keys[r] for r in order]
+    starts = [0] + [i for i in range(1, len(sk)) if sk[i] != sk[i - 1]] + [len(sk)]
+    uin = np.array([sk[i][0] for i in starts[:-1]], np.uint64)
+    uout = np.array([sk[i][1] for i in starts[:-1]], np.uint64)
+    pm = np.array([parity_mask(int(o)) ^ parity_mask(int(i)) for o, i in zip(uout, uin)], np.uint64)
+    return dict(out=uout, in_=uin, pm=pm, raw=raw, upper_start=np.array(starts, np.int64))

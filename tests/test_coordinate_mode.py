@@ -109,3 +109,62 @@ def test_laughlin_three_fold_ground_state():
     assert sorted(k for _, k in low) == [(0, 2), (1, 2), (2, 2)]
     assert low[2][0] - low[0][0] < 1e-7
     assert levels[3][0] - low[2][0] > 0.04
+
+
+# ---------------------------------------------------------------------------- device recipe tables
+def replay_table(para, t, H, kshift):
+    """The upper amplitudes a recipe table describes, evaluated on the host in its order."""
+    from momed.preparation import _coords, _shift_decipher
+    sh = _shift_decipher(kshift, para.Nc_conserve, para.dim)
+    kl, shv = _coords(para, sh, False)
+    sys_size = para.Nk if all(g != 0 for g in para.Gk) else 1
+    out = []
+    for u in range(len(t["out"])):
+        acc = 0j
+        for r in t["raw"][t["upper_start"][u]:t["upper_start"][u + 1]]:
+            ks, cs, fl = r[:4], r[4:8], int(r[8])
+            cc = [(int(c) - 1) // para.Nc_mix for c in cs]
+            kc = [tuple(kl[d][int(k)] + shv[d][c] for d in range(para.dim)) for k, c in zip(ks, cc)]
+            d_ = complex(H(kc[0], kc[1], kc[2], kc[3], *[int(c) for c in cs]))
+            e_ = complex(H(kc[0], kc[1], kc[3], kc[2], int(cs[0]), int(cs[1]), int(cs[3]), int(cs[2])))
+            v = complex((d_.real - e_.real) / sys_size, (d_.imag - e_.imag) / sys_size)
+            if fl & 1:
+                v = -v
+            mode = (fl >> 1) & 3
+            if mode == 1:
+                v = v.conjugate()
+            elif mode == 2:
+                v = complex(v.real, 0.0)
+            acc = acc + v
+        out.append(acc)
+    return np.array(out)
+
+
+@pytest.mark.parametrize("kshift", [(0.0, 0.0), (0.25, 0.5), (0.1, 0.7)])
+def test_recipe_table_replays_the_builder(kshift):
+    """The structure table that the device recipe evaluates, replayed on the host with the same
+    H_two and float kshift, gives the builder's merged upper list bit for bit (terms the builder
+    dropped as exactly zero replay to zero)."""
+    rec = momed.LandauCoulomb()
+    para = momed.EDPara(k_list=L.K_LIST, Gk=L.GK, H_two=rec.H_two, two_momentum_coordinate=True)
+    from momed.preparation import twobody_recipe_table
+    t = twobody_recipe_table(para)
+    got = replay_table(para, t, rec.H_two, kshift)
+    ref = momed.ED_scatterlist_twobody(para, kshift=kshift)
+    keys = {(int(i), int(o)): a for i, o, a in zip(ref.in_, ref.out, ref.amp)}
+    assert len(t["out"]) >= len(ref)
+    for i, o, a in zip(t["in_"], t["out"], got):
+        want = keys.get((int(i), int(o)), 0j)
+        assert a == want or (want == 0 and a == 0), (i, o, a, want)
+
+
+def test_recipe_interaction_is_the_reference_test_formula():
+    """LandauCoulomb.H_two (the host form of the device recipe) against the port of the reference
+    test's V_int, on random float coordinates (1e-14 relative; cispi there, cos/sin of pi x here)."""
+    rec = momed.LandauCoulomb()
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        ks = [tuple(rng.uniform(-1.5, 1.5, 2)) for _ in range(4)]
+        a = rec.H_two(*ks)
+        b = L.V_int(*ks)
+        assert abs(a - b) <= 1e-14 * max(1.0, abs(b))
