@@ -261,6 +261,15 @@ MOMED_API int  momed_serve_stats(momed_server* s, int64_t* queued, int64_t* comp
 MOMED_API const char* momed_serve_last_error(momed_server* s);
 MOMED_API int  momed_serve_stop(momed_server* s);
 
+/* The block map's autotuned launch for the working operator and basis (its sector size class)
+ * at block width nb (1..32), precision MOMED_PREC_FP64 (c128) or MOMED_PREC_MIXED (c64), with
+ * (has_param = 1) or without the H(u) = A + u B form: rows per warp (1, 2, 4), grid (0: one
+ * CTA per SM fewer than resident, 1: resident, 2: twice resident), the chosen and the default
+ * launch's device time (ms).  The tuner runs at a key's first launch (MOMED_AUTOTUNE=0 turns it
+ * off); MOMED_ESTATE until then.  No reference counterpart (a measurement aid). */
+MOMED_API int  momed_block_tuning(momed_handle* h, int32_t nb, int32_t precision, int32_t has_param,
+                                  int32_t* rows_per_warp, int32_t* grid_mult, double* ms, double* ms_default);
+
 /* Kernels this library has launched in the process so far (all handles). */
 MOMED_API int64_t momed_kernel_launches(void);
 

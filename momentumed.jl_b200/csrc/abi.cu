@@ -440,6 +440,25 @@ int momed_set_scatter(momed_handle* h, const double* amp, const uint64_t* in, co
     });
 }
 
+int momed_block_tuning(momed_handle* h, int32_t nb, int32_t precision, int32_t has_param, int32_t* rows_per_warp,
+                       int32_t* grid_mult, double* ms, double* ms_default) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(h->op_set && h->n > 0, MOMED_ESTATE, "no working basis and operator");
+        MOMED_REQUIRE(rows_per_warp && grid_mult, MOMED_EINVAL, "null output");
+        int g = 0, r = 0;
+        float a = 0.f, b = 0.f;
+        const bool hb = has_param && h->op.has_b;
+        if (!block_tuning_lookup(h->op.view(), h->n, nb, precision == MOMED_PREC_FP64, hb, &g, &r, &a, &b))
+            return (int)MOMED_ESTATE;
+        *rows_per_warp = r;
+        *grid_mult = g;
+        if (ms) *ms = a;
+        if (ms_default) *ms_default = b;
+        return (int)MOMED_OK;
+    });
+}
+
 int momed_set_twobody_recipe(momed_handle* h, const momed_para* p, int32_t recipe, const double* params,
                              int32_t nparams, const int32_t* raw, int64_t nraw, const int64_t* upper_start,
                              int64_t nupper, const int64_t* entry_upper, const int32_t* entry_partner,

@@ -14,6 +14,7 @@
 // sides whose estimated eigenvalue error stays above the target are finished by an
 // FP64 single-vector Lanczos warm-started from their refined vectors.
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -425,8 +426,72 @@ struct BlockLanczos {
     DevBuf<RT> ud;
     int64_t launches = 0;
     double dgks = 0.5;   // second Gram-Schmidt pass when |w'|^2 < dgks |w|^2 (set by run)
+    // The steps of a restart cycle (k .. m-1) as one CUDA graph: captured the first time a cycle
+    // starts at k on a given basis buffer (the restart alternates two), replayed afterwards.  A
+    // step needs no host decision (the second Gram-Schmidt pass is predicated on a device flag),
+    // so the cycle's ~12 launches per step go to the device as one graph launch.  The first
+    // cycle runs eagerly (the block map's autotuner times its candidates there, outside capture).
+    struct CycleGraph {
+        int k;
+        const VT* base;
+        cudaGraphExec_t exec;
+        int64_t kernels;
+    };
+    std::vector<CycleGraph> graphs;
+    bool use_graphs = false;
+    int64_t graph_replays = 0;
+
+    ~BlockLanczos() {
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+    }
+    // steps [k, m): replayed from a captured graph when graphs are on, else launched one by one
+    void cycle(int k, int64_t& steps) {
+        steps += m - k;
+        if (use_graphs) {
+            for (auto& g : graphs)
+                if (g.k == k && g.base == V.p) {
+                    MOMED_CUDA_TRY(cudaGraphLaunch(g.exec, st));
+                    note_launches(g.kernels);
+                    ++graph_replays;
+                    return;
+                }
+            const int64_t l0 = launches_total();
+            cudaGraph_t graph = nullptr;
+            MOMED_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            bool ok = true;
+            try {
+                for (int j = k; j < m; ++j) step(j);
+            } catch (const Error&) {
+                ok = false;
+            }
+            cudaError_t e = cudaStreamEndCapture(st, &graph);
+            cudaGraphExec_t exec = nullptr;
+            if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+                cudaGraphDestroy(graph);
+                graphs.push_back({k, V.p, exec, launches_total() - l0});
+                MOMED_CUDA_TRY(cudaGraphLaunch(exec, st));
+                ++graph_replays;
+                return;
+            }
+            // capture refused: clear the error state and run this solve without graphs
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            use_graphs = false;
+        }
+        for (int j = k; j < m; ++j) step(j);
+    }
 
     BlockLanczos(momed_handle* hh, int mm, const std::vector<double>& u) : h(hh), N(hh->n), m(mm), st(hh->stream) {
+        {
+            const char* e = std::getenv("MOMED_GRAPHS");
+            use_graphs = !(e && e[0] == '0') && !hh->prof;   // per-launch timing needs eager launches
+        }
+        {   // kernel attributes are set before any capture
+            constexpr size_t smem_max = (size_t)kMaxCols * NB * sizeof(double2);
+            if (smem_max > 48 * 1024)
+                MOMED_CUDA_TRY(cudaFuncSetAttribute(k_bupdate<VT, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    (int)smem_max));
+        }
         grid = std::max(1, std::min<int>((int)((N + rows_tile<NB>() - 1) / rows_tile<NB>()), sms() * 4));   // max row blocks
         ugrid = std::max(1, std::min<int>((int)((N * NB + kT - 1) / kT), sms() * 8));
         V.resize((size_t)(m + 1) * N * NB);
@@ -457,12 +522,8 @@ struct BlockLanczos {
     }
     void update(int ncols, const double2* coef, VT* w, const int* active, const int* act) {
         size_t smem = (size_t)ncols * NB * sizeof(double2);
-        auto k = k_bupdate<VT, NB>;
-        // process-wide kernel attribute: always the largest size, so concurrent callers never lower it
-        constexpr size_t smem_max = (size_t)kMaxCols * NB * sizeof(double2);
-        if (smem_max > 48 * 1024)
-            MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max));
-        k<<<ugrid, kT, smem, st>>>(V.p, N, ncols, coef, w, npart.p, active, act);
+        // the shared-memory attribute (process-wide, always the largest size) is set by the constructor
+        k_bupdate<VT, NB><<<ugrid, kT, smem, st>>>(V.p, N, ncols, coef, w, npart.p, active, act);
         ++launches;
     }
     // column k0 made orthogonal to columns [0, k0) (two classical Gram-Schmidt passes), then normalised
@@ -553,7 +614,11 @@ struct BlockLanczos {
         std::vector<int> nconv(NB, 0);
         out.broken.assign(NB, 0);
         for (;;) {
-            for (int j = k; j < m; ++j) { step(j); ++steps; }
+            if (restarts == 0) {
+                for (int j = k; j < m; ++j) { step(j); ++steps; }
+            } else {
+                cycle(k, steps);
+            }
             MOMED_CUDA_TRY(cudaMemcpyAsync(ha.data(), alpha.p, ha.size() * 8, cudaMemcpyDeviceToHost, st));
             MOMED_CUDA_TRY(cudaMemcpyAsync(hb.data(), beta.p, hb.size() * 8, cudaMemcpyDeviceToHost, st));
             MOMED_CUDA_TRY(cudaStreamSynchronize(st));

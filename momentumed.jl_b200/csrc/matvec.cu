@@ -24,6 +24,10 @@
 //   - the index of a target is two independent table reads (index.cuh);
 //   - lanes accumulate privately and reduce with shuffles: no atomics.
 #include <algorithm>
+#include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "candidates.cuh"
 
@@ -287,7 +291,7 @@ __device__ __forceinline__ void consume_hits(const HitRing<R>& hl, int start, in
 template <typename R, int NB, bool HAS_B>
 __global__ void __launch_bounds__(kWarps * 32, (std::is_same<R, double>::value && NB == 32) ? 3 : 4)
 k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-                 const R* __restrict__ u, int64_t rows) {
+                 const R* __restrict__ u, int64_t rows, int rpw) {
     using C2 = typename Cx<R>::T;
     constexpr int RPL = Blk<R, NB>::RPL;
     constexpr int LPH = NB / RPL;      // lanes per hit
@@ -305,7 +309,10 @@ k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
     const C2* __restrict__ A = amp_a<R>(ov);
     const C2* __restrict__ B = amp_b<R>(ov);
     const unsigned lt = (1u << lane) - 1u;
-    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+    // a warp takes chunks of rpw consecutive rows (the autotuner's rows per warp)
+    const int64_t nchunks = (rows + rpw - 1) / rpw;
+    for (int64_t chunk = (int64_t)blockIdx.x * kWarps + wid; chunk < nchunks; chunk += (int64_t)gridDim.x * kWarps)
+    for (int64_t row = chunk * rpw; row < rows && row < (chunk + 1) * rpw; ++row) {
         const uint64_t s = __ldg(iv.basis + row);
         C2 aa[RPL], ab[RPL];
 #pragma unroll
@@ -453,20 +460,127 @@ void launch_count_hits(const IndexView& iv, const OpView& ov, unsigned long long
     note_launches(1);
 }
 
+// ---------------------------------------------------------------------------------------
+// Autotuner of the block map.  Two launch parameters are chosen by timing on the operator and
+// basis at hand, once per (term list, orbitals used, size class of the sector, block width,
+// precision): the persistent grid (resident CTAs per SM, or twice that for dynamic balance at
+// the tail) and the rows per warp (1, 2 or 4 consecutive rows per work item: neighbouring
+// basis states share most of their targets, so their x gathers meet in L1/L2).  Each candidate
+// runs twice (the second timed with CUDA events on the launching stream); the fastest is cached
+// for the process and reported by momed_block_tuning.  Tuning needs a stream outside capture;
+// a launch inside a capture before its key is tuned uses the default (resident grid, 1 row).
+struct TuneKey {
+    int64_t nterms, size_class;
+    int64_t groups;      // term groups and the per-row candidate bound: with nterms, the term list
+    int nb, dbl, hb;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(nterms, size_class, groups, nb, dbl, hb) <
+               std::tie(o.nterms, o.size_class, o.groups, o.nb, o.dbl, o.hb);
+    }
+};
+struct TuneChoice {
+    int grid_mult = 0;   // 0: resident CTAs per SM - 1, 1: resident, 2: twice resident
+    int rpw = 1;
+    float ms = 0.f, ms_default = 0.f;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneChoice> g_tune;
+
+bool autotune_enabled() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("MOMED_AUTOTUNE");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
+template <typename K>
+int tuned_grid(K kernel, int64_t rows, int rpw, int mult) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, 0);
+    if (per_sm <= 0) per_sm = 1;
+    const int64_t resident = (int64_t)sms * (mult == 0 ? std::max(1, per_sm - 1) : per_sm * mult);
+    const int64_t need = ((rows + rpw - 1) / rpw + kWarps - 1) / kWarps;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(need, resident));
+}
+
+template <typename R, int NBV, bool HB>
+void launch_block(const IndexView& iv, const OpView& ov, const typename Cx<R>::T* x, typename Cx<R>::T* y,
+                  const R* u, int64_t rows, cudaStream_t st, const TuneKey& key) {
+    auto k = k_block_matvec_v<R, NBV, HB>;
+    TuneChoice ch;
+    bool have = false;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) { ch = it->second; have = true; }
+    }
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (!have && autotune_enabled() && cs == cudaStreamCaptureStatusNone && rows >= 4096) {
+        cudaEvent_t e0, e1;
+        MOMED_CUDA_TRY(cudaEventCreate(&e0));
+        MOMED_CUDA_TRY(cudaEventCreate(&e1));
+        float best = 1e30f, dflt = 0.f;
+        for (int mult = 0; mult <= 2; ++mult)
+            for (int rpw : {1, 2, 4}) {
+                const int g = tuned_grid(k, rows, rpw, mult);
+                k<<<g, kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows, rpw);
+                MOMED_CUDA_TRY(cudaEventRecord(e0, st));
+                k<<<g, kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows, rpw);
+                MOMED_CUDA_TRY(cudaEventRecord(e1, st));
+                MOMED_CUDA_TRY(cudaEventSynchronize(e1));
+                MOMED_CUDA_TRY(cudaGetLastError());
+                note_launches(2);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (mult == 1 && rpw == 1) dflt = ms;
+                if (ms < best) { best = ms; ch.grid_mult = mult; ch.rpw = rpw; }
+            }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        ch.ms = best;
+        ch.ms_default = dflt;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune.emplace(key, ch);
+    } else if (!have) {
+        ch.grid_mult = 1;
+        ch.rpw = 1;
+    }
+    k<<<tuned_grid(k, rows, ch.rpw, ch.grid_mult), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows, ch.rpw);
+}
+
+TuneKey tune_key(const OpView& ov, int64_t rows, int nb, bool dbl, bool hb) {
+    TuneKey k;
+    k.nterms = ov.nterms;
+    int64_t c = 0;
+    while ((rows >> c) > 1) ++c;                  // sectors within a factor 2 share a choice
+    k.size_class = c;
+    k.groups = (int64_t)ov.ngroups * 4096 + ov.max_groups_per_row;
+    k.nb = nb;
+    k.dbl = dbl ? 1 : 0;
+    k.hb = hb ? 1 : 0;
+    return k;
+}
+
 template <typename R>
 static void block_dispatch(const IndexView& iv, const OpView& ov, const typename Cx<R>::T* x, typename Cx<R>::T* y,
                            const R* u, int32_t nb, int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
+    const TuneKey key = tune_key(ov, rows, nb, std::is_same<R, double>::value, hb);
 #define MOMED_BLK(NBV)                                                                                   \
     case NBV:                                                                                            \
-        if (hb) {                                                                                        \
-            auto k = k_block_matvec_v<R, NBV, true>;                                                     \
-            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);                  \
-        } else {                                                                                         \
-            auto k = k_block_matvec_v<R, NBV, false>;                                                    \
-            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(iv, ov, x, y, u, rows);                  \
-        }                                                                                                \
+        if (hb) launch_block<R, NBV, true>(iv, ov, x, y, u, rows, st, key);                             \
+        else launch_block<R, NBV, false>(iv, ov, x, y, u, rows, st, key);                               \
         break;
     switch (nb) {
         MOMED_BLK(1)
@@ -481,6 +595,19 @@ static void block_dispatch(const IndexView& iv, const OpView& ov, const typename
 #undef MOMED_BLK
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
+}
+
+bool block_tuning_lookup(const OpView& ov, int64_t rows, int nb, bool dbl, bool hb, int* grid_mult, int* rpw,
+                         float* ms, float* ms_default) {
+    const TuneKey key = tune_key(ov, rows, nb, dbl, hb);
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it == g_tune.end()) return false;
+    *grid_mult = it->second.grid_mult;
+    *rpw = it->second.rpw;
+    *ms = it->second.ms;
+    *ms_default = it->second.ms_default;
+    return true;
 }
 
 void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2* x, float2* y, const float* u,

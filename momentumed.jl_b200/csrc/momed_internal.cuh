@@ -287,6 +287,10 @@ void launch_block_matvec_c64(const IndexView& iv, const OpView& ov, const float2
 void launch_block_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y,
                               const double* u, int32_t nb, int64_t rows, cudaStream_t st);
 
+// the block map autotuner's choice for this operator, sector size class and block width
+bool block_tuning_lookup(const OpView& ov, int64_t rows, int nb, bool dbl, bool hb, int* grid_mult, int* rpw,
+                         float* ms, float* ms_default);
+
 // analysis.cu: one-body reduced density matrix of psi on the working basis ([norb][norb] c128)
 void rdm1(momed_handle* h, const double* psi, int norb, double* rdm);
 // ED_step_inner_prod of g vectors [g][N] on the working basis, orbital overlaps orb[norb] ([g][g] c128)

@@ -17,6 +17,7 @@
 // A solve is deterministic (seeded start vector, fixed reduction order), so a request's
 // result is the same alone and in any mix.
 #include <algorithm>
+#include <cstdlib>
 #include <chrono>
 #include <cstring>
 #include <condition_variable>
@@ -290,9 +291,16 @@ void worker_loop(momed_server* S, int slot) {
                     }
                 }
                 if (nu == 1) {
-                    // one right-hand side: the FP64 single-vector solver (a mixed request gets FP64
-                    // arithmetic throughout, which is faster here and at least as accurate)
-                    o.precision = MOMED_PREC_FP64;
+                    // one right-hand side: FP64 arithmetic (a mixed request gets FP64 throughout,
+                    // at least as accurate); momed_eigsolve picks the block solver for nev >= 2 on
+                    // large sectors.  MOMED_SERVE_ALONE=mixed keeps mixed precision for requests
+                    // alone (for measurements).
+                    static const bool alone_mixed = [] {
+                        const char* e = std::getenv("MOMED_SERVE_ALONE");
+                        return e && std::string(e) == "mixed";
+                    }();
+                    o.precision = (alone_mixed && r->opts.precision == MOMED_PREC_MIXED) ? MOMED_PREC_MIXED
+                                                                                         : MOMED_PREC_FP64;
                     rc = momed_eigsolve_impl(h, &o, nullptr, gvals.data(), gres.data(), nullptr, &ginfo);
                 } else {
                     std::vector<double> us(nu);

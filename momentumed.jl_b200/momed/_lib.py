@@ -73,6 +73,8 @@ SIGNATURES = {
     "momed_set_twobody_recipe": (C.c_int, [C.c_void_p, C.POINTER(Para), C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
                                            C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int64]),
     "momed_set_kshift": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "momed_block_tuning": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                                     C.POINTER(C.c_int32), C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "momed_eigsolve_general": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.POINTER(Info)]),
     "momed_batch_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_int32, C.c_void_p,
@@ -285,6 +287,17 @@ class Handle:
         ep = np.ascontiguousarray(entry_partner, np.int32)
         self._check(lib().momed_set_twobody_recipe(self._h, C.byref(p), kind, _p(prm), len(prm), _p(raw), len(raw),
                                                    _p(us), len(us) - 1, _p(eu), _p(ep), len(eu)))
+
+    def block_tuning(self, nb: int, precision: int = PREC_MIXED, has_param: bool = True):
+        """The block map autotuner's choice for this operator / sector class (None before tuning)."""
+        r, g, a, b = C.c_int32(), C.c_int32(), C.c_double(), C.c_double()
+        rc = lib().momed_block_tuning(self._h, nb, precision, int(has_param), C.byref(r), C.byref(g), C.byref(a),
+                                      C.byref(b))
+        if rc == ESTATE:
+            return None
+        self._check(rc)
+        return {"rows_per_warp": r.value, "grid": ["resident-1", "resident", "2x resident"][g.value],
+                "ms": a.value, "ms_default": b.value}
 
     def set_kshift(self, kshift):
         """Regenerate the recipe's amplitudes on the device at kshift [Nc_conserve][dim]."""
