@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--serve-meshes", default="3x5,3x9,3x10", help="subset of 3x5,3x9,3x10,4x9")
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-hbm-gb", type=float, default=100.0)
+    ap.add_argument("--serve-policy", default="", help="served arm switches: alone=fp64|mixed,sparse=1|0")
+    ap.add_argument("--serve-only", action="store_true", help="only the serving stream (one JSON object)")
     return ap.parse_args()
 
 
@@ -336,7 +338,13 @@ def serve_bench(args, device: int):
 
     # plain: one request at a time, FP64 single-vector Lanczos, live against arrivals; once with
     # the matrix-free map and once with the sparse method (the matrix built for each request)
-    def run_plain(sparse):
+    def run_plain(sparse, block=False):
+        # the plain GPU Lanczos is the reference's algorithm (single-vector Krylov) on the device;
+        # block=True runs the library's default solver (block Lanczos for nev >= 2) one at a time
+        if block:
+            os.environ.pop("MOMED_BLOCK", None)
+        else:
+            os.environ["MOMED_BLOCK"] = "0"
         vals_, lat_, service_ = [], [], []
         cur = None
         t0 = time.perf_counter()
@@ -358,11 +366,18 @@ def serve_bench(args, device: int):
             vals_.append(v)
             service_.append(s1 - s0)
             lat_.append(s1 - t0 - r["arrival"])
-        return vals_, lat_, service_, time.perf_counter() - t0
+        span = time.perf_counter() - t0
+        os.environ.pop("MOMED_BLOCK", None)
+        return vals_, lat_, service_, span
 
     plain_vals, plain_lat, plain_service, plain_span = run_plain(False)
     sp_vals, sp_lat, sp_service, sp_span = run_plain(True)
+    bl_vals, bl_lat, bl_service, bl_span = run_plain(False, block=True)
     h.close()
+    # serving policy switches (MOMED_SERVE_ALONE=fp64|mixed, MOMED_SERVE_SPARSE=1|0) for the served arm
+    for kv in [x for x in args.serve_policy.split(",") if x]:
+        k, v = kv.split("=")
+        os.environ[{"alone": "MOMED_SERVE_ALONE", "sparse": "MOMED_SERVE_SPARSE"}[k]] = v
 
     def run_server():
         srv = momed.Server(device, slots=args.serve_slots, hbm_budget=int(args.serve_hbm_gb * (1 << 30)))
@@ -415,14 +430,23 @@ def serve_bench(args, device: int):
         "plain_one_at_a_time": {"solves_per_s": n / plain_span, "latency_ms_p50": 1e3 * pct(plain_lat, 50),
                                 "latency_ms_p99": 1e3 * pct(plain_lat, 99),
                                 "service_ms_p50": 1e3 * pct(plain_service, 50), "precision": "fp64",
-                                "method": "map"},
+                                "method": "map, single-vector Lanczos"},
         "plain_sparse_one_at_a_time": {"solves_per_s": n / sp_span, "latency_ms_p50": 1e3 * pct(sp_lat, 50),
                                        "latency_ms_p99": 1e3 * pct(sp_lat, 99),
                                        "service_ms_p50": 1e3 * pct(sp_service, 50), "precision": "fp64",
-                                       "method": "sparse (matrix built per request)",
+                                       "method": "sparse (matrix built per request), single-vector Lanczos",
                                        "max_rel_eig_err_vs_map": max(
                                            float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0)))
                                            for a, b in zip(sp_vals, plain_vals))},
+        "solver_one_at_a_time": {"solves_per_s": n / bl_span, "latency_ms_p50": 1e3 * pct(bl_lat, 50),
+                                 "latency_ms_p99": 1e3 * pct(bl_lat, 99),
+                                 "service_ms_p50": 1e3 * pct(bl_service, 50), "precision": "fp64",
+                                 "method": "map, the library's default solver (block Lanczos for nev >= 2 on "
+                                           ">= 16384 states)",
+                                 "max_rel_eig_err_vs_map": max(
+                                     float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0)))
+                                     for a, b in zip(bl_vals, plain_vals))},
+        "policy": args.serve_policy or "default (alone: fp64, sparse method when it fits)",
         "speedup_served_vs_plain": (n / s_span) / (n / plain_span),
         "speedup_served_vs_plain_sparse": (n / s_span) / (n / sp_span),
     }
@@ -647,6 +671,12 @@ def main():
             import torch.distributed as dist
             dist.destroy_process_group()
         return
+    if args.serve_only:
+        if rank == 0:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps({"serving": serve_bench(args, local)}), flush=True)
+        return
     if args.workload != "batch_3x9":
         run_plain_workload(args, rank, world, local)
         if world > 1:
@@ -777,6 +807,7 @@ def main():
         h.set_scatter_pair(amp_a, amp_b, in_, out, pm)
         picks = sorted({int(round(j * (NU - 1) / max(args.plain - 1, 1))) for j in range(args.plain)})
         lat, errs = [], []
+        os.environ["MOMED_BLOCK"] = "0"          # the plain GPU Lanczos: single-vector Krylov
         for sidx, bvals, _ in all_vals:
             h.select_sector(sidx, len(sectors[sidx][1]))
             h.set_param(float(u[picks[0]]))               # untimed: this sector's index and operator checks
@@ -809,6 +840,22 @@ def main():
                 lat_sp.append(pe[0].elapsed_time(pe[1]))
                 errs.append(float(np.max(np.abs(bvals[j] - pv) / np.maximum(np.abs(pv), 1.0))))
         h.release_sparse()
+        os.environ.pop("MOMED_BLOCK", None)
+        # the same solves by the library's default FP64 solver (block Lanczos, B = 4 for nev 4)
+        lat_bl = []
+        for sidx, bvals, _ in all_vals:
+            h.select_sector(sidx, len(sectors[sidx][1]))
+            for j in picks:
+                h.set_param(float(u[j]))
+                pe = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+                torch.cuda.synchronize()
+                pe[0].record(stream)
+                pv, _, _, _ = h.eigsolve(NEV, krylovdim=KRYLOV, tol=1e-12, seed=1, want_vectors=False,
+                                         precision=_lib.PREC_FP64)
+                pe[1].record(stream)
+                torch.cuda.synchronize()
+                lat_bl.append(pe[0].elapsed_time(pe[1]))
+                errs.append(float(np.max(np.abs(bvals[j] - pv) / np.maximum(np.abs(pv), 1.0))))
         h.set_param(1.0)
         plain = {"solves_per_s": 1e3 * len(lat) / sum(lat), "latency_ms_p50": float(np.percentile(lat, 50)),
                  "latency_ms_p99": float(np.percentile(lat, 99)), "solves": len(lat),
@@ -816,7 +863,11 @@ def main():
                  "max_rel_eig_err_batched_vs_fp64": max(errs),
                  "sparse_method": {"solves_per_s": 1e3 * len(lat_sp) / sum(lat_sp),
                                    "latency_ms_p50": float(np.percentile(lat_sp, 50)),
-                                   "note": "the same solves with the matrix built per (sector, U0) inside the timing"}}
+                                   "note": "the same solves with the matrix built per (sector, U0) inside the timing"},
+                 "block_solver": {"solves_per_s": 1e3 * len(lat_bl) / sum(lat_bl),
+                                  "latency_ms_p50": float(np.percentile(lat_bl, 50)),
+                                  "note": "the same solves by the default FP64 solver (block Lanczos) on the map"},
+                 "solver": "single-vector FP64 Lanczos on the map (the reference's Krylov method)"}
 
     # ---------------------------------------------------------------- the same sweep on the sparse method
     # (each step builds the sector's CSR entries with A and B parts, then the batched solver runs its

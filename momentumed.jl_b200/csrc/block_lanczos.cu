@@ -440,10 +440,11 @@ struct BlockKrylov {
             mx = std::max(mx, std::hypot(b[i].x, b[i].y));
             d = std::max(d, std::hypot(a[i].x - b[i].x, a[i].y - b[i].y));
         }
-        // inner products of unit-norm FP32 vectors: the split-TF32 products carry ~2^-21
+        // split-TF32 products carry ~2^-21 and the tensor-memory sums over 256 rows are FP32:
+        // a few 1e-6 relative to the largest coefficient (H-scaled vectors reach |C| ~ |H|)
         const double rel = d / std::max(mx, 1e-30);
         tc_maxdiff = std::max(tc_maxdiff, d);
-        if (!(d <= 1e-5))
+        if (!(rel <= 1e-5))
             throw Error{MOMED_ECUDA, "tensor-core projection differs from the CUDA-core projection: max |diff| " +
                                          std::to_string(d) + " (relative " + std::to_string(rel) + ")"};
     }
@@ -646,6 +647,7 @@ struct BlockKrylov {
             // restart: keep the leading Ritz vectors (whole blocks), the residual block follows
             int keep = nev + (m - nev) / 3;
             keep = std::max(keep, std::min(nwant, m - B));
+            keep = std::min(keep, m - 3 * B);          // at least three new blocks per cycle
             int nkb = (keep + B - 1) / B;
             nkb = std::max(1, std::min(nkb, mb - 1));
             const int nk = nkb * B;
@@ -673,12 +675,23 @@ struct BlockKrylov {
     }
 };
 
-// basis blocks for a solve of nev pairs with Krylov dimension hint krylovdim
-int pick_blocks(int64_t N, int nev, int krylovdim, int B) {
-    int cols = std::max(krylovdim + B, nev + 3 * B);
-    cols = std::min(cols, std::min(kMaxBlkCols, kMaxCoef / B));
-    int mb = std::max(3, cols / B);
+// Basis blocks of a cycle.  A block Krylov space of mb blocks carries polynomials of degree mb
+// only, so a block basis must hold many more vectors than a single-vector one of the same
+// convergence: emulated on a 3x6 sector (nev 4-10), restarts with 20 blocks of 4 or 16 of 8
+// needed 1.1-1.7x the maps of the single-vector solver at krylovdim 30 (in 1/B of the
+// launches), 8 blocks of 8 needed 2-6x.  Capped by the kernels' column limits and by device
+// memory (the basis and its restart copy); 0 when even 6 blocks do not fit.
+int pick_blocks(int64_t N, int nev, int krylovdim, int B, size_t elem_bytes) {
+    int mb = B <= 4 ? 20 : (B <= 8 ? 16 : 8);
+    mb = std::max(mb, (krylovdim + B - 1) / B + 2);
+    mb = std::max(mb, (nev + B - 1) / B + 4);
+    mb = std::min(mb, std::min(kMaxBlkCols, kMaxCoef / B) / B);
     if ((int64_t)(mb + 1) * B > N) mb = (int)std::max<int64_t>(1, N / B - 1);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b > 0)
+        while (mb > 6 && 2.0 * (mb + 1) * (double)N * B * elem_bytes > 0.6 * (double)free_b) --mb;
+    if (mb < 6 || 2.0 * (mb + 1) * (double)N * B * elem_bytes > 0.6 * (double)(free_b ? free_b : ~size_t(0)))
+        return 0;
     return mb;
 }
 
@@ -689,7 +702,9 @@ int solve_blocked(momed_handle* h, const momed_solve_opts* o, int nev, const dou
     const int64_t N = h->n;
     const double tol = o->tol > 0 ? o->tol : 1e-12;
     const int maxiter = o->maxiter > 0 ? o->maxiter : 100;
-    const int mb = pick_blocks(N, nev, o->krylovdim > 0 ? o->krylovdim : 30, B);
+    const int mb = pick_blocks(N, nev, o->krylovdim > 0 ? o->krylovdim : 30, B,
+                               o->precision == MOMED_PREC_MIXED ? sizeof(float2) : sizeof(double2));
+    if (mb == 0) throw Breakdown{};           // no room for a block basis: the single-vector solver
     cudaStream_t st = h->stream;
     if (o->precision == MOMED_PREC_MIXED) {
         const int extra = std::min(4, std::max(0, mb * B - 2 * B - nev));
@@ -729,7 +744,9 @@ int solve_blocked(momed_handle* h, const momed_solve_opts* o, int nev, const dou
             return 0;
         }
         // FP64 block Lanczos warm-started from the refined vectors
-        BlockKrylov<double2, B> K(h, mb);
+        const int mb64 = pick_blocks(N, nev, o->krylovdim > 0 ? o->krylovdim : 30, B, sizeof(double2));
+        if (mb64 == 0) throw Breakdown{};
+        BlockKrylov<double2, B> K(h, mb64);
         auto r3 = K.run(nev, tol, 0.0, maxiter, X1.p, std::min(kk, B), o->seed, nev, X);
         theta = r3.theta;
         res = r3.resid;

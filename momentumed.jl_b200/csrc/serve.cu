@@ -104,7 +104,16 @@ int64_t estimate_bytes(int64_t N, const momed_solve_opts& o, int64_t nb = 0) {
     if (m > N) m = N;
     int64_t nev = o.nev;
     int64_t b = 8 * N;                                // basis
-    if (nb > 0) {
+    if (nb == 0 && nev >= 2 && N >= 16384) {
+        // the block solver (momed_eigsolve for nev >= 2 on large sectors): a block basis of mb
+        // blocks of B vectors and its restart copy (FP64 at worst), the Ritz and returned vectors
+        const int64_t B = nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
+        int64_t mb = B <= 4 ? 20 : (B <= 8 ? 16 : 8);
+        mb = std::max<int64_t>(mb, (m + B - 1) / B + 2);
+        mb = std::min<int64_t>(mb, std::min<int64_t>(256, 2048 / B) / B);
+        b += 2 * (mb + 1) * N * B * 16;
+        b += 4 * (nev + 4) * N * 16;
+    } else if (nb > 0) {
         // batched solver: the Krylov basis and its restart copy (FP64 fallback at worst), Ritz
         // vectors X, W = H X and scratch, the fallback's vectors and the returned vectors
         const int64_t k1 = nev + 4;
@@ -136,6 +145,12 @@ momed_solve_opts group_opts(const std::vector<std::shared_ptr<Request>>& g) {
     o.want_vectors = 0;
     o.vecs_on_device = 0;
     return o;
+}
+
+// policy switches read per request (environment; for measurements of the serving policy)
+std::string knob(const char* name, const char* dflt) {
+    const char* e = std::getenv(name);
+    return e ? std::string(e) : std::string(dflt);
 }
 
 int64_t pow2_at_least(int64_t n) {
@@ -189,7 +204,8 @@ void worker_loop(momed_server* S, int slot) {
             // ~0.8 s each alone on the sparse method.  The matrix size comes from the hits per row
             // that earlier solves on the operator measured.
             bool sparse_fits = false;
-            if (N >= kSparseMinRows && opp && r->op < (int32_t)S->op_hits_per_row.size()) {
+            if (N >= kSparseMinRows && opp && r->op < (int32_t)S->op_hits_per_row.size() &&
+                knob("MOMED_SERVE_SPARSE", "1") != "0") {
                 const double hpr = S->op_hits_per_row[r->op];
                 const int64_t sp = (N + 1) * 8 + (int64_t)((hpr + 1.0) * (double)N) * sparse_bytes_per_entry(opp->has_b);
                 sparse_fits = hpr > 0.0 && S->used + r->bytes + sp <= S->budget;
@@ -263,7 +279,7 @@ void worker_loop(momed_server* S, int slot) {
             // the sparse method when its matrix fits what the budget has left (its bytes are held
             // for this solve only); a group's batched solver then runs its FP32 maps as a block SpMV
             int64_t sp_bytes = 0;
-            if (N >= kSparseMinRows) {
+            if (N >= kSparseMinRows && knob("MOMED_SERVE_SPARSE", "1") != "0") {
                 ensure_ready(h);                      // index and validation: h->nnz counts every hit
                 const int64_t need = (N + 1) * 8 + (h->nnz + N) * sparse_bytes_per_entry(h->op.has_b);
                 std::lock_guard<std::mutex> lk(S->mu);
@@ -295,10 +311,7 @@ void worker_loop(momed_server* S, int slot) {
                     // at least as accurate); momed_eigsolve picks the block solver for nev >= 2 on
                     // large sectors.  MOMED_SERVE_ALONE=mixed keeps mixed precision for requests
                     // alone (for measurements).
-                    static const bool alone_mixed = [] {
-                        const char* e = std::getenv("MOMED_SERVE_ALONE");
-                        return e && std::string(e) == "mixed";
-                    }();
+                    const bool alone_mixed = knob("MOMED_SERVE_ALONE", "fp64") == "mixed";
                     o.precision = (alone_mixed && r->opts.precision == MOMED_PREC_MIXED) ? MOMED_PREC_MIXED
                                                                                          : MOMED_PREC_FP64;
                     rc = momed_eigsolve_impl(h, &o, nullptr, gvals.data(), gres.data(), nullptr, &ginfo);

@@ -73,34 +73,59 @@ function __init__()
     end
 end
 
-# The device map: one library handle holding the sorted basis and the completed term list.
+# The device map: one library handle holding the sorted basis and the term list of the LinearMap
+# (Hermitian-completed for an upper-Hermitian operator, as it is otherwise).
 mutable struct B200LinearMap{bits, F <: AbstractFloat} <: AbstractGPULinearMap{bits, F}
     handle::Ptr{Cvoid}
     space::HilbertSubspace{bits}
+    hermitian::Bool
+    terms::Tuple{Vector{ComplexF64}, Vector{UInt64}, Vector{UInt64}, Vector{UInt64}}   # amp, in, out, parity
 end
 
 Base.size(A::B200LinearMap) = (length(A.space), length(A.space))
 Base.eltype(::B200LinearMap{bits, F}) where {bits, F} = Complex{F}
-Base.adjoint(A::B200LinearMap) = A      # the completed list is Hermitian
+# AdjointLinearMap (linear_map.jl:46-55, 120-139): a completed Hermitian list is its own adjoint;
+# otherwise a device map over the adjoint terms (conjugated amplitudes, creation and annihilation
+# masks exchanged).
+function Base.adjoint(A::B200LinearMap{bits, F}) where {bits, F}
+    A.hermitian && return A
+    amp, inm, outm, par = A.terms
+    return device_map(B200LinearMap{bits, F}, A.space, false, (conj.(amp), outm, inm, par))
+end
+
+function device_map(::Type{T}, space, hermitian::Bool, terms) where {T}
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    check(C_NULL, ccall((:momed_create, libmomed), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, h))
+    basis = UInt64[mbs.n for mbs in space.list]
+    check(h[], ccall((:momed_set_basis, libmomed), Cint, (Ptr{Cvoid}, Ptr{UInt64}, Int64, Int32),
+                     h[], basis, length(basis), 0))
+    amp, inm, outm, par = terms
+    check(h[], ccall((:momed_set_scatter, libmomed), Cint,
+                     (Ptr{Cvoid}, Ptr{ComplexF64}, Ptr{UInt64}, Ptr{UInt64}, Ptr{UInt64}, Int64),
+                     h[], amp, inm, outm, par, length(amp)))
+    M = T(h[], space, hermitian, terms)
+    finalizer(m -> (m.handle != C_NULL && ccall((:momed_destroy, libmomed), Cint, (Ptr{Cvoid},), m.handle);
+                    m.handle = C_NULL), M)
+    return M
+end
 
 # create_gpu_linearmap hook (pattern of MomentumEDCUDAExt.jl:94-113): flatten and upload.
 function create_gpu_linearmap(A::LinearMap{bits, F}, ::Val{:b200}) where {bits, F}
-    h = Ref{Ptr{Cvoid}}(C_NULL)
-    check(C_NULL, ccall((:momed_create, libmomed), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, h))
-    basis = UInt64[mbs.n for mbs in A.space.list]
-    check(h[], ccall((:momed_set_basis, libmomed), Cint, (Ptr{Cvoid}, Ptr{UInt64}, Int64, Int32),
-                     h[], basis, length(basis), 0))
     amp = ComplexF64[ComplexF64(s.Amp) for s in A.scat_list]
     inm = UInt64[s.in.n for s in A.scat_list]
     outm = UInt64[s.out.n for s in A.scat_list]
     par = UInt64[s.parity_mask for s in A.scat_list]
-    check(h[], ccall((:momed_set_scatter, libmomed), Cint,
-                     (Ptr{Cvoid}, Ptr{ComplexF64}, Ptr{UInt64}, Ptr{UInt64}, Ptr{UInt64}, Int64),
-                     h[], amp, inm, outm, par, length(amp)))
-    M = B200LinearMap{bits, F}(h[], A.space)
-    finalizer(m -> (m.handle != C_NULL && ccall((:momed_destroy, libmomed), Cint, (Ptr{Cvoid},), m.handle);
-                    m.handle = C_NULL), M)
-    return M
+    return device_map(B200LinearMap{bits, F}, A.space, is_hermitian_list(amp, inm, outm), (amp, inm, outm, par))
+end
+
+# A list is Hermitian when every term's adjoint (masks exchanged, amplitude conjugated) is in it,
+# as the completion of an upper-Hermitian operator makes it (linear_map.jl:22-33).
+function is_hermitian_list(amp, inm, outm)
+    d = Dict{Tuple{UInt64, UInt64}, ComplexF64}()
+    for (a, i, o) in zip(amp, inm, outm)
+        d[(i, o)] = a
+    end
+    return all(get(d, (o, i), NaN + 0im) == conj(a) for (a, i, o) in zip(amp, inm, outm))
 end
 
 # callable (y, x): H*x with host vectors (the CPU LinearMap convention, linear_map.jl:100-118)
@@ -116,14 +141,28 @@ end
 function krylov_map_solve(H::B200LinearMap{bits, F}, N_eigen::Int64; ishermitian::Bool = true,
                           vec0 = nothing, krylovdim::Int = 30, tol::Real = 1e-12, maxiter::Int = 100,
                           seed::Integer = 0, precision::Symbol = :fp64, kwargs...) where {bits, F}
-    ishermitian || error("the B200 map solves Hermitian problems")
     m = length(H.space)
     nev = min(N_eigen, m)
+    vecs = zeros(ComplexF64, m, nev)            # column i = eigenvector i (layout [nev][N] in C)
+    resid = zeros(Float64, nev)
+    info = MomedInfo()
+    if !ishermitian
+        # Arnoldi with Krylov-Schur restarts: complex eigenvalues ordered by real part (:SR)
+        opts = MomedSolveOpts(nev, krylovdim, maxiter, 0, tol, seed, 1, 0)
+        vri = zeros(Float64, 2nev)
+        v0buf = vec0 === nothing ? ComplexF64[] : Vector{ComplexF64}(vec0)
+        GC.@preserve v0buf begin
+            v0 = vec0 === nothing ? Ptr{ComplexF64}(C_NULL) : pointer(v0buf)
+            check(H.handle, ccall((:momed_eigsolve_general, libmomed), Cint,
+                                  (Ptr{Cvoid}, Ref{MomedSolveOpts}, Ptr{ComplexF64}, Ptr{Float64}, Ptr{Float64},
+                                   Ptr{ComplexF64}, Ref{MomedInfo}),
+                                  H.handle, opts, v0, vri, resid, vecs, info))
+        end
+        vals = ComplexF64[complex(vri[2i - 1], vri[2i]) for i in 1:nev]
+        return vals, [Vector{Complex{F}}(vecs[:, i]) for i in 1:nev], info
+    end
     opts = MomedSolveOpts(nev, krylovdim, maxiter, precision === :mixed ? 1 : 0, tol, seed, 1, 0)
     vals = zeros(Float64, nev)
-    resid = zeros(Float64, nev)
-    vecs = zeros(ComplexF64, m, nev)            # column i = eigenvector i (layout [nev][N] in C)
-    info = MomedInfo()
     eigsolve_call(H.handle, opts, vec0, vals, resid, vecs, info)
     return vals, [Vector{Complex{F}}(vecs[:, i]) for i in 1:nev], info
 end

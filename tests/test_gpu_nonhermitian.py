@@ -26,10 +26,19 @@ def as_oracle(sl):
 
 
 def non_hermitian(a, b, seed):
-    """The one-body list plus the upper two-body list taken as it is (no completion)."""
+    """A genuinely non-Hermitian operator: the Hermitian-completed list of the recipe with the
+    amplitudes of the terms below the diagonal (in < out) multiplied by 1.3 exp(0.7 i), taken as it
+    is (upper_hermitian = false).  (The upper list alone is triangular in the sorted basis, with the
+    real diagonal as its spectrum.)"""
     para, _ = mesh_para(a, b, seed)
-    return para, momed.MBOperator(momed.ED_scatterlist_onebody(para), momed.ED_scatterlist_twobody(para),
-                                  upper_hermitian=False)
+    herm = momed.MBOperator(momed.ED_scatterlist_onebody(para), momed.ED_scatterlist_twobody(para),
+                            upper_hermitian=True)
+    full = core.hermitian_complete(herm)
+    amp = full.amp.copy()
+    low = full.in_ < full.out
+    amp[low] *= 1.3 * np.exp(0.7j)
+    sl = core.ScatterList(amp, full.out, full.in_, full.pm, full.bits, full.element_type)
+    return para, momed.MBOperator(sl, upper_hermitian=False)
 
 
 def lapack_sr(basis, op):

@@ -63,26 +63,31 @@ def setup(h, c):
     return basis
 
 
-def check(c, vals, vecs, resid, R):
+def check(c, vals, vecs, resid, R, fp64=True):
+    """FP64 solves: residual <= 1e-8 and overlap >= 1 - 1e-9 (Davis-Kahan, and the sketch).  Mixed
+    solves are accepted on eigenvalue accuracy (error ~ r^2 / gap <= 1e-11 |E|), so their
+    residuals reach ~1e-6 (stated, <= 1e-5 here) and the eigenvectors agree to ~r / gap: the
+    sketch deviation must stay within the Davis-Kahan bound (r_device + r_oracle) / gap."""
     nev = c["nev"]
     ref = np.asarray(c["vals"])
     err = np.abs(vals[:nev] - ref[:nev]) / np.abs(ref[:nev])
     assert np.max(err) <= 1e-10, (c["case"], err)
-    assert np.max(resid[:nev]) <= 1e-8, (c["case"], resid)
+    assert np.max(resid[:nev]) <= (1e-8 if fp64 else 1e-5), (c["case"], resid)
     for i in range(nev):
         others = np.delete(ref, i)
         gap = float(np.min(np.abs(others - ref[i])))
         if gap < 1e-6 * max(1.0, abs(ref[i])):
             continue                                     # a degenerate pair: no single-vector overlap
         sin_dk = (resid[i] + c["resid"][i]) / gap
-        assert np.sqrt(max(0.0, 1.0 - sin_dk ** 2)) >= 1 - 1e-9, (c["case"], i, sin_dk)
+        if fp64:
+            assert np.sqrt(max(0.0, 1.0 - sin_dk ** 2)) >= 1 - 1e-9, (c["case"], i, sin_dk)
         if vecs is not None:
             s_ref = np.asarray(c["sketch_re"][i]) + 1j * np.asarray(c["sketch_im"][i])
             s = R.conj() @ vecs[i]
             ph = np.vdot(s_ref, s)
             ph /= abs(ph)
             dev = np.linalg.norm(s - ph * s_ref) / np.linalg.norm(s_ref)
-            assert dev <= 5e-5, (c["case"], i, dev)
+            assert dev <= (5e-5 if fp64 else max(5e-5, 3.0 * sin_dk)), (c["case"], i, dev, sin_dk)
 
 
 CASES = sorted(FIX)
@@ -103,7 +108,7 @@ def test_single_vector_solver_vs_oracle(h, case, precision):
     prec = _lib.PREC_MIXED if precision == "mixed" else _lib.PREC_FP64
     vals, vecs, resid, info = h.eigsolve(c["nev"], krylovdim=c["krylovdim"], tol=1e-12, maxiter=300, seed=1,
                                          precision=prec)
-    check(c, vals, vecs, resid, probes(len(basis), c["sketch_seed"]))
+    check(c, vals, vecs, resid, probes(len(basis), c["sketch_seed"]), fp64=precision == "fp64")
 
 
 def test_batched_sweep_3x9_vs_oracle(h):
@@ -119,7 +124,7 @@ def test_batched_sweep_3x9_vs_oracle(h):
     for c in cs:
         j = int(np.argmin(np.abs(u - c["u"])))
         assert abs(u[j] - c["u"]) < 1e-15
-        check(c, vals[j], vecs[j], resid[j], R)
+        check(c, vals[j], vecs[j], resid[j], R, fp64=False)
 
 
 @pytest.mark.parametrize("case", [k for k in CASES if not k.startswith("c3_3x9_s3_")])
@@ -130,4 +135,4 @@ def test_batched_solver_vs_oracle(h, case):
                                             tol=1e-12, precision=_lib.PREC_MIXED, want_vectors=True)
     R = probes(len(basis), c["sketch_seed"])
     for j in range(2):
-        check(c, vals[j], vecs[j], resid[j], R)
+        check(c, vals[j], vecs[j], resid[j], R, fp64=False)
