@@ -460,10 +460,14 @@ def mv_bytes(N: int, nnz: int, nscat: int, s: int) -> float:
 
 
 def block_size(nev: int, N: int) -> int:
-    """Block size the eigensolver picks for nev pairs on N states (0: single-vector Lanczos)."""
-    if nev < 2 or N < 16384:
+    """Block size the FP64 eigensolver picks for nev pairs on N states (0: single-vector Lanczos;
+    block_size_for in block_lanczos.cu)."""
+    if os.environ.get("MOMED_BLOCK"):
+        b = int(os.environ["MOMED_BLOCK"])
+        return b if b in (4, 8, 16) and N >= 16 * b else 0
+    if nev < 2 or N < 500000:
         return 0
-    return 4 if nev <= 4 else (8 if nev <= 10 else 16)
+    return 4 if nev <= 10 else 8
 
 
 def sp_bytes(N: int, nnz_sp: int, s: int) -> float:

@@ -602,6 +602,9 @@ struct BlockLanczos {
         // 1/2 (3x9, 32 U0, nev 4: 16% faster; 0.01 the same); an FP32 basis with nev 12 in m 36
         // needed 1.65x the maps at 0.1, so FP32 with more wanted pairs keeps 1/2.
         dgks = (std::is_same<VT, float2>::value && 5 * nev > m) ? 0.5 : 0.1;
+        // graphs captured by an earlier run of this object carry that run's dgks: capture anew
+        for (auto& g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
         if (start) MOMED_CUDA_TRY(cudaMemcpyAsync(col(0), start, (size_t)N * NB * sizeof(VT), cudaMemcpyDeviceToDevice, st));
         else k_brandom<VT><<<ugrid, kT, 0, st>>>(col(0), N * NB, seed);
         normalize(col(0));

@@ -49,6 +49,13 @@ constexpr int kProjRows = 64;      // rows of W staged per tile in k_bl_proj
 constexpr int kMaxBlkCols = 256;   // basis columns one projection covers (m <= 256)
 constexpr int kMaxCoef = 2048;     // m * B coefficients one update holds in shared memory
 
+// row phases of a projection over ncol columns: all 256 threads busy for wide bases, at most 16
+// for the Gram matrix of one block (fewer partial sums to reduce)
+__host__ __device__ inline int proj_phases(int ncol) {
+    const int p = kBT / ncol;
+    return p < 16 ? p : 16;
+}
+
 template <typename VT> struct Real;
 template <> struct Real<float2> { using T = float; };
 template <> struct Real<double2> { using T = double; };
@@ -67,7 +74,7 @@ __global__ void __launch_bounds__(kBT)
 k_bl_proj(const VT* __restrict__ Q, int64_t blk_stride, int ncol, int64_t N, const VT* __restrict__ W,
           double2* __restrict__ partial) {
     __shared__ double2 wt[kProjRows * B];
-    const int P = kBT / ncol;                       // row phases (ncol <= kBT)
+    const int P = proj_phases(ncol);                // row phases (ncol <= kBT)
     const int t = threadIdx.x;
     const int c = t % ncol, p = t / ncol;
     const bool active = p < P;
@@ -83,6 +90,7 @@ k_bl_proj(const VT* __restrict__ Q, int64_t blk_stride, int ncol, int64_t N, con
         for (int e = t; e < rows * B; e += kBT) wt[e] = ld2(W + n0 * B + e);
         __syncthreads();
         if (active) {
+#pragma unroll 4
             for (int i = p; i < rows; i += P) {
                 const double2 q = ld2(qc + (n0 + i) * B);
 #pragma unroll
@@ -101,17 +109,30 @@ k_bl_proj(const VT* __restrict__ Q, int64_t blk_stride, int ncol, int64_t N, con
     }
 }
 
-// out[e] = sum over g < nparts of partial[g][e], e < count (fixed order: deterministic)
-__global__ void k_bl_reduce(const double2* __restrict__ partial, int nparts, int count, double2* __restrict__ out) {
-    const int e = blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= count) return;
-    double sx = 0.0, sy = 0.0;
-    for (int g = 0; g < nparts; ++g) {
+// out[e] = sum over g < nparts of partial[g][e]: one CTA per output, the threads take parts in
+// a fixed stride and a fixed tree combines them (deterministic; thousands of parts per output
+// for the Gram matrices of one block)
+__global__ void __launch_bounds__(256) k_bl_reduce(const double2* __restrict__ partial, int nparts, int count,
+                                                   double2* __restrict__ out) {
+    __shared__ double sx[256], sy[256];
+    const int e = blockIdx.x, t = threadIdx.x;
+    double ax = 0.0, ay = 0.0;
+    for (int g = t; g < nparts; g += 256) {
         const double2 v = partial[(size_t)g * count + e];
-        sx += v.x;
-        sy += v.y;
+        ax += v.x;
+        ay += v.y;
     }
-    out[e] = make_double2(sx, sy);
+    sx[t] = ax;
+    sy[t] = ay;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (t < o) {
+            sx[t] += sx[t + o];
+            sy[t] += sy[t + o];
+        }
+        __syncthreads();
+    }
+    if (t == 0) out[e] = make_double2(sx[0], sy[0]);
 }
 
 // W[n][r] -= sum_c Q_c[n] C[c][r]  (c < ncol; C [ncol][B] FP64, staged in shared memory as ACC)
@@ -417,7 +438,7 @@ struct BlockKrylov {
                 launch_proj_tc_c64(reinterpret_cast<const float2*>(base), ncol, N, reinterpret_cast<const float2*>(W),
                                    B, partial.p, pgrid * kBT / 64, &ns, tcerr.p, st);
                 const int count = ncol * B;
-                k_bl_reduce<<<(count + 255) / 256, 256, 0, st>>>(partial.p, ns, count, out);
+                k_bl_reduce<<<count, 256, 0, st>>>(partial.p, ns, count, out);
                 MOMED_CUDA_TRY(cudaGetLastError());
                 note_launches(1);
                 if (tc_check) check_tc(base, ncol, W, out);
@@ -440,6 +461,13 @@ struct BlockKrylov {
             mx = std::max(mx, std::hypot(b[i].x, b[i].y));
             d = std::max(d, std::hypot(a[i].x - b[i].x, a[i].y - b[i].y));
         }
+        // scale: the largest coefficient or the largest column norm of W (|q^H w| <= |w|), so that
+        // the tiny coefficients of a second Gram-Schmidt pass are judged against |w|
+        proj_cuda(W, B, W, ref.p);
+        std::vector<double2> g((size_t)B * B);
+        MOMED_CUDA_TRY(cudaMemcpyAsync(g.data(), ref.p, g.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
+        MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int r = 0; r < B; ++r) mx = std::max(mx, std::sqrt(std::max(g[(size_t)r * B + r].x, 0.0)));
         // split-TF32 products carry ~2^-21 and the tensor-memory sums over 256 rows are FP32:
         // a few 1e-6 relative to the largest coefficient (H-scaled vectors reach |C| ~ |H|)
         const double rel = d / std::max(mx, 1e-30);
@@ -450,9 +478,9 @@ struct BlockKrylov {
     }
     void proj_cuda(const VT* base, int ncol, const VT* W, double2* out) {
         k_bl_proj<VT, B><<<pgrid, kBT, 0, st>>>(base, N * B, ncol, N, W, partial.p);
-        const int P = kBT / ncol;
+        const int P = proj_phases(ncol);
         const int count = ncol * B;
-        k_bl_reduce<<<(count + 255) / 256, 256, 0, st>>>(partial.p, pgrid * P, count, out);
+        k_bl_reduce<<<count, 256, 0, st>>>(partial.p, pgrid * P, count, out);
         MOMED_CUDA_TRY(cudaGetLastError());
         note_launches(2);
     }
@@ -773,14 +801,20 @@ int solve_blocked(momed_handle* h, const momed_solve_opts* o, int nev, const dou
 // solve while a sparse matrix is built stays single-vector.  MOMED_BLOCK (environment) forces a
 // size (0 disables).
 int block_size_for(momed_handle* h, int nev, int precision) {
-    if (h->sparse_only) return 0;
+    if (h->sparse_only || h->block_solver == 0) return 0;
     if (h->sparse.built && precision != MOMED_PREC_MIXED) return 0;
     if (const char* e = std::getenv("MOMED_BLOCK")) {
         const int b = std::atoi(e);
         return (b == 4 || b == 8 || b == 16) && h->n >= 16 * b ? b : 0;
     }
-    if (nev < 2 || h->n < 16384) return 0;
-    return nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
+    // Measured on B200 (FP64 / mixed solves per second, single-vector -> block): 3x9 (174k states,
+    // nev 4) 6.69 -> 4.35 with B = 4 (the block needs 3.4x the maps: 560 against 165); 3x10 (1.0M,
+    // nev 6) 0.487 -> 0.647 with B = 4, 0.527 with B = 8 (mixed 0.34 / 0.50); two-component 4x6
+    // (4.7M, nev 8) 0.063 -> 0.067 with B = 8 (mixed 0.040 -> 0.058).  The block map's saving per
+    // vector grows with the sector, its extra maps do not: the block solver from 500k states.
+    if (nev < 2 || h->n < 500000) return 0;
+    if (precision == MOMED_PREC_MIXED) return nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
+    return nev <= 10 ? 4 : 8;
 }
 
 // The block solver's part of momed_eigsolve: fills theta/res (at least nev entries) and X

@@ -230,6 +230,7 @@ struct momed_handle {
     momed::Operator op;
     std::vector<int64_t> op_order;         // device term slot q holds entry op_order[q] of the uploaded list
     momed::TwoBodyRecipe recipe;           // amplitudes regenerated on the device (momed_set_kshift)
+    int32_t block_solver = -1;             // -1: the block solver when it pays, 0: single-vector only
     momed::SparseMatrix sparse;           // built by momed_build_sparse; maps use it while built
     bool sparse_only = false;              // an uploaded matrix (momed_set_sparse_csr) without a basis
     bool op_set = false;

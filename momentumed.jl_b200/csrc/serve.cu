@@ -53,6 +53,7 @@ struct Request {
     double u = 1.0;
     momed_solve_opts opts{};
     int64_t bytes = 0;
+    bool single = false;         // solved by the single-vector solver (the block basis exceeds the budget)
     clock_t_::time_point arrival, start, done;
     int32_t status = 0;          // 0 queued, 1 running, 2 done, 3 failed, 4 cancelled
     int32_t rc = MOMED_OK;
@@ -99,12 +100,12 @@ constexpr int64_t kSparseMinRows = 1 << 12;
 
 // HBM a solve needs: basis, index tables (bounded), Krylov basis, Ritz/refinement buffers.
 // nb: right-hand sides of a batched solve (a power of two), 0 for the single-vector solver.
-int64_t estimate_bytes(int64_t N, const momed_solve_opts& o, int64_t nb = 0) {
+int64_t estimate_bytes(int64_t N, const momed_solve_opts& o, int64_t nb = 0, bool single = false) {
     int64_t m = o.krylovdim > 0 ? o.krylovdim : 30;
     if (m > N) m = N;
     int64_t nev = o.nev;
     int64_t b = 8 * N;                                // basis
-    if (nb == 0 && nev >= 2 && N >= 16384) {
+    if (nb == 0 && !single && nev >= 2 && N >= 500000) {
         // the block solver (momed_eigsolve for nev >= 2 on large sectors): a block basis of mb
         // blocks of B vectors and its restart copy (FP64 at worst), the Ritz and returned vectors
         const int64_t B = nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
@@ -306,6 +307,7 @@ void worker_loop(momed_server* S, int slot) {
                         unreserve();          // the device is shorter than the budget: use the map
                     }
                 }
+                h->block_solver = (nu == 1 && r->single) ? 0 : -1;
                 if (nu == 1) {
                     // one right-hand side: FP64 arithmetic (a mixed request gets FP64 throughout,
                     // at least as accurate); momed_eigsolve picks the block solver for nev >= 2 on
@@ -415,6 +417,10 @@ MOMED_API int momed_serve_submit(momed_server* S, int32_t op_id, const uint64_t*
     r->u = u;
     r->opts = *opts;
     r->bytes = estimate_bytes(n, *opts);
+    if (r->bytes > S->budget) {          // the block solver's basis does not fit: single-vector Lanczos
+        r->single = true;
+        r->bytes = estimate_bytes(n, *opts, 0, true);
+    }
     uint64_t hsh = 0x9E3779B97F4A7C15ull ^ (uint64_t)n;
     for (int64_t i = 0; i < n; ++i) {
         hsh ^= basis[i] + 0x9E3779B97F4A7C15ull + (hsh << 6) + (hsh >> 2);

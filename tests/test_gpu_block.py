@@ -1,11 +1,12 @@
 """Block Lanczos (several Krylov vectors per map launch) against LAPACK and the single-vector solver.
 
-momed_eigsolve switches to the block solver for nev >= 2 on sectors of >= 16384 states; the
+momed_eigsolve switches to the block solver for nev >= 2 on sectors of >= 500k states; the
 MOMED_BLOCK environment variable forces a block size (4, 8, 16) or the single-vector solver (0),
 so these tests also run it on small sectors where LAPACK gives the exact answer.
 
 Bars: eigenvalues within 1e-10 relative of LAPACK (or of the single-vector FP64 solver on
-sectors too large for LAPACK), FP64 residuals <= 1e-9, eigenspace overlap >= 1 - 1e-9.
+sectors too large for LAPACK); FP64 solves: residuals <= 1e-9, eigenspace overlap >= 1 - 1e-9; mixed
+solves are accepted on eigenvalue accuracy (error ~ r^2 / gap), their residuals (~1e-6) stated.
 """
 import os
 from contextlib import contextmanager
@@ -88,14 +89,18 @@ def test_block_matches_single_vector_3x8(h):
             with block(b):
                 vals, vecs, resid, info = h.eigsolve(6, krylovdim=40, tol=1e-12, seed=1, precision=prec)
             assert np.max(np.abs(vals - ref) / np.abs(ref)) < 1e-10, (b, prec, vals, ref)
-            assert np.max(resid) <= 1e-9
-            assert overlap(rvecs.T, vecs.T) >= 1 - 1e-9
+            if prec == _lib.PREC_FP64:
+                assert np.max(resid) <= 1e-9
+                assert overlap(rvecs.T, vecs.T) >= 1 - 1e-9
+            else:                     # accepted on eigenvalue accuracy: residuals ~1e-6, stated
+                assert np.max(resid) <= 1e-5
+                assert overlap(rvecs.T, vecs.T) >= 1 - 1e-6
 
 
 def test_block_is_default_for_large_sectors(h):
-    """nev >= 2 on >= 16384 states takes the block solver: its maps are block-map launches."""
-    setup(h, 3, 8, 5, (8,), 2)
-    assert h.n >= 16384
+    """nev >= 2 on >= 500k states takes the block solver: its maps are block-map launches."""
+    setup(h, 3, 10, 1, (10,), 3)
+    assert h.n >= 500000
     h.profile(True)
     vals, _, resid, info = h.eigsolve(4, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
     nblk, _ = h.profile_read(_lib.KERNEL_BLOCK_MATVEC_C128)
@@ -103,6 +108,9 @@ def test_block_is_default_for_large_sectors(h):
     h.profile(False)
     assert nblk > 0 and info["converged"] >= 4
     assert nsingle <= 4 * 2            # only the final FP64 residual maps are single-vector
+    with block(0):                     # and MOMED_BLOCK=0 keeps the single-vector solver
+        ref, _, _, _ = h.eigsolve(4, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
+    assert np.max(np.abs(vals - ref) / np.abs(ref)) < 1e-10
 
 
 def test_block_start_vector_and_two_component(h):
