@@ -442,7 +442,7 @@ def serve_bench(args, device: int):
                                  "latency_ms_p99": 1e3 * pct(bl_lat, 99),
                                  "service_ms_p50": 1e3 * pct(bl_service, 50), "precision": "fp64",
                                  "method": "map, the library's default solver (block Lanczos for nev >= 2 on "
-                                           ">= 16384 states)",
+                                           ">= 500000 states)",
                                  "max_rel_eig_err_vs_map": max(
                                      float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0)))
                                      for a, b in zip(bl_vals, plain_vals))},
@@ -617,7 +617,8 @@ def run_plain_workload(args, rank, world, local):
                 pass
         N0 = len(sectors[order[W]][1])
         metric = ("solves/s (sparse method: device-built CSR matrix + FP64 single-vector Lanczos, one sector "
-                  "per step)" if sparse else "solves/s (plain FP64 single-vector Lanczos, one sector per step)")
+                  "per step)" if sparse else
+                  f"solves/s (plain FP64 {'block' if bsz else 'single-vector'} Lanczos, one sector per step)")
         if sparse:
             kernel = "CSR SpMV c128 (k_spmv<double>)"
             extra = {"sparse": {"build_ms_mean": float(np.mean(build_ms)), "entries_mean": float(np.mean(nnz_mean)),
