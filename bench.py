@@ -49,6 +49,9 @@ KRYLOV = 30
 # of `bench.py --profile-only` (dram__bytes_read.sum + dram__bytes_write.sum = 46.5 + 28.8 MB): the
 # x block and the term tables stay in L2, so the per-hit gathers of the algorithmic count hit L2.
 MV_DRAM_BYTES = 75.3e6
+# DRAM bytes per launch of the c64 block map over the hit cache (ncu dram__bytes_read + write on the
+# headline sector); None until captured
+MV_DRAM_BYTES_HC = None
 METRIC = "batched solves/s, p50/p99 latency vs plain GPU Lanczos at <=1e-10 eig error"
 
 
@@ -465,6 +468,8 @@ def block_size(nev: int, N: int) -> int:
     if os.environ.get("MOMED_BLOCK"):
         b = int(os.environ["MOMED_BLOCK"])
         return b if b in (4, 8, 16) and N >= 16 * b else 0
+    if os.environ.get("MOMED_HITCACHE", "") != "0":
+        return 0               # over the map's hit cache (built for every bench sector) single-vector wins
     if nev < 2 or N < 500000:
         return 0
     return 4 if nev <= 10 else 8
@@ -537,7 +542,12 @@ def run_plain_workload(args, rank, world, local):
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(K)]
     n_mv, ms_mv = h.profile_read(_lib.KERNEL_SPMV_C128 if sparse else _lib.KERNEL_MATVEC_C128)
     n_bmv, ms_bmv = h.profile_read(_lib.KERNEL_BLOCK_MATVEC_C128)
+    n_hmv, ms_hmv = h.profile_read(_lib.KERNEL_HC_MATVEC_C128)
+    n_hbmv, ms_hbmv = h.profile_read(_lib.KERNEL_HC_BLOCK_C128)
     h.profile(False)
+    use_hc = not sparse and (n_hmv + n_hbmv) > 0      # the solves ran over the map's hit cache
+    if use_hc:
+        n_mv, ms_mv, n_bmv, ms_bmv = n_hmv, ms_hmv, n_hbmv, ms_hbmv
     # nev >= 2 on large sectors runs the block solver (block_size_for in block_lanczos.cu): its maps
     # are block maps of B right-hand sides, the single-vector launches only the final residual maps
     bsz = block_size(nev, len(sectors[order[W]][1])) if not sparse else 0
@@ -546,12 +556,17 @@ def run_plain_workload(args, rank, world, local):
     launches = _lib.kernel_launches() - launches0
     elapsed = all_max(sum(step_ms) / 1e3, world)
     value = all_sum(K, world) / elapsed
-    nb, nnz_mean, build_ms = [], [], []
+    nb, nnz_mean, build_ms, hc_info = [], [], [], []
     for i in range(K):
         sidx = order[W + i]
         h.select_sector(sidx, len(sectors[sidx][1]))
         st = h.stats()
-        if sparse:
+        if use_hc:
+            hc = h.build_hit_cache()
+            hc_info.append(hc)
+            nb.append(hc_bytes(len(sectors[sidx][1]), hc["hits"], len(pair[0]), max(bsz, 1), 16))
+            nnz_mean.append(st["nnz"])
+        elif sparse:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             nsp = h.build_sparse()
@@ -626,11 +641,17 @@ def run_plain_workload(args, rank, world, local):
                                 "algorithmic_bytes": "column + c128 value per entry, row pointers, x and y once "
                                                      "(x gathers served from L2)"}}
         elif bsz:
-            kernel = f"block map c128 x{bsz} (k_block_matvec_v<double, {bsz}>, block Lanczos)"
+            kernel = (f"block map c128 x{bsz} over the hit cache (k_block_hc<double, {bsz}>, block Lanczos)" if use_hc
+                      else f"block map c128 x{bsz} (k_block_matvec_v<double, {bsz}>, block Lanczos)")
             extra = {"block_lanczos": {"block": bsz, "maps_per_launch": bsz}}
         else:
-            kernel = "map c128 (k_matvec<double>)"
+            kernel = "map c128 over the hit cache (k_matvec_hc<double>)" if use_hc else "map c128 (k_matvec<double>)"
             extra = {}
+        if use_hc:
+            extra["hit_cache"] = {"hits_per_sector": float(np.mean([c["hits"] for c in hc_info])),
+                                  "bytes_per_sector": float(np.mean([c["bytes"] for c in hc_info])),
+                                  "build_ms": float(np.mean([c["build_ms"] for c in hc_info])),
+                                  "note": "built inside each timed solve (first map of the sector)"}
         line = {
             "metric": metric, "value": value,
             "unit": "solves/s", "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": elapsed * 1e3 / K,
@@ -657,6 +678,13 @@ def run_plain_workload(args, rank, world, local):
 
 
 # ----------------------------------------------------------------------------- our arm
+def hc_bytes(N: int, hits: int, nscat: int, nb: int, s: int) -> float:
+    """Algorithmic bytes of one map launch over the hit cache: each row's hit range, run ends and
+    diagonal sums (A and B parts), x read and y written for nb right-hand sides, one 8-byte hit
+    record and one nb-wide gather per off-diagonal hit, and the amplitude table (A and B) once."""
+    return N * (16 + 2 * s + 2 * s * nb) + hits * (8 + s * nb) + nscat * 2 * s
+
+
 def block_bytes(N: int, nnz: int, nscat: int, nb: int, s: int) -> float:
     """Algorithmic bytes of one block matvec launch: basis keys, x stream read and y write for nb
     right-hand sides, one nb-wide gather per (row, term) hit, and the term list (two amplitudes
@@ -745,18 +773,27 @@ def main():
     # per-launch device time of the dominant kernel: the first (up to 3) timed sectors again with
     # per-launch events (which need eager launches: the timed steps replay captured graphs)
     h.profile(True)
+    hc_info = []
     for sidx, _, _ in all_vals[:3]:
         step_device(sidx)
+        hc_info.append(h.hit_cache_info())              # the cache the solve built (None: candidate map)
     torch.cuda.synchronize()
     n_mv, ms_mv = h.profile_read(_lib.KERNEL_BLOCK_MATVEC_C64)
+    n_hc, ms_hc = h.profile_read(_lib.KERNEL_HC_BLOCK_C64)
     h.profile(False)
+    use_hc = n_hc > 0
+    if use_hc:
+        n_mv, ms_mv = n_hc, ms_hc
     tuning = h.block_tuning(32, _lib.PREC_MIXED, True)
-    # algorithmic bytes of the dominant kernel (c64 block matvec), averaged over the timed sectors
+    # algorithmic bytes of the dominant kernel (c64 block map), averaged over the profiled sectors
     mv_bytes = []
-    for sidx, _, _ in all_vals[:3]:                      # the sectors the per-launch time was taken on
-        h.select_sector(sidx, len(sectors[sidx][1]))
-        st = h.stats()
-        mv_bytes.append(block_bytes(len(sectors[sidx][1]), st["nnz"], len(amp_a), 32, 8))
+    for (sidx, _, _), hc in zip(all_vals[:3], hc_info):
+        if use_hc:
+            mv_bytes.append(hc_bytes(len(sectors[sidx][1]), hc["hits"], len(amp_a), 32, 8))
+        else:
+            h.select_sector(sidx, len(sectors[sidx][1]))
+            st = h.stats()
+            mv_bytes.append(block_bytes(len(sectors[sidx][1]), st["nnz"], len(amp_a), 32, 8))
     bytes_per_launch = float(np.mean(mv_bytes))
     solves_local = K * NU
     elapsed_max = all_max(elapsed, world)
@@ -955,8 +992,10 @@ def main():
             "speedup_vs_plain_sparse": (value / world) / plain["sparse_method"]["solves_per_s"] if plain else None,
             "sparse_method_batched": sparse_batched,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": MV_DRAM_BYTES, "peak_source": peak_src,
-                         "kernel": "block matvec c64 x32 (k_block_matvec_v<float, 32>)",
+                         "frac": achieved / peak, "traffic": MV_DRAM_BYTES_HC if use_hc else MV_DRAM_BYTES,
+                         "peak_source": peak_src,
+                         "kernel": ("block map c64 x32 over the hit cache (k_block_hc<float, 32>)" if use_hc
+                                    else "block matvec c64 x32 (k_block_matvec_v<float, 32>)"),
                          "launches": n_mv, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "cpu_baseline": cpu,
@@ -968,6 +1007,11 @@ def main():
             "clocks": clk.summary(),
             "batching": {"cuda_graphs": "restart cycles replayed as captured graphs (first cycle eager)",
                          "block_map_autotune": tuning},
+            "hit_cache": ({"hits_per_sector": float(np.mean([c["hits"] for c in hc_info])),
+                           "bytes_per_sector": float(np.mean([c["bytes"] for c in hc_info])),
+                           "build_ms": float(np.mean([c["build_ms"] for c in hc_info])),
+                           "note": "built inside each timed step, at the sector's first map"}
+                          if use_hc else None),
             "solver": {"matvecs_per_step": int(np.mean([i["matvecs"] for i in infos])),
                        "fp64_matvecs_per_step": int(np.mean([i["matvecs_fp64"] for i in infos])),
                        "restarts_per_step": float(np.mean([i["restarts"] for i in infos])),

@@ -270,6 +270,21 @@ MOMED_API int  momed_serve_stop(momed_server* s);
 MOMED_API int  momed_block_tuning(momed_handle* h, int32_t nb, int32_t precision, int32_t has_param,
                                   int32_t* rows_per_warp, int32_t* grid_mult, double* ms, double* ms_default);
 
+/* Hit cache of the matrix-free map: for the current sector basis and term list, the target row
+ * and term slot of every off-diagonal (row, term) hit (8 bytes each) and each row's diagonal
+ * sums, so that a map skips the candidate stage (mask tests, signs, index lookups) and forms
+ * only the values, from the term list, at each application.  The eigensolvers build it at their
+ * start when it fits a quarter of the free device memory and no HBM budget is set
+ * (MOMED_HITCACHE=0: never, =1: whatever its size); momed_build_hit_cache builds it on request
+ * (MOMED_ENOMEM when it does not fit, MOMED_ESTATE while a sparse matrix is built).  It is
+ * dropped with the basis, the operator, a sparse-matrix build, or new amplitudes of a
+ * parametrised operator.  No reference counterpart: the reference map evaluates every term at
+ * every application (ka_linearmap_kernel!, MomentumED/src/method/gpu_interface.jl:128-163). */
+MOMED_API int  momed_build_hit_cache(momed_handle* h, int64_t* hits, int64_t* bytes);
+MOMED_API int  momed_hit_cache_info(momed_handle* h, int32_t* built, int64_t* hits, int64_t* bytes,
+                                    double* build_ms);
+MOMED_API int  momed_release_hit_cache(momed_handle* h);
+
 /* Kernels this library has launched in the process so far (all handles). */
 MOMED_API int64_t momed_kernel_launches(void);
 
@@ -283,6 +298,11 @@ MOMED_API int64_t momed_kernel_launches(void);
 #define MOMED_KERNEL_SPMV_C128          4
 #define MOMED_KERNEL_SPMV_C64           5
 #define MOMED_KERNEL_BLOCK_SPMV_C64     6
+#define MOMED_KERNEL_HC_MATVEC_C128     7   /* the map over its hit cache */
+#define MOMED_KERNEL_HC_MATVEC_C64      8
+#define MOMED_KERNEL_HC_BLOCK_C64       9
+#define MOMED_KERNEL_HC_BLOCK_C128      10
+#define MOMED_KERNEL_KINDS              11
 MOMED_API int  momed_profile(momed_handle* h, int32_t enable);
 MOMED_API int  momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms);
 

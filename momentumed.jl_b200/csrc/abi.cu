@@ -51,7 +51,7 @@ void prof_end(momed_handle* h, int kind) {
     if (!h->prof) return;
     h->prof_kind[(h->prof_used - 1) / 2] = kind;
     MOMED_CUDA_TRY(cudaEventRecord(h->prof_ev[h->prof_used++], h->stream));
-    if (kind >= 0 && kind < 7) ++h->prof_launches[kind];
+    if (kind >= 0 && kind < MOMED_KERNEL_KINDS) ++h->prof_launches[kind];
 }
 
 OpView Operator::view() const {
@@ -170,6 +170,7 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
     h->op_set = true;
     h->op_validated = false;
     h->sparse.release();
+    h->hcache.release();
 }
 
 // Build the index when the basis changed or the operator reaches bits outside it, and
@@ -272,6 +273,7 @@ void after_basis_change(momed_handle* h) {
     h->index_dirty = true;
     h->op_validated = false;
     h->sparse.release();
+    h->hcache.release();
     h->sparse_only = false;
 }
 
@@ -522,6 +524,10 @@ int momed_matvec(momed_handle* h, const void* x, void* y, int32_t precision, int
             launch_spmv_c128(h->sparse, (const double2*)dx, (double2*)dy, n, st);
         else if (h->sparse.built)
             launch_spmv_c64(h->sparse, (const float2*)dx, (float2*)dy, n, st);
+        else if (h->hcache.built && precision == MOMED_C128)
+            launch_matvec_hc_c128(h, (const double2*)dx, (double2*)dy, h->op.has_b ? h->u_dev.p : nullptr, n, st);
+        else if (h->hcache.built)
+            launch_matvec_hc_c64(h, (const float2*)dx, (float2*)dy, h->op.has_b ? h->u_dev32.p : nullptr, n, st);
         else if (precision == MOMED_C128)
             launch_matvec_c128(index_view(h), h->op.view(), (const double2*)dx, (double2*)dy,
                                h->op.has_b ? h->u_dev.p : nullptr, n, st);
@@ -706,19 +712,52 @@ int momed_last_kernel_ms(momed_handle* h, double* ms) {
 
 int64_t momed_kernel_launches(void) { return launches_total(); }
 
+int momed_build_hit_cache(momed_handle* h, int64_t* hits, int64_t* bytes) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_REQUIRE(!h->sparse.built && !h->sparse_only, MOMED_ESTATE,
+                      "a sparse matrix is built: maps read it (momed_release_sparse first)");
+        ensure_ready(h);
+        build_hit_cache(h);
+        if (hits) *hits = h->hcache.nnz;
+        if (bytes) *bytes = h->hcache.bytes;
+        return MOMED_OK;
+    });
+}
+
+int momed_hit_cache_info(momed_handle* h, int32_t* built, int64_t* hits, int64_t* bytes, double* build_ms) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        if (built) *built = h->hcache.built ? 1 : 0;
+        if (hits) *hits = h->hcache.nnz;
+        if (bytes) *bytes = h->hcache.bytes;
+        if (build_ms) *build_ms = h->hcache.build_ms;
+        return MOMED_OK;
+    });
+}
+
+int momed_release_hit_cache(momed_handle* h) {
+    if (!h) return MOMED_EINVAL;
+    return guarded(h, [&]() {
+        MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->hcache.release();
+        return MOMED_OK;
+    });
+}
+
 int momed_profile(momed_handle* h, int32_t enable) {
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {
         MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
         h->prof_used = 0;
-        for (int k = 0; k < 7; ++k) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; }
+        for (int k = 0; k < MOMED_KERNEL_KINDS; ++k) { h->prof_launches[k] = 0; h->prof_ms[k] = 0.0; }
         h->prof = enable != 0;
         return MOMED_OK;
     });
 }
 
 int momed_profile_read(momed_handle* h, int32_t kind, int64_t* launches, double* total_ms) {
-    if (!h || kind < 0 || kind > 6) return MOMED_EINVAL;
+    if (!h || kind < 0 || kind >= MOMED_KERNEL_KINDS) return MOMED_EINVAL;
     return guarded(h, [&]() {
         prof_drain(h);
         if (launches) *launches = h->prof_launches[kind];

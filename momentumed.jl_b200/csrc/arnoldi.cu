@@ -213,6 +213,7 @@ int momed_eigsolve_general_impl(momed_handle* h, const momed_solve_opts* o, cons
     MOMED_REQUIRE(!h->sparse.built && !h->sparse_only, MOMED_ESTATE,
                   "the non-Hermitian solver runs on the matrix-free map (release the sparse matrix first)");
     ensure_ready(h);
+    ensure_hit_cache(h);
     const int64_t N = h->n;
     MOMED_REQUIRE(o->nev >= 1, MOMED_EINVAL, "N should be at least 1");
     const int nev = (int)std::min<int64_t>(o->nev, N);

@@ -399,6 +399,11 @@ template <> struct BlockMv<float2> {
             prof_end(h, MOMED_KERNEL_BLOCK_SPMV_C64);
             return;
         }
+        if (h->hcache.built) {
+            launch_block_hc_c64(h, x, y, u, nb, h->n, h->stream);
+            prof_end(h, MOMED_KERNEL_HC_BLOCK_C64);
+            return;
+        }
         launch_block_matvec_c64(index_view(h), h->op.view(), x, y, u, nb, h->n, h->stream);
         prof_end(h, MOMED_KERNEL_BLOCK_MATVEC_C64);
     }
@@ -406,6 +411,11 @@ template <> struct BlockMv<float2> {
 template <> struct BlockMv<double2> {
     static void run(momed_handle* h, const double2* x, double2* y, const double* u, int nb) {
         prof_begin(h);
+        if (h->hcache.built) {
+            launch_block_hc_c128(h, x, y, u, nb, h->n, h->stream);
+            prof_end(h, MOMED_KERNEL_HC_BLOCK_C128);
+            return;
+        }
         launch_block_matvec_c128(index_view(h), h->op.view(), x, y, u, nb, h->n, h->stream);
         prof_end(h, MOMED_KERNEL_BLOCK_MATVEC_C128);
     }
@@ -1470,6 +1480,7 @@ using namespace momed;
 int momed_batch_solve_impl(momed_handle* h, const momed_solve_opts* o, const double* u, int32_t nu, double* vals,
                            double* resid, double* vecs, momed_info* info) {
     ensure_ready(h);
+    if (!h->sparse.built) ensure_hit_cache(h);
     // without a second operator (momed_set_scatter) every parameter solves H = A
     MOMED_REQUIRE(nu >= 1 && nu <= 32, MOMED_EINVAL, "nu must be 1..32 per call");
     int nb = 1;

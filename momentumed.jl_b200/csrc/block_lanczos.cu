@@ -415,6 +415,9 @@ struct BlockKrylov {
                 launch_block_spmv_c64(h->sparse, reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(y), u,
                                       B, N, st);
                 prof_end(h, MOMED_KERNEL_BLOCK_SPMV_C64);
+            } else if (h->hcache.built) {
+                launch_block_hc_c64(h, reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(y), u, B, N, st);
+                prof_end(h, MOMED_KERNEL_HC_BLOCK_C64);
             } else {
                 launch_block_matvec_c64(index_view(h), h->op.view(), reinterpret_cast<const float2*>(x),
                                         reinterpret_cast<float2*>(y), u, B, N, st);
@@ -422,9 +425,15 @@ struct BlockKrylov {
             }
         } else {
             const double* u = h->op.has_b ? reinterpret_cast<const double*>(ud.p) : nullptr;
-            launch_block_matvec_c128(index_view(h), h->op.view(), reinterpret_cast<const double2*>(x),
-                                     reinterpret_cast<double2*>(y), u, B, N, st);
-            prof_end(h, MOMED_KERNEL_BLOCK_MATVEC_C128);
+            if (h->hcache.built) {
+                launch_block_hc_c128(h, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), u, B, N,
+                                     st);
+                prof_end(h, MOMED_KERNEL_HC_BLOCK_C128);
+            } else {
+                launch_block_matvec_c128(index_view(h), h->op.view(), reinterpret_cast<const double2*>(x),
+                                         reinterpret_cast<double2*>(y), u, B, N, st);
+                prof_end(h, MOMED_KERNEL_BLOCK_MATVEC_C128);
+            }
         }
         matvecs += B;
     }
@@ -807,11 +816,14 @@ int block_size_for(momed_handle* h, int nev, int precision) {
         const int b = std::atoi(e);
         return (b == 4 || b == 8 || b == 16) && h->n >= 16 * b ? b : 0;
     }
-    // Measured on B200 (FP64 / mixed solves per second, single-vector -> block): 3x9 (174k states,
-    // nev 4) 6.69 -> 4.35 with B = 4 (the block needs 3.4x the maps: 560 against 165); 3x10 (1.0M,
-    // nev 6) 0.487 -> 0.647 with B = 4, 0.527 with B = 8 (mixed 0.34 / 0.50); two-component 4x6
-    // (4.7M, nev 8) 0.063 -> 0.067 with B = 8 (mixed 0.040 -> 0.058).  The block map's saving per
-    // vector grows with the sector, its extra maps do not: the block solver from 500k states.
+    // Measured on B200 (FP64 / mixed solves per second, single-vector -> block) with the candidate
+    // map: 3x9 (174k states, nev 4) 6.69 -> 4.35 with B = 4 (the block needs 2.8x the maps: 464
+    // against 165); 3x10 (1.0M, nev 6) 0.487 -> 0.647 with B = 4, 0.527 with B = 8 (mixed 0.34 /
+    // 0.50); two-component 4x6 (4.7M, nev 8) 0.063 -> 0.080 with B = 4, 0.067 with B = 8 (mixed
+    // 0.040 -> 0.058).  The block map's saving is the candidate stage shared by B vectors; over a
+    // hit cache there is no candidate stage and the single-vector solver wins (3x10: 1.91 against
+    // 1.60 with B = 4).  So: the block solver from 500k states when the map has no hit cache.
+    if (h->hcache.built) return 0;
     if (nev < 2 || h->n < 500000) return 0;
     if (precision == MOMED_PREC_MIXED) return nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
     return nev <= 10 ? 4 : 8;

@@ -44,11 +44,17 @@ template <> struct Prec<double2> { static constexpr int value = MOMED_C128; };
 template <> struct Prec<float2> { static constexpr int value = MOMED_C64; };
 
 // the CSR SpMV while a sparse matrix is built (momed_build_sparse), else the matrix-free map
+// (over its hit cache while one is built)
 void apply_h(momed_handle* h, const double2* x, double2* y) {
     prof_begin(h);
     if (h->sparse.built) {
         launch_spmv_c128(h->sparse, x, y, h->n, h->stream);
         prof_end(h, MOMED_KERNEL_SPMV_C128);
+        return;
+    }
+    if (h->hcache.built) {
+        launch_matvec_hc_c128(h, x, y, h->op.has_b ? h->u_dev.p : nullptr, h->n, h->stream);
+        prof_end(h, MOMED_KERNEL_HC_MATVEC_C128);
         return;
     }
     launch_matvec_c128(index_view(h), h->op.view(), x, y, h->op.has_b ? h->u_dev.p : nullptr, h->n, h->stream);
@@ -59,6 +65,11 @@ void apply_h(momed_handle* h, const float2* x, float2* y) {
     if (h->sparse.built) {
         launch_spmv_c64(h->sparse, x, y, h->n, h->stream);
         prof_end(h, MOMED_KERNEL_SPMV_C64);
+        return;
+    }
+    if (h->hcache.built) {
+        launch_matvec_hc_c64(h, x, y, h->op.has_b ? h->u_dev32.p : nullptr, h->n, h->stream);
+        prof_end(h, MOMED_KERNEL_HC_MATVEC_C64);
         return;
     }
     launch_matvec_c64(index_view(h), h->op.view(), x, y, h->op.has_b ? h->u_dev32.p : nullptr, h->n, h->stream);
@@ -393,7 +404,10 @@ using namespace momed;
 
 int momed_eigsolve_impl(momed_handle* h, const momed_solve_opts* o, const double* vec0, double* vals, double* resid,
                         void* vecs, momed_info* info) {
-    if (!h->sparse.built) ensure_ready(h);   // a built sparse matrix needs no index or operator check
+    if (!h->sparse.built) {                  // a built sparse matrix needs no index or operator check
+        ensure_ready(h);
+        ensure_hit_cache(h);
+    }
     const int64_t N = h->n;
     const int nev = (int)std::min<int64_t>(o->nev, N);
     MOMED_REQUIRE(o->nev >= 1, MOMED_EINVAL, "N should be at least 1");

@@ -29,7 +29,7 @@
 #include <mutex>
 #include <tuple>
 
-#include "candidates.cuh"
+#include "blockio.cuh"
 
 namespace momed {
 
@@ -209,20 +209,8 @@ k_count(IndexView iv, OpView ov, unsigned long long* hits, unsigned long long* m
 // right-hand sides (one index lookup per hit); hits are compacted into three lists by amplitude
 // kind (B only, A only, both), and each hit's NB values are read by LPH = NB / RPL lanes with RPL
 // right-hand sides per lane (RPL = min(NB, 4) for c64; for c128 2 at NB = 32, else 1: 16-byte
-// loads), so one warp iteration consumes HPI = 32 / LPH hits.  B-only hits accumulate into
-// a separate sum that is scaled by u once per row.
-template <typename R> struct BlkMax;
-template <> struct BlkMax<float> { static constexpr int RPL = 4; };
-template <> struct BlkMax<double> { static constexpr int RPL = 2; };
-template <typename R, int NB> struct Blk {
-    static constexpr int RPL = NB < BlkMax<R>::RPL ? NB : BlkMax<R>::RPL;
-};
-// c128 below 32 right-hand sides: one 16-byte value per lane keeps the register count (and so the
-// occupancy) of the candidate stage; two per lane measured slower there
-template <int NB> struct Blk<double, NB> {
-    static constexpr int RPL = NB == 32 ? 2 : 1;
-};
-
+// loads, laid out as blockio.cuh describes), so one warp iteration consumes HPI = 32 / LPH hits.
+// B-only hits accumulate into a separate sum that is scaled by u once per row.
 // Per-warp rings of found hits, one per amplitude kind.  A batch of 32 candidates yields about
 // a dozen hits; they wait in the ring until 32 of a kind are pending, so the accumulation runs
 // whole iterations and keeps several gathers in flight.
@@ -233,30 +221,10 @@ template <typename R> struct HitRing {
     typename Cx<R>::T cb[kRing];
 };
 
-// RPL consecutive complex values starting at p (p aligned to RPL values)
-template <typename R, int RPL>
-__device__ __forceinline__ void load_rpl(const typename Cx<R>::T* __restrict__ p, typename Cx<R>::T* v) {
-    if constexpr (std::is_same<R, float>::value && RPL == 4) {
-        float4 a = __ldg(reinterpret_cast<const float4*>(p));
-        float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
-        v[0] = make_float2(a.x, a.y);
-        v[1] = make_float2(a.z, a.w);
-        v[2] = make_float2(b.x, b.y);
-        v[3] = make_float2(b.z, b.w);
-    } else if constexpr (std::is_same<R, float>::value && RPL == 2) {
-        float4 a = __ldg(reinterpret_cast<const float4*>(p));
-        v[0] = make_float2(a.x, a.y);
-        v[1] = make_float2(a.z, a.w);
-    } else {
-#pragma unroll
-        for (int q = 0; q < RPL; ++q) v[q] = __ldg(p + q);
-    }
-}
-
 // Accumulate the hits at ring positions start .. start + n - 1 (mod kRing) of amplitude kind KIND
 // into acc: each hit's NB values are read by NB / RPL lanes.  N > 0 fixes n = N at compile time.
 template <typename R, int NB, int KIND, int N>
-__device__ __forceinline__ void consume_hits(const HitRing<R>& hl, int start, int n, int hslot, int r0,
+__device__ __forceinline__ void consume_hits(const HitRing<R>& hl, int start, int n, int hslot, int kk,
                                              const typename Cx<R>::T* __restrict__ x, const R* ur,
                                              typename Cx<R>::T* acc) {
     using C2 = typename Cx<R>::T;
@@ -268,7 +236,7 @@ __device__ __forceinline__ void consume_hits(const HitRing<R>& hl, int start, in
         C2 cb;
         if constexpr (KIND == 2) cb = hl.cb[p];
         C2 xv[RPL];
-        load_rpl<R, RPL>(x + (int64_t)hl.j[KIND][p] * NB + r0, xv);
+        load_lane<R, NB>(x + (int64_t)hl.j[KIND][p] * NB, kk, xv);
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
             R cx = c.x, cy = c.y;
@@ -300,12 +268,12 @@ k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
     __shared__ HitRing<R> s_hits[kWarps];
     stage_tables(sh, iv);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int hslot = lane / LPH, r0 = (lane % LPH) * RPL;
+    const int hslot = lane / LPH, kk = lane % LPH;
     WarpScratch& ws = s_ws[wid];
     HitRing<R>& hl = s_hits[wid];
     R ur[RPL];
 #pragma unroll
-    for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? u[r0 + q] : R(0);
+    for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? u[BlkIO<R, NB>::rhs(kk, q)] : R(0);
     const C2* __restrict__ A = amp_a<R>(ov);
     const C2* __restrict__ B = amp_b<R>(ov);
     const unsigned lt = (1u << lane) - 1u;
@@ -357,26 +325,26 @@ k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
                 n2 += __popc(m2);
                 __syncwarp();
                 if (HAS_B && n0 >= 32) {          // B only: accumulate, scale by u once per row
-                    consume_hits<R, NB, 0, 32>(hl, hd0, 32, hslot, r0, x, ur, ab);
+                    consume_hits<R, NB, 0, 32>(hl, hd0, 32, hslot, kk, x, ur, ab);
                     hd0 = (hd0 + 32) & (kRing - 1);
                     n0 -= 32;
                 }
                 if (n1 >= 32) {                   // A only
-                    consume_hits<R, NB, 1, 32>(hl, hd1, 32, hslot, r0, x, ur, aa);
+                    consume_hits<R, NB, 1, 32>(hl, hd1, 32, hslot, kk, x, ur, aa);
                     hd1 = (hd1 + 32) & (kRing - 1);
                     n1 -= 32;
                 }
                 if (HAS_B && n2 >= 32) {          // both: A + u B per right-hand side
-                    consume_hits<R, NB, 2, 32>(hl, hd2, 32, hslot, r0, x, ur, aa);
+                    consume_hits<R, NB, 2, 32>(hl, hd2, 32, hslot, kk, x, ur, aa);
                     hd2 = (hd2 + 32) & (kRing - 1);
                     n2 -= 32;
                 }
                 __syncwarp();
             }
         });
-        if (HAS_B) consume_hits<R, NB, 0, 0>(hl, hd0, n0, hslot, r0, x, ur, ab);
-        consume_hits<R, NB, 1, 0>(hl, hd1, n1, hslot, r0, x, ur, aa);
-        if (HAS_B) consume_hits<R, NB, 2, 0>(hl, hd2, n2, hslot, r0, x, ur, aa);
+        if (HAS_B) consume_hits<R, NB, 0, 0>(hl, hd0, n0, hslot, kk, x, ur, ab);
+        consume_hits<R, NB, 1, 0>(hl, hd1, n1, hslot, kk, x, ur, aa);
+        if (HAS_B) consume_hits<R, NB, 2, 0>(hl, hd2, n2, hslot, kk, x, ur, aa);
         __syncwarp();
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -398,16 +366,15 @@ k_block_matvec_v(IndexView iv, OpView ov, const typename Cx<R>::T* __restrict__ 
             }
         }
         if (hslot == 0) {
-            C2 xd[RPL];
-            load_rpl<R, RPL>(x + row * NB + r0, xd);
+            C2 xd[RPL], o[RPL];
+            load_lane<R, NB>(x + row * NB, kk, xd);
 #pragma unroll
             for (int q = 0; q < RPL; ++q) {
                 R cx = dax + ur[q] * dbx, cy = day + ur[q] * dby;
-                C2 o;
-                o.x = aa[q].x + cx * xd[q].x - cy * xd[q].y;
-                o.y = aa[q].y + cx * xd[q].y + cy * xd[q].x;
-                y[row * NB + r0 + q] = o;
+                o[q].x = aa[q].x + cx * xd[q].x - cy * xd[q].y;
+                o[q].y = aa[q].y + cx * xd[q].y + cy * xd[q].x;
             }
+            store_lane<R, NB>(y + row * NB, kk, o);
         }
     }
 }

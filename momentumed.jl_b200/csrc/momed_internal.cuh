@@ -205,6 +205,37 @@ struct SparseMatrix {
     }
 };
 
+// Hit cache of the matrix-free map (hitcache.cu): per sector basis and term list, every
+// off-diagonal hit's target row and term slot (sign in bit 31), in runs by amplitude kind.
+struct HitCacheView {
+    const int64_t* row_ptr;    // [n + 1]
+    const int2* seg;           // [n] ends of the B-only and A-only runs, relative to row_ptr[row]
+    const uint2* hit;          // [nnz] {target row, term slot | sign << 31}
+    const double2* dg64;       // [2n] diagonal sums: A part, B part
+    const float2* dg32;        // [2n] the same in c64
+};
+
+struct HitCache {
+    bool built = false;
+    int64_t nnz = 0, bytes = 0;
+    double build_ms = 0.0;
+    DevBuf<int64_t> row_ptr;
+    DevBuf<int2> seg;
+    DevBuf<uint2> hit;
+    DevBuf<double2> dg64;
+    DevBuf<float2> dg32;
+    HitCacheView view() const;
+    void release() {
+        built = false;
+        nnz = bytes = 0;
+        row_ptr.release();
+        seg.release();
+        hit.release();
+        dg64.release();
+        dg32.release();
+    }
+};
+
 struct Index {
     int32_t mode = INDEX_SEARCH;
     PartDesc hi{}, lo{};
@@ -232,6 +263,8 @@ struct momed_handle {
     momed::TwoBodyRecipe recipe;           // amplitudes regenerated on the device (momed_set_kshift)
     int32_t block_solver = -1;             // -1: the block solver when it pays, 0: single-vector only
     momed::SparseMatrix sparse;           // built by momed_build_sparse; maps use it while built
+    momed::HitCache hcache;               // maps use it while built (and no sparse matrix is)
+    bool hit_cache_ok = true;              // the solvers may build it (not on serving slots)
     bool sparse_only = false;              // an uploaded matrix (momed_set_sparse_csr) without a basis
     bool op_set = false;
     bool op_validated = false;
@@ -256,8 +289,8 @@ struct momed_handle {
     std::vector<cudaEvent_t> prof_ev;      // pairs (start, stop)
     std::vector<int> prof_kind;            // kind of each pair
     size_t prof_used = 0;                  // events used in the current record
-    int64_t prof_launches[7] = {0, 0, 0, 0, 0, 0, 0};
-    double prof_ms[7] = {0, 0, 0, 0, 0, 0, 0};      // folded-in time of pairs already read
+    int64_t prof_launches[MOMED_KERNEL_KINDS] = {};
+    double prof_ms[MOMED_KERNEL_KINDS] = {};        // folded-in time of pairs already read
 };
 
 namespace momed {
@@ -269,6 +302,20 @@ const uint32_t* device_binomials();
 void build_index(momed_handle* h);
 IndexView index_view(const momed_handle* h);
 int64_t validate_operator(momed_handle* h);   // counts (row, term) targets missing from the basis
+
+// hitcache.cu
+int64_t hit_cache_bytes(int64_t n, int64_t hits);
+bool hit_cache_wanted(const momed_handle* h);
+void build_hit_cache(momed_handle* h);
+void ensure_hit_cache(momed_handle* h);
+void launch_matvec_hc_c128(const momed_handle* h, const double2* x, double2* y, const double* u, int64_t rows,
+                           cudaStream_t st);
+void launch_matvec_hc_c64(const momed_handle* h, const float2* x, float2* y, const float* u, int64_t rows,
+                          cudaStream_t st);
+void launch_block_hc_c64(const momed_handle* h, const float2* x, float2* y, const float* u, int32_t nb, int64_t rows,
+                         cudaStream_t st);
+void launch_block_hc_c128(const momed_handle* h, const double2* x, double2* y, const double* u, int32_t nb,
+                          int64_t rows, cudaStream_t st);
 
 // matvec.cu
 void launch_matvec_c128(const IndexView& iv, const OpView& ov, const double2* x, double2* y,

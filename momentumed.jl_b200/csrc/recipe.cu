@@ -232,6 +232,7 @@ void set_kshift(momed_handle* h, const double* kshift) {
     }
     MOMED_CUDA_TRY(cudaStreamSynchronize(st));   // sh is read by the async copy
     h->sparse.release();                          // its values were built from the old amplitudes
+    if (h->op.has_b) h->hcache.release();         // its runs are sorted by which parts are non-zero
 }
 
 }  // namespace momed

@@ -383,6 +383,7 @@ MOMED_API int momed_serve_start(int device, int32_t slots, int64_t hbm_budget, m
             delete S;
             return rc;
         }
+        h->hit_cache_ok = false;           // the admission budget does not count a hit cache
         S->handles.push_back(h);
     }
     for (int i = 0; i < slots; ++i) S->workers.emplace_back(worker_loop, S, i);

@@ -31,9 +31,10 @@
 // map does.  A host matrix (create_gpu_matrix of the reference's host CSC) can be uploaded
 // instead of built (upload_sparse), after validation of its row pointers and columns.
 #include <algorithm>
+#include <cstdlib>
 #include <string>
 
-#include "candidates.cuh"
+#include "blockio.cuh"
 
 namespace momed {
 
@@ -168,7 +169,29 @@ template <typename R> struct SpVal;
 template <> struct SpVal<double> { using T = double2; };
 template <> struct SpVal<float> { using T = float2; };
 
-template <typename R>
+// Streaming loads of the column and value arrays: read once per SpMV, so they are not allocated
+// in L1, which keeps it for the x gathers (ld.global.nc.L1::no_allocate).
+__device__ __forceinline__ int32_t ld_stream(const int32_t* p) {
+    int32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double2 ld_stream(const double2* p) {
+    double2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float2 ld_stream(const float2* p) {
+    float2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "l"(p));
+    return v;
+}
+template <bool STREAM, typename T> __device__ __forceinline__ T ld_cv(const T* p) {
+    if constexpr (STREAM) return ld_stream(p);
+    else return __ldg(p);
+}
+
+template <typename R, bool STREAM>
 __global__ void __launch_bounds__(kWarps * 32)
 k_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, const typename SpVal<R>::T* __restrict__ val,
        const typename SpVal<R>::T* __restrict__ x, typename SpVal<R>::T* __restrict__ y, int64_t rows) {
@@ -183,8 +206,8 @@ k_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, con
             C2 v[4], xv[4];
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                c[q] = __ldg(col + p + 32 * q);
-                v[q] = __ldg(val + p + 32 * q);
+                c[q] = ld_cv<STREAM>(col + p + 32 * q);
+                v[q] = ld_cv<STREAM>(val + p + 32 * q);
             }
 #pragma unroll
             for (int q = 0; q < 4; ++q) xv[q] = __ldg(x + c[q]);
@@ -195,8 +218,8 @@ k_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, con
             }
         }
         for (; p < e; p += 32) {
-            const int c = __ldg(col + p);
-            const C2 v = __ldg(val + p), xv = __ldg(x + c);
+            const int c = ld_cv<STREAM>(col + p);
+            const C2 v = ld_cv<STREAM>(val + p), xv = __ldg(x + c);
             ar += v.x * xv.x - v.y * xv.y;
             ai += v.x * xv.y + v.y * xv.x;
         }
@@ -216,39 +239,30 @@ k_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, con
 
 // Block SpMV for the batched solver: NB right-hand sides interleaved as x[row * NB + r], the
 // operator of right-hand side r is A + u[r] B (u null: val32 for all).  Each entry's NB values
-// are read by NB / RPL lanes, RPL = min(NB, 4) values per lane (16-byte loads), so a warp
-// iteration consumes 32 RPL / NB entries, two iterations in flight.
+// are read by NB / RPL lanes, RPL = min(NB, 4) values per lane (16-byte loads, laid out as
+// blockio.cuh describes), so a warp iteration consumes 32 RPL / NB entries, two iterations in
+// flight.
 template <int NB, bool HAS_B>
 __global__ void __launch_bounds__(kWarps * 32)
 k_block_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, const float2* __restrict__ pa,
              const float2* __restrict__ pb, const float2* __restrict__ x, float2* __restrict__ y,
              const float* __restrict__ u, int64_t rows) {
-    constexpr int RPL = NB < 4 ? NB : 4;
-    constexpr int LPH = NB / RPL;      // lanes per entry
-    constexpr int HPI = 32 / LPH;      // entries per warp iteration
+    using IO = BlkIO<float, NB>;
+    constexpr int RPL = IO::RPL;
+    constexpr int LPH = IO::LPH;       // lanes per entry
+    constexpr int HPI = IO::HPI;       // entries per warp iteration
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int hslot = lane / LPH, r0 = (lane % LPH) * RPL;
+    const int hslot = lane / LPH, kk = lane % LPH;
     float ur[RPL];
 #pragma unroll
-    for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? __ldg(u + r0 + q) : 0.f;
+    for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? __ldg(u + IO::rhs(kk, q)) : 0.f;
     auto entry = [&](int64_t p, float2* acc, float2* accb) {
         const int c = __ldg(col + p);
         const float2 a = __ldg(pa + p);
         float2 b = make_float2(0.f, 0.f);
         if (HAS_B) b = __ldg(pb + p);
         float2 xv[RPL];
-        const float2* xp = x + (int64_t)c * NB + r0;
-        if constexpr (RPL == 4) {
-            const float4 v0 = __ldg(reinterpret_cast<const float4*>(xp));
-            const float4 v1 = __ldg(reinterpret_cast<const float4*>(xp) + 1);
-            xv[0] = make_float2(v0.x, v0.y);
-            xv[1] = make_float2(v0.z, v0.w);
-            xv[2] = make_float2(v1.x, v1.y);
-            xv[3] = make_float2(v1.z, v1.w);
-        } else {
-#pragma unroll
-            for (int q = 0; q < RPL; ++q) xv[q] = __ldg(xp + q);
-        }
+        load_lane<float, NB>(x + (int64_t)c * NB, kk, xv);
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {     // A and B parts apart; B is scaled by u once per row
             acc[q].x += a.x * xv[q].x - a.y * xv[q].y;
@@ -285,16 +299,23 @@ k_block_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ co
                 acc[q].y += __shfl_xor_sync(kFull, acc[q].y, o);
             }
         }
-        if (hslot == 0) {
-#pragma unroll
-            for (int q = 0; q < RPL; ++q) y[row * NB + r0 + q] = acc[q];
-        }
+        if (hslot == 0) store_lane<float, NB>(y + row * NB, kk, acc);
     }
 }
 
 __global__ void k_round_c64(const double2* __restrict__ v, float2* __restrict__ o, int64_t n) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         o[i] = make_float2((float)v[i].x, (float)v[i].y);
+}
+
+// MOMED_SPMV_STREAM=0 reads the column and value arrays through L1 like the x gathers
+bool spmv_stream() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("MOMED_SPMV_STREAM");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
 }
 
 int spmv_grid(int64_t rows) {
@@ -317,6 +338,7 @@ int64_t sparse_bytes_per_entry(bool pair) { return 4 + 16 + 8 + (pair ? 16 : 0);
 void build_sparse(momed_handle* h, double u) {
     SparseMatrix& sp = h->sparse;
     sp.release();
+    h->hcache.release();          // maps read the matrix while it is built
     const int64_t n = h->n;
     cudaStream_t st = h->stream;
     MOMED_REQUIRE(n <= (int64_t)INT32_MAX, MOMED_EINVAL, "sparse method: basis larger than 2^31-1 states");
@@ -420,14 +442,16 @@ void upload_sparse(momed_handle* h, int64_t n, const int64_t* row_ptr, const int
 
 void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
-    k_spmv<double><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val.p, x, y, rows);
+    if (spmv_stream()) k_spmv<double, true><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val.p, x, y, rows);
+    else k_spmv<double, false><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val.p, x, y, rows);
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }
 
 void launch_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
-    k_spmv<float><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val32.p, x, y, rows);
+    if (spmv_stream()) k_spmv<float, true><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val32.p, x, y, rows);
+    else k_spmv<float, false><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val32.p, x, y, rows);
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }

@@ -82,6 +82,10 @@ SIGNATURES = {
     "momed_build_sparse": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "momed_sparse_copy": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_release_sparse": (C.c_int, [C.c_void_p]),
+    "momed_build_hit_cache": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+    "momed_hit_cache_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64), C.POINTER(C.c_double)]),
+    "momed_release_hit_cache": (C.c_int, [C.c_void_p]),
     "momed_set_sparse_csr": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_bracket": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "momed_rdm1": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
@@ -109,7 +113,8 @@ SIGNATURES.update({
 })
 
 (KERNEL_MATVEC_C128, KERNEL_MATVEC_C64, KERNEL_BLOCK_MATVEC_C64, KERNEL_BLOCK_MATVEC_C128, KERNEL_SPMV_C128,
- KERNEL_SPMV_C64, KERNEL_BLOCK_SPMV_C64) = range(7)
+ KERNEL_SPMV_C64, KERNEL_BLOCK_SPMV_C64, KERNEL_HC_MATVEC_C128, KERNEL_HC_MATVEC_C64, KERNEL_HC_BLOCK_C64,
+ KERNEL_HC_BLOCK_C128) = range(11)
 QUEUED, RUNNING, DONE, FAILED, CANCELLED = range(5)
 
 
@@ -433,6 +438,26 @@ class Handle:
     def release_sparse(self):
         self._check(lib().momed_release_sparse(self._h))
         self._sparse_nnz = None
+
+    # ---------------------------------------------------------------- hit cache of the map
+    def build_hit_cache(self) -> dict:
+        """Record every off-diagonal hit's target row and term slot for the working basis and
+        operator, so that maps skip the candidate stage; the eigensolvers build it by themselves
+        when it fits a quarter of the free device memory (MOMED_HITCACHE=0 turns that off)."""
+        hits, nbytes = C.c_int64(), C.c_int64()
+        self._check(lib().momed_build_hit_cache(self._h, C.byref(hits), C.byref(nbytes)))
+        return self.hit_cache_info()
+
+    def hit_cache_info(self):
+        """{"hits", "bytes", "build_ms"} of the built hit cache, or None."""
+        built, hits, nbytes, ms = C.c_int32(), C.c_int64(), C.c_int64(), C.c_double()
+        self._check(lib().momed_hit_cache_info(self._h, C.byref(built), C.byref(hits), C.byref(nbytes), C.byref(ms)))
+        if not built.value:
+            return None
+        return {"hits": hits.value, "bytes": nbytes.value, "build_ms": ms.value}
+
+    def release_hit_cache(self):
+        self._check(lib().momed_release_hit_cache(self._h))
 
     def stats(self):
         nnz, mode, tb = C.c_int64(), C.c_int32(), C.c_int64()
