@@ -83,7 +83,7 @@ def parse():
     ap.add_argument("--serve-meshes", default="3x5,3x9,3x10", help="subset of 3x5,3x9,3x10,4x9")
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-hbm-gb", type=float, default=100.0)
-    ap.add_argument("--serve-policy", default="", help="served arm switches: alone=fp64|mixed,sparse=1|0")
+    ap.add_argument("--serve-policy", default="", help="served arm switches: alone=fp64|mixed,sparse=1|0,hitcache=1|0")
     ap.add_argument("--serve-only", action="store_true", help="only the serving stream (one JSON object)")
     return ap.parse_args()
 
@@ -342,12 +342,15 @@ def serve_bench(args, device: int):
     # plain: one request at a time, FP64 single-vector Lanczos, live against arrivals; once with
     # the matrix-free map and once with the sparse method (the matrix built for each request)
     def run_plain(sparse, block=False):
-        # the plain GPU Lanczos is the reference's algorithm (single-vector Krylov) on the device;
-        # block=True runs the library's default solver (block Lanczos for nev >= 2) one at a time
+        # the plain GPU Lanczos is the reference's algorithm on the device: single-vector Krylov
+        # over the map that evaluates every term at every application (no hit cache);
+        # block=True runs the library's default solver one at a time (over the hit cache)
         if block:
             os.environ.pop("MOMED_BLOCK", None)
+            os.environ.pop("MOMED_HITCACHE", None)
         else:
             os.environ["MOMED_BLOCK"] = "0"
+            os.environ["MOMED_HITCACHE"] = "0"
         vals_, lat_, service_ = [], [], []
         cur = None
         t0 = time.perf_counter()
@@ -371,16 +374,18 @@ def serve_bench(args, device: int):
             lat_.append(s1 - t0 - r["arrival"])
         span = time.perf_counter() - t0
         os.environ.pop("MOMED_BLOCK", None)
+        os.environ.pop("MOMED_HITCACHE", None)
         return vals_, lat_, service_, span
 
     plain_vals, plain_lat, plain_service, plain_span = run_plain(False)
     sp_vals, sp_lat, sp_service, sp_span = run_plain(True)
     bl_vals, bl_lat, bl_service, bl_span = run_plain(False, block=True)
     h.close()
-    # serving policy switches (MOMED_SERVE_ALONE=fp64|mixed, MOMED_SERVE_SPARSE=1|0) for the served arm
+    # serving policy switches (MOMED_SERVE_ALONE=fp64|mixed, MOMED_SERVE_SPARSE=1|0,
+    # MOMED_SERVE_HITCACHE=1|0) for the served arm
     for kv in [x for x in args.serve_policy.split(",") if x]:
         k, v = kv.split("=")
-        os.environ[{"alone": "MOMED_SERVE_ALONE", "sparse": "MOMED_SERVE_SPARSE"}[k]] = v
+        os.environ[{"alone": "MOMED_SERVE_ALONE", "sparse": "MOMED_SERVE_SPARSE", "hitcache": "MOMED_SERVE_HITCACHE"}[k]] = v
 
     def run_server():
         srv = momed.Server(device, slots=args.serve_slots, hbm_budget=int(args.serve_hbm_gb * (1 << 30)))
@@ -427,13 +432,14 @@ def serve_bench(args, device: int):
                    "slowest_solves": [{"mesh": k[0], "nev": v, "device_s": round(k[3], 3), "matvecs": k[2]}
                                       for k, v in slow],
                    "precision": "mixed requests: batched mixed solver for groups on one sector, FP64 "
-                                "single-vector solver for a request alone (sparse method when its "
-                                "matrix fits the budget)",
+                                "single-vector solver for a request alone; maps over the hit cache when "
+                                "it fits the budget, else the sparse method when its matrix fits",
                    "all_converged": bool(all(s_conv)), "max_rel_eig_err_vs_plain_fp64": max(errs)},
         "plain_one_at_a_time": {"solves_per_s": n / plain_span, "latency_ms_p50": 1e3 * pct(plain_lat, 50),
                                 "latency_ms_p99": 1e3 * pct(plain_lat, 99),
                                 "service_ms_p50": 1e3 * pct(plain_service, 50), "precision": "fp64",
-                                "method": "map, single-vector Lanczos"},
+                                "method": "map evaluating every term at every application (no hit cache), "
+                                          "single-vector Lanczos"},
         "plain_sparse_one_at_a_time": {"solves_per_s": n / sp_span, "latency_ms_p50": 1e3 * pct(sp_lat, 50),
                                        "latency_ms_p99": 1e3 * pct(sp_lat, 99),
                                        "service_ms_p50": 1e3 * pct(sp_service, 50), "precision": "fp64",
@@ -444,12 +450,12 @@ def serve_bench(args, device: int):
         "solver_one_at_a_time": {"solves_per_s": n / bl_span, "latency_ms_p50": 1e3 * pct(bl_lat, 50),
                                  "latency_ms_p99": 1e3 * pct(bl_lat, 99),
                                  "service_ms_p50": 1e3 * pct(bl_service, 50), "precision": "fp64",
-                                 "method": "map, the library's default solver (block Lanczos for nev >= 2 on "
-                                           ">= 500000 states)",
+                                 "method": "the library's default solver on the map: single-vector Lanczos "
+                                           "over the hit cache (block Lanczos where no cache fits)",
                                  "max_rel_eig_err_vs_map": max(
                                      float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0)))
                                      for a, b in zip(bl_vals, plain_vals))},
-        "policy": args.serve_policy or "default (alone: fp64, sparse method when it fits)",
+        "policy": args.serve_policy or "default (alone: fp64; hit cache, else sparse method, when it fits)",
         "speedup_served_vs_plain": (n / s_span) / (n / plain_span),
         "speedup_served_vs_plain_sparse": (n / s_span) / (n / sp_span),
     }
@@ -468,9 +474,8 @@ def block_size(nev: int, N: int) -> int:
     if os.environ.get("MOMED_BLOCK"):
         b = int(os.environ["MOMED_BLOCK"])
         return b if b in (4, 8, 16) and N >= 16 * b else 0
-    if os.environ.get("MOMED_HITCACHE", "") != "0":
-        return 0               # over the map's hit cache (built for every bench sector) single-vector wins
-    if nev < 2 or N < 500000:
+    cached = os.environ.get("MOMED_HITCACHE", "") != "0"   # the bench sectors' hit caches all fit
+    if nev < 2 or N < (2000000 if cached else 500000):
         return 0
     return 4 if nev <= 10 else 8
 

@@ -821,10 +821,10 @@ int block_size_for(momed_handle* h, int nev, int precision) {
     // against 165); 3x10 (1.0M, nev 6) 0.487 -> 0.647 with B = 4, 0.527 with B = 8 (mixed 0.34 /
     // 0.50); two-component 4x6 (4.7M, nev 8) 0.063 -> 0.080 with B = 4, 0.067 with B = 8 (mixed
     // 0.040 -> 0.058).  The block map's saving is the candidate stage shared by B vectors; over a
-    // hit cache there is no candidate stage and the single-vector solver wins (3x10: 1.91 against
-    // 1.60 with B = 4).  So: the block solver from 500k states when the map has no hit cache.
-    if (h->hcache.built) return 0;
-    if (nev < 2 || h->n < 500000) return 0;
+    // hit cache there is no candidate stage and the saving is the B-wide gathers only: 3x10 1.93
+    // single-vector against 1.60 with B = 4, two-component 4x6 0.181 against 0.250.  So: the
+    // block solver from 500k states on the candidate map, from 2M states over a hit cache.
+    if (nev < 2 || h->n < (h->hcache.built ? 2000000 : 500000)) return 0;
     if (precision == MOMED_PREC_MIXED) return nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
     return nev <= 10 ? 4 : 8;
 }

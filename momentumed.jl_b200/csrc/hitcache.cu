@@ -167,22 +167,18 @@ template <> __device__ __forceinline__ const double2* hc_diag<double>(const HitC
 template <> __device__ __forceinline__ const float2* hc_diag<float>(const HitCacheView& v) { return v.dg32; }
 
 // hit records are read once per map: not allocated in L1, which stays with the x gathers and the
-// amplitude table (ld.global.nc.L1::no_allocate)
-template <bool STREAM>
+// amplitude table (ld.global.nc.L1::no_allocate; 1-2% faster maps than cached loads)
 __device__ __forceinline__ uint2 ld_hit(const uint2* p) {
-    if constexpr (STREAM) {
-        uint2 v;
-        asm volatile("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
-        return v;
-    } else {
-        return __ldg(p);
-    }
+    uint2 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+    return v;
 }
 
-bool hc_stream() {
+// MOMED_HC_BATCH=0: every lane group loads its own hit record and amplitude (for comparison)
+bool hc_batch() {
     static int on = -1;
     if (on < 0) {
-        const char* e = std::getenv("MOMED_HC_STREAM");
+        const char* e = std::getenv("MOMED_HC_BATCH");
         on = (e && e[0] == '0') ? 0 : 1;
     }
     return on == 1;
@@ -198,25 +194,31 @@ __device__ __forceinline__ C2 signed_amp(const C2* __restrict__ amp, uint32_t tw
 // y = H x over the cache, one right-hand side: a warp per row, lanes stride over its hits four
 // at a time (hit records coalesced, amplitude and x gathers in flight together); the value of a
 // hit is sign * (A + u B) of its term slot, as the candidate map forms it.
-template <typename R, bool HAS_B, bool STREAM>
+// comb[t] = A[t] + u B[t], formed as the candidate map forms a hit's value (same rounding)
+template <typename R>
+__global__ void k_hc_combine(const typename Cx<R>::T* __restrict__ A, const typename Cx<R>::T* __restrict__ B,
+                             const R* __restrict__ u_ptr, typename Cx<R>::T* __restrict__ comb, int64_t n) {
+    const R u = *u_ptr;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        typename Cx<R>::T a = A[t];
+        const typename Cx<R>::T b = B[t];
+        a.x += u * b.x;
+        a.y += u * b.y;
+        comb[t] = a;
+    }
+}
+
+// amp: the term amplitudes at the map's u (A, or A + u B from k_hc_combine); the diagonal sums
+// keep their A and B parts and take u here.
+template <typename R, bool HAS_B>
 __global__ void __launch_bounds__(kWarps * 32)
-k_matvec_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-            const R* __restrict__ u_ptr, int64_t rows) {
+k_matvec_hc(HitCacheView hv, const typename Cx<R>::T* __restrict__ amp, const typename Cx<R>::T* __restrict__ x,
+            typename Cx<R>::T* __restrict__ y, const R* __restrict__ u_ptr, int64_t rows) {
     using C2 = typename Cx<R>::T;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const R u = HAS_B ? *u_ptr : R(0);
-    const C2* __restrict__ A = amp_a<R>(ov);
-    const C2* __restrict__ B = amp_b<R>(ov);
     const C2* __restrict__ dg = hc_diag<R>(hv);
-    auto val = [&](uint32_t tw) {
-        C2 a = signed_amp(A, tw);
-        if (HAS_B) {
-            const C2 b = signed_amp(B, tw);
-            a.x += u * b.x;
-            a.y += u * b.y;
-        }
-        return a;
-    };
+    auto val = [&](uint32_t tw) { return signed_amp(amp, tw); };
     for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
         const int64_t b = __ldg(hv.row_ptr + row), e = __ldg(hv.row_ptr + row + 1);
         R ar = 0, ai = 0;
@@ -225,7 +227,7 @@ k_matvec_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x,
             uint2 h[4];
             C2 v[4], xv[4];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) h[q] = ld_hit<STREAM>(hv.hit + p + 32 * q);
+            for (int q = 0; q < 4; ++q) h[q] = ld_hit(hv.hit + p + 32 * q);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
                 v[q] = val(h[q].y);
@@ -238,7 +240,7 @@ k_matvec_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x,
             }
         }
         for (; p < e; p += 32) {
-            const uint2 h = ld_hit<STREAM>(hv.hit + p);
+            const uint2 h = ld_hit(hv.hit + p);
             const C2 v = val(h.y), xv = __ldg(x + h.x);
             ar += v.x * xv.x - v.y * xv.y;
             ai += v.x * xv.y + v.y * xv.x;
@@ -269,7 +271,10 @@ k_matvec_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x,
 // The three runs of a row are read with their kind fixed at compile time: B-only hits
 // accumulate into a sum scaled by u once per row, A-only hits into the A sum, and hits with
 // both parts form A + u B per right-hand side (the candidate map's three hit rings).
-template <typename R, int NB, bool HAS_B, bool STREAM>
+// BATCH: the warp loads 32 hit records of a run at once (lane l: record l, with its amplitude),
+// the next 32 while it consumes these, and hands each lane group its hit by shuffles, so the
+// record -> amplitude -> x chain of one hit is no longer exposed at every step.
+template <typename R, int NB, bool HAS_B, bool BATCH>
 __global__ void __launch_bounds__(kWarps * 32)
 k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
            const R* __restrict__ u, int64_t rows) {
@@ -288,14 +293,9 @@ k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, 
     // KIND 0: accb += c x (c = B); 1: acc += c x (c = A); 2: acc += (A + u B) x
     auto run = [&](auto kind_tag, int64_t beg, int64_t end, C2* acc, C2* accb) {
         constexpr int KIND = decltype(kind_tag)::value;
-        auto one = [&](int64_t p) {
-            const uint2 h = ld_hit<STREAM>(hv.hit + p);
-            C2 c, cb;
-            if constexpr (KIND == 0) c = signed_amp(B, h.y);
-            else c = signed_amp(A, h.y);
-            if constexpr (KIND == 2) cb = signed_amp(B, h.y);
+        auto fma = [&](uint32_t j, C2 c, C2 cb) {
             C2 xv[RPL];
-            load_lane<R, NB>(x + (int64_t)h.x * NB, kk, xv);
+            load_lane<R, NB>(x + (int64_t)j * NB, kk, xv);
 #pragma unroll
             for (int q = 0; q < RPL; ++q) {
                 R cx = c.x, cy = c.y;
@@ -308,12 +308,53 @@ k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, 
                 a[q].y += cx * xv[q].y + cy * xv[q].x;
             }
         };
-        int64_t p = beg + hslot;
-        for (; p + HPI < end; p += 2 * HPI) {
-            one(p);
-            one(p + HPI);
+        // the hit at p: target and signed amplitude(s) of its kind
+        auto fetch = [&](int64_t p, uint32_t& j, C2& c, C2& cb) {
+            const uint2 h = ld_hit(hv.hit + p);
+            j = h.x;
+            if constexpr (KIND == 0) c = signed_amp(B, h.y);
+            else c = signed_amp(A, h.y);
+            if constexpr (KIND == 2) cb = signed_amp(B, h.y);
+        };
+        if constexpr (!BATCH) {
+            auto one = [&](int64_t p) {
+                uint32_t j;
+                C2 c, cb;
+                fetch(p, j, c, cb);
+                fma(j, c, cb);
+            };
+            int64_t p = beg + hslot;
+            for (; p + HPI < end; p += 2 * HPI) {
+                one(p);
+                one(p + HPI);
+            }
+            if (p < end) one(p);
+        } else {
+            if (beg >= end) return;
+            uint32_t jn = 0;
+            C2 cn, cbn;
+            cn.x = cn.y = cbn.x = cbn.y = R(0);
+            if (beg + lane < end) fetch(beg + lane, jn, cn, cbn);
+            for (int64_t b0 = beg; b0 < end; b0 += 32) {
+                const uint32_t jv = jn;
+                const C2 cv = cn, cbv = cbn;
+                if (b0 + 32 + lane < end) fetch(b0 + 32 + lane, jn, cn, cbn);   // the next 32, in flight
+                const int nb = (int)((end - b0) < 32 ? (end - b0) : 32);
+#pragma unroll 2
+                for (int k = 0; k < nb; k += HPI) {
+                    const int src = k + hslot;
+                    const uint32_t j = __shfl_sync(kFull, jv, src);
+                    C2 c, cb;
+                    c.x = __shfl_sync(kFull, cv.x, src);
+                    c.y = __shfl_sync(kFull, cv.y, src);
+                    if constexpr (KIND == 2) {
+                        cb.x = __shfl_sync(kFull, cbv.x, src);
+                        cb.y = __shfl_sync(kFull, cbv.y, src);
+                    }
+                    if (src < nb) fma(j, c, cb);
+                }
+            }
         }
-        if (p < end) one(p);
     };
 
     for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
@@ -366,6 +407,13 @@ k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, 
 
 template <typename K>
 int hc_grid(K kernel, int64_t rows) { return persistent_grid(kernel, rows); }
+
+template <typename R> const typename Cx<R>::T* amp_a_host(const OpView& ov);
+template <> const double2* amp_a_host<double>(const OpView& ov) { return ov.t_amp; }
+template <> const float2* amp_a_host<float>(const OpView& ov) { return ov.t_amp32; }
+template <typename R> const typename Cx<R>::T* amp_b_host(const OpView& ov);
+template <> const double2* amp_b_host<double>(const OpView& ov) { return ov.t_ampb; }
+template <> const float2* amp_b_host<float>(const OpView& ov) { return ov.t_ampb32; }
 
 }  // namespace
 
@@ -459,29 +507,57 @@ void ensure_hit_cache(momed_handle* h) {
     if (!h->hcache.built && hit_cache_wanted(h)) build_hit_cache(h);
 }
 
+template <typename R> struct CombSlot;
+template <> struct CombSlot<double> {
+    static DevBuf<double2>& buf(HitCache& c) { return c.comb64; }
+    static double& u(HitCache& c) { return c.comb_u64; }
+    static bool& ok(HitCache& c) { return c.comb_ok64; }
+};
+template <> struct CombSlot<float> {
+    static DevBuf<float2>& buf(HitCache& c) { return c.comb32; }
+    static double& u(HitCache& c) { return c.comb_u32; }
+    static bool& ok(HitCache& c) { return c.comb_ok32; }
+};
+
+// u is the handle's parameter on the device (h->u_dev / u_dev32): the combined amplitudes are
+// formed again whenever the handle's u differs from the one they were formed at.
 template <typename R>
-static void matvec_hc_dispatch(const momed_handle* h, const typename Cx<R>::T* x, typename Cx<R>::T* y, const R* u,
+static void matvec_hc_dispatch(momed_handle* h, const typename Cx<R>::T* x, typename Cx<R>::T* y, const R* u,
                                int64_t rows, cudaStream_t st) {
+    using C2 = typename Cx<R>::T;
     if (rows <= 0) return;
     const HitCacheView hv = h->hcache.view();
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
-    const bool sm = hc_stream();
-    auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, ov, x, y, up, rows); };
-    if (hb && sm) go(k_matvec_hc<R, true, true>, u);
-    else if (hb) go(k_matvec_hc<R, true, false>, u);
-    else if (sm) go(k_matvec_hc<R, false, true>, nullptr);
-    else go(k_matvec_hc<R, false, false>, nullptr);
+    const C2* amp = amp_a_host<R>(ov);
+    if (hb) {
+        HitCache& hc = h->hcache;
+        auto& cb = CombSlot<R>::buf(hc);
+        if (!CombSlot<R>::ok(hc) || CombSlot<R>::u(hc) != h->u) {
+            const int64_t n = ov.nterms;
+            cb.resize(std::max<int64_t>(n, 1));
+            const int g = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 1184));
+            k_hc_combine<R><<<g, 256, 0, st>>>(amp, amp_b_host<R>(ov), u, cb.p, n);
+            MOMED_CUDA_TRY(cudaGetLastError());
+            note_launches(1);
+            CombSlot<R>::u(hc) = h->u;
+            CombSlot<R>::ok(hc) = true;
+        }
+        amp = cb.p;
+    }
+    auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, amp, x, y, up, rows); };
+    if (hb) go(k_matvec_hc<R, true>, u);
+    else go(k_matvec_hc<R, false>, nullptr);
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }
 
-void launch_matvec_hc_c128(const momed_handle* h, const double2* x, double2* y, const double* u, int64_t rows,
+void launch_matvec_hc_c128(momed_handle* h, const double2* x, double2* y, const double* u, int64_t rows,
                            cudaStream_t st) {
     matvec_hc_dispatch<double>(h, x, y, u, rows, st);
 }
 
-void launch_matvec_hc_c64(const momed_handle* h, const float2* x, float2* y, const float* u, int64_t rows,
+void launch_matvec_hc_c64(momed_handle* h, const float2* x, float2* y, const float* u, int64_t rows,
                           cudaStream_t st) {
     matvec_hc_dispatch<float>(h, x, y, u, rows, st);
 }
@@ -493,7 +569,7 @@ static void block_hc_dispatch(const momed_handle* h, const typename Cx<R>::T* x,
     const HitCacheView hv = h->hcache.view();
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
-    const bool sm = hc_stream();
+    const bool sm = hc_batch();
     auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, ov, x, y, up, rows); };
 #define MOMED_BHC(NBV)                                                                        \
     case NBV:                                                                                 \

@@ -224,10 +224,18 @@ struct HitCache {
     DevBuf<uint2> hit;
     DevBuf<double2> dg64;
     DevBuf<float2> dg32;
+    // A + u B per term slot at the u of the single-vector map (one amplitude load per hit)
+    DevBuf<double2> comb64;
+    DevBuf<float2> comb32;
+    double comb_u64 = 0.0, comb_u32 = 0.0;
+    bool comb_ok64 = false, comb_ok32 = false;
     HitCacheView view() const;
     void release() {
         built = false;
         nnz = bytes = 0;
+        comb64.release();
+        comb32.release();
+        comb_ok64 = comb_ok32 = false;
         row_ptr.release();
         seg.release();
         hit.release();
@@ -308,9 +316,9 @@ int64_t hit_cache_bytes(int64_t n, int64_t hits);
 bool hit_cache_wanted(const momed_handle* h);
 void build_hit_cache(momed_handle* h);
 void ensure_hit_cache(momed_handle* h);
-void launch_matvec_hc_c128(const momed_handle* h, const double2* x, double2* y, const double* u, int64_t rows,
+void launch_matvec_hc_c128(momed_handle* h, const double2* x, double2* y, const double* u, int64_t rows,
                            cudaStream_t st);
-void launch_matvec_hc_c64(const momed_handle* h, const float2* x, float2* y, const float* u, int64_t rows,
+void launch_matvec_hc_c64(momed_handle* h, const float2* x, float2* y, const float* u, int64_t rows,
                           cudaStream_t st);
 void launch_block_hc_c64(const momed_handle* h, const float2* x, float2* y, const float* u, int32_t nb, int64_t rows,
                          cudaStream_t st);

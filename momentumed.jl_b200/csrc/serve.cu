@@ -256,6 +256,7 @@ void worker_loop(momed_server* S, int slot) {
             h->basis.resize(std::max<int64_t>(N, 1));
             MOMED_CUDA_TRY(cudaMemcpyAsync(h->basis.p, r->basis.data(), N * 8, cudaMemcpyHostToDevice, h->stream));
             h->n = N;
+            h->hcache.release();
             h->index_dirty = true;
             h->op_validated = false;
             h->basis_or = 0;
@@ -277,28 +278,48 @@ void worker_loop(momed_server* S, int slot) {
                 MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(uf), cudaMemcpyHostToDevice, h->stream));
                 MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));
             }
-            // the sparse method when its matrix fits what the budget has left (its bytes are held
-            // for this solve only); a group's batched solver then runs its FP32 maps as a block SpMV
-            int64_t sp_bytes = 0;
-            if (N >= kSparseMinRows && knob("MOMED_SERVE_SPARSE", "1") != "0") {
+            // The map's hit cache when it fits what the budget has left, else the sparse method
+            // when its matrix fits (their bytes are held for this solve only); otherwise the
+            // candidate map.  A group's batched solver runs its FP32 maps over the cache (or as a
+            // block SpMV over the matrix).  MOMED_SERVE_HITCACHE=0 / MOMED_SERVE_SPARSE=0 skip one.
+            int64_t sp_bytes = 0, hc_bytes = 0;
+            if (N >= kSparseMinRows) {
                 ensure_ready(h);                      // index and validation: h->nnz counts every hit
-                const int64_t need = (N + 1) * 8 + (h->nnz + N) * sparse_bytes_per_entry(h->op.has_b);
                 std::lock_guard<std::mutex> lk(S->mu);
                 S->op_hits_per_row[r->op] = (double)h->nnz / (double)N;
-                if (S->used + need <= S->budget) {
-                    S->used += need;
-                    sp_bytes = need;
+                if (knob("MOMED_SERVE_HITCACHE", "1") != "0") {
+                    const int64_t need = hit_cache_bytes(N, h->nnz);
+                    if (S->used + need <= S->budget) {
+                        S->used += need;
+                        hc_bytes = need;
+                    }
+                }
+                if (hc_bytes == 0 && knob("MOMED_SERVE_SPARSE", "1") != "0") {
+                    const int64_t need = (N + 1) * 8 + (h->nnz + N) * sparse_bytes_per_entry(h->op.has_b);
+                    if (S->used + need <= S->budget) {
+                        S->used += need;
+                        sp_bytes = need;
+                    }
                 }
             }
             auto unreserve = [&]() {
                 h->sparse.release();
-                if (sp_bytes > 0) {
+                h->hcache.release();
+                if (sp_bytes > 0 || hc_bytes > 0) {
                     std::lock_guard<std::mutex> lk(S->mu);
-                    S->used -= sp_bytes;
-                    sp_bytes = 0;
+                    S->used -= sp_bytes + hc_bytes;
+                    sp_bytes = hc_bytes = 0;
                 }
             };
             try {
+                if (hc_bytes > 0) {
+                    try {
+                        build_hit_cache(h);
+                    } catch (const Error& e) {
+                        if (e.code != MOMED_ENOMEM) throw;
+                        unreserve();          // the device is shorter than the budget: candidate map
+                    }
+                }
                 if (sp_bytes > 0) {
                     try {
                         build_sparse(h, u);

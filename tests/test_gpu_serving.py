@@ -6,6 +6,7 @@ practice), and they match the one-at-a-time solver within 1e-10 relative.  Failu
 are exercised on the host: over-budget refusal, cancellation of a queued request, bounded
 polls.  Nothing here faults, traps or hangs the GPU.
 """
+import os
 import time
 
 import numpy as np
@@ -194,16 +195,27 @@ def test_queued_requests_on_one_sector_are_batched(workload):
 
 
 def test_sparse_method_and_map_fallback_by_budget(workload):
-    """A 3x8 request (~30k states) is solved on the sparse method when its matrix fits the budget
-    and on the matrix-free map when only the Krylov state fits: the same eigenvalues either way."""
+    """A 3x8 request (~30k states) is solved over the map's hit cache when it fits the budget, on
+    the sparse method when the cache is switched off and the matrix fits, and on the candidate map
+    when only the Krylov state fits: the same eigenvalues every way."""
     p35, p38, b35, b38 = workload
     vals = {}
-    for budget in (8 << 30, 96 << 20):           # room for the matrix / for the solve only
-        srv = _lib.Server(0, slots=1, hbm_budget=budget)
-        op = srv.register_operator(*p38)
-        rid = srv.submit(op, b38[1], 1.1, 4, tol=1e-12, seed=5)
-        vals[budget] = wait_all(srv, [rid], {rid: 4})[rid][0]
-        assert srv.stats()["failed"] == 0
-        srv.stop()
-    a, b = vals[8 << 30], vals[96 << 20]
-    assert np.max(np.abs(a - b) / np.abs(b)) < 1e-10
+    for budget, knobs in ((8 << 30, {}), (8 << 30, {"MOMED_SERVE_HITCACHE": "0"}), (96 << 20, {})):
+        old = {k: os.environ.get(k) for k in knobs}
+        os.environ.update(knobs)
+        try:
+            srv = _lib.Server(0, slots=1, hbm_budget=budget)
+            op = srv.register_operator(*p38)
+            rid = srv.submit(op, b38[1], 1.1, 4, tol=1e-12, seed=5)
+            vals[(budget, tuple(knobs))] = wait_all(srv, [rid], {rid: 4})[rid][0]
+            assert srv.stats()["failed"] == 0
+            srv.stop()
+        finally:
+            for k, v in old.items():
+                if v is None:
+                    del os.environ[k]
+                else:
+                    os.environ[k] = v
+    ref = vals[(96 << 20, ())]
+    for v in vals.values():
+        assert np.max(np.abs(v - ref) / np.abs(ref)) < 1e-10
