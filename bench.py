@@ -83,7 +83,7 @@ def parse():
     ap.add_argument("--serve-meshes", default="3x5,3x9,3x10", help="subset of 3x5,3x9,3x10,4x9")
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-hbm-gb", type=float, default=100.0)
-    ap.add_argument("--serve-policy", default="", help="served arm switches: alone=fp64|mixed,sparse=1|0,hitcache=1|0")
+    ap.add_argument("--serve-policy", default="", help="served arm switches: alone=fp64|mixed,sparse=1|0,hitcache=1|0,large=<concurrent large solves>")
     ap.add_argument("--serve-only", action="store_true", help="only the serving stream (one JSON object)")
     return ap.parse_args()
 
@@ -385,7 +385,8 @@ def serve_bench(args, device: int):
     # MOMED_SERVE_HITCACHE=1|0) for the served arm
     for kv in [x for x in args.serve_policy.split(",") if x]:
         k, v = kv.split("=")
-        os.environ[{"alone": "MOMED_SERVE_ALONE", "sparse": "MOMED_SERVE_SPARSE", "hitcache": "MOMED_SERVE_HITCACHE"}[k]] = v
+        os.environ[{"alone": "MOMED_SERVE_ALONE", "sparse": "MOMED_SERVE_SPARSE", "hitcache": "MOMED_SERVE_HITCACHE",
+                    "large": "MOMED_SERVE_LARGE_MAX"}[k]] = v
 
     def run_server():
         srv = momed.Server(device, slots=args.serve_slots, hbm_budget=int(args.serve_hbm_gb * (1 << 30)))
@@ -475,7 +476,7 @@ def block_size(nev: int, N: int) -> int:
         b = int(os.environ["MOMED_BLOCK"])
         return b if b in (4, 8, 16) and N >= 16 * b else 0
     cached = os.environ.get("MOMED_HITCACHE", "") != "0"   # the bench sectors' hit caches all fit
-    if nev < 2 or N < (2000000 if cached else 500000):
+    if nev < 6 or N < (2000000 if cached else 500000):
         return 0
     return 4 if nev <= 10 else 8
 

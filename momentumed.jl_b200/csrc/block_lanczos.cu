@@ -820,11 +820,13 @@ int block_size_for(momed_handle* h, int nev, int precision) {
     // map: 3x9 (174k states, nev 4) 6.69 -> 4.35 with B = 4 (the block needs 2.8x the maps: 464
     // against 165); 3x10 (1.0M, nev 6) 0.487 -> 0.647 with B = 4, 0.527 with B = 8 (mixed 0.34 /
     // 0.50); two-component 4x6 (4.7M, nev 8) 0.063 -> 0.080 with B = 4, 0.067 with B = 8 (mixed
-    // 0.040 -> 0.058).  The block map's saving is the candidate stage shared by B vectors; over a
-    // hit cache there is no candidate stage and the saving is the B-wide gathers only: 3x10 1.93
+    // 0.040 -> 0.058); 4x9 Ne = 12 (34.8M, nev 4) 69.9 s -> 108.7 s with B = 4 (560 maps against
+    // 209).  With few wanted pairs per block vector the block Krylov space needs too many more
+    // vectors.  The block map's saving is the candidate stage shared by B vectors; over a hit
+    // cache there is no candidate stage and the saving is the B-wide gathers only: 3x10 1.93
     // single-vector against 1.60 with B = 4, two-component 4x6 0.181 against 0.250.  So: the
-    // block solver from 500k states on the candidate map, from 2M states over a hit cache.
-    if (nev < 2 || h->n < (h->hcache.built ? 2000000 : 500000)) return 0;
+    // block solver for nev >= 6, from 500k states on the candidate map, from 2M over a hit cache.
+    if (nev < 6 || h->n < (h->hcache.built ? 2000000 : 500000)) return 0;
     if (precision == MOMED_PREC_MIXED) return nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
     return nev <= 10 ? 4 : 8;
 }

@@ -174,15 +174,7 @@ __device__ __forceinline__ uint2 ld_hit(const uint2* p) {
     return v;
 }
 
-// MOMED_HC_BATCH=0: every lane group loads its own hit record and amplitude (for comparison)
-bool hc_batch() {
-    static int on = -1;
-    if (on < 0) {
-        const char* e = std::getenv("MOMED_HC_BATCH");
-        on = (e && e[0] == '0') ? 0 : 1;
-    }
-    return on == 1;
-}
+
 
 template <typename C2>
 __device__ __forceinline__ C2 signed_amp(const C2* __restrict__ amp, uint32_t tw) {
@@ -271,10 +263,11 @@ k_matvec_hc(HitCacheView hv, const typename Cx<R>::T* __restrict__ amp, const ty
 // The three runs of a row are read with their kind fixed at compile time: B-only hits
 // accumulate into a sum scaled by u once per row, A-only hits into the A sum, and hits with
 // both parts form A + u B per right-hand side (the candidate map's three hit rings).
-// BATCH: the warp loads 32 hit records of a run at once (lane l: record l, with its amplitude),
-// the next 32 while it consumes these, and hands each lane group its hit by shuffles, so the
-// record -> amplitude -> x chain of one hit is no longer exposed at every step.
-template <typename R, int NB, bool HAS_B, bool BATCH>
+// Each lane group loads its own hit record and amplitude, two hits in flight per lane.  Loading
+// 32 records per warp at once (the next 32 in flight) and handing them out by shuffles was
+// measured slower (0.84 against 0.70 ms per launch on the headline sector: more registers, the
+// shuffles on the issue path).
+template <typename R, int NB, bool HAS_B>
 __global__ void __launch_bounds__(kWarps * 32)
 k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
            const R* __restrict__ u, int64_t rows) {
@@ -316,45 +309,18 @@ k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, 
             else c = signed_amp(A, h.y);
             if constexpr (KIND == 2) cb = signed_amp(B, h.y);
         };
-        if constexpr (!BATCH) {
-            auto one = [&](int64_t p) {
-                uint32_t j;
-                C2 c, cb;
-                fetch(p, j, c, cb);
-                fma(j, c, cb);
-            };
-            int64_t p = beg + hslot;
-            for (; p + HPI < end; p += 2 * HPI) {
-                one(p);
-                one(p + HPI);
-            }
-            if (p < end) one(p);
-        } else {
-            if (beg >= end) return;
-            uint32_t jn = 0;
-            C2 cn, cbn;
-            cn.x = cn.y = cbn.x = cbn.y = R(0);
-            if (beg + lane < end) fetch(beg + lane, jn, cn, cbn);
-            for (int64_t b0 = beg; b0 < end; b0 += 32) {
-                const uint32_t jv = jn;
-                const C2 cv = cn, cbv = cbn;
-                if (b0 + 32 + lane < end) fetch(b0 + 32 + lane, jn, cn, cbn);   // the next 32, in flight
-                const int nb = (int)((end - b0) < 32 ? (end - b0) : 32);
-#pragma unroll 2
-                for (int k = 0; k < nb; k += HPI) {
-                    const int src = k + hslot;
-                    const uint32_t j = __shfl_sync(kFull, jv, src);
-                    C2 c, cb;
-                    c.x = __shfl_sync(kFull, cv.x, src);
-                    c.y = __shfl_sync(kFull, cv.y, src);
-                    if constexpr (KIND == 2) {
-                        cb.x = __shfl_sync(kFull, cbv.x, src);
-                        cb.y = __shfl_sync(kFull, cbv.y, src);
-                    }
-                    if (src < nb) fma(j, c, cb);
-                }
-            }
+        auto one = [&](int64_t p) {
+            uint32_t j;
+            C2 c, cb;
+            fetch(p, j, c, cb);
+            fma(j, c, cb);
+        };
+        int64_t p = beg + hslot;
+        for (; p + HPI < end; p += 2 * HPI) {
+            one(p);
+            one(p + HPI);
         }
+        if (p < end) one(p);
     };
 
     for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
@@ -569,14 +535,11 @@ static void block_hc_dispatch(const momed_handle* h, const typename Cx<R>::T* x,
     const HitCacheView hv = h->hcache.view();
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
-    const bool sm = hc_batch();
     auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, ov, x, y, up, rows); };
 #define MOMED_BHC(NBV)                                                                        \
     case NBV:                                                                                 \
-        if (hb && sm) go(k_block_hc<R, NBV, true, true>, u);                                  \
-        else if (hb) go(k_block_hc<R, NBV, true, false>, u);                                  \
-        else if (sm) go(k_block_hc<R, NBV, false, true>, nullptr);                            \
-        else go(k_block_hc<R, NBV, false, false>, nullptr);                                   \
+        if (hb) go(k_block_hc<R, NBV, true>, u);                                              \
+        else go(k_block_hc<R, NBV, false>, nullptr);                                          \
         break;
     switch (nb) {
         MOMED_BHC(1)

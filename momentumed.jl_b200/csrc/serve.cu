@@ -87,7 +87,8 @@ namespace {
 
 // A solve of at least this many states keeps the GPU (and its L2, which holds the map's input
 // vector and index tables) busy on its own; two at once only evict each other's working sets.
-// Such requests run one at a time; smaller ones still overlap with them and with each other.
+// Such requests run one at a time (MOMED_SERVE_LARGE_MAX raises that count); smaller ones still
+// overlap with them and with each other.
 constexpr int64_t kLargeRows = 1 << 17;
 // Smallest group that the batched solver serves faster per request than the single-vector solver.
 constexpr int kMinGroup = 3;
@@ -177,9 +178,10 @@ void worker_loop(momed_server* S, int slot) {
             std::deque<std::shared_ptr<Request>>::iterator pick;
             auto find = [&]() {
                 while (!S->queue.empty() && S->queue.front()->status == 4) S->queue.pop_front();
+                const int large_max = std::max(1, std::atoi(knob("MOMED_SERVE_LARGE_MAX", "1").c_str()));
                 for (auto it = S->queue.begin(); it != S->queue.end(); ++it) {
                     if ((*it)->status == 4) continue;
-                    if ((int64_t)(*it)->basis.size() >= kLargeRows && S->large_running > 0) continue;
+                    if ((int64_t)(*it)->basis.size() >= kLargeRows && S->large_running >= large_max) continue;
                     if (S->used + (*it)->bytes > S->budget) return false;
                     pick = it;
                     return true;

@@ -465,11 +465,17 @@ void launch_block_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, c
     if (rows <= 0) return;
     const bool hb = u != nullptr && sp.pb32.p != nullptr;
     const float2* pa = hb ? sp.pa32.p : sp.val32.p;
-    const int g = spmv_grid(rows);
+    // grid = the CTAs that are resident at once (the wide variants hold up to 70 registers, 3 CTAs
+    // per SM): a grid-strided launch larger than that runs its surplus CTAs as a partial wave
 #define MOMED_BSP(NBV)                                                                                   \
     case NBV:                                                                                            \
-        if (hb) k_block_spmv<NBV, true><<<g, kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, pa, sp.pb32.p, x, y, u, rows); \
-        else k_block_spmv<NBV, false><<<g, kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, pa, nullptr, x, y, nullptr, rows); \
+        if (hb) {                                                                                        \
+            auto k = k_block_spmv<NBV, true>;                                                            \
+            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, pa, sp.pb32.p, x, y, u, rows); \
+        } else {                                                                                         \
+            auto k = k_block_spmv<NBV, false>;                                                           \
+            k<<<persistent_grid(k, rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, pa, nullptr, x, y, nullptr, rows); \
+        }                                                                                                \
         break;
     switch (nb) {
         MOMED_BSP(1)
