@@ -955,6 +955,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
     const int maxiter = o->maxiter > 0 ? o->maxiter : 100;
     cudaStream_t st = h->stream;
     std::vector<double> uv(u, u + nu);
+    const double u_handle = h->u;
     MOMED_CUDA_TRY(cudaEventRecord(h->ev0, st));
     int64_t matvecs = 0, matvecs64 = 0;
     int restarts = 0;
@@ -1429,8 +1430,10 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
             while (conv < nev && (conv < nconv3[q] || rq[conv] <= tol)) ++conv;
         } else if (!okv[q]) {
             // invariant Krylov space: this parameter is solved on its own by the single-vector solver
+            // (at its u: the handle's u, host and device, is put back below)
             double uq = uv[q];
             float uf = (float)uq;
+            h->u = uq;
             MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &uq, sizeof(double), cudaMemcpyHostToDevice, st));
             MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(float), cudaMemcpyHostToDevice, st));
             momed_solve_opts o2 = *o;
@@ -1451,13 +1454,14 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
         }
         if (vecs)
             MOMED_CUDA_TRY(cudaMemcpyAsync(vecs + (size_t)q * nev * N * 2, X1.p, (size_t)nev * N * sizeof(double2),
-                                           cudaMemcpyDeviceToHost, st));
+                                           o->vecs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
         MOMED_CUDA_TRY(cudaStreamSynchronize(st));
     }
-    double one = 1.0;
-    float onef = 1.0f;
-    MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &one, sizeof(double), cudaMemcpyHostToDevice, st));
-    MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &onef, sizeof(float), cudaMemcpyHostToDevice, st));
+    // the handle's own u (momed_set_param) again on the device
+    h->u = u_handle;
+    const float u32 = (float)u_handle;
+    MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u_handle, sizeof(double), cudaMemcpyHostToDevice, st));
+    MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &u32, sizeof(float), cudaMemcpyHostToDevice, st));
     MOMED_CUDA_TRY(cudaEventRecord(h->ev1, st));
     MOMED_CUDA_TRY(cudaStreamSynchronize(st));
     float ms = 0.f;

@@ -826,8 +826,11 @@ int block_size_for(momed_handle* h, int nev, int precision) {
     // cache there is no candidate stage and the saving is the B-wide gathers only: 3x10 1.93
     // single-vector against 1.60 with B = 4, two-component 4x6 0.181 against 0.250.  So: the
     // block solver for nev >= 6, from 500k states on the candidate map, from 2M over a hit cache.
+    // Mixed precision goes to the batched solver with one right-hand side instead (its anchored
+    // FP64 refinement): two-component 4x6, nev 8: 2.73 s against 7.56 s for the mixed block solver
+    // (whose FP64 phase restarts from B of the refined vectors) and 4.2 s for the FP64 one.
     if (nev < 6 || h->n < (h->hcache.built ? 2000000 : 500000)) return 0;
-    if (precision == MOMED_PREC_MIXED) return nev <= 4 ? 4 : (nev <= 10 ? 8 : 16);
+    if (precision == MOMED_PREC_MIXED) return h->sparse.built ? (nev <= 10 ? 8 : 16) : 0;
     return nev <= 10 ? 4 : 8;
 }
 

@@ -176,6 +176,16 @@ __device__ __forceinline__ uint2 ld_hit(const uint2* p) {
 
 
 
+// MOMED_HC_PF=0: the block map loads each pair of hit records right before using them
+bool hc_prefetch() {
+    static int on = -1;
+    if (on < 0) {
+        const char* e = std::getenv("MOMED_HC_PF");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on == 1;
+}
+
 template <typename C2>
 __device__ __forceinline__ C2 signed_amp(const C2* __restrict__ amp, uint32_t tw) {
     C2 a = __ldg(amp + (tw & 0x7fffffffu));
@@ -267,7 +277,9 @@ k_matvec_hc(HitCacheView hv, const typename Cx<R>::T* __restrict__ amp, const ty
 // 32 records per warp at once (the next 32 in flight) and handing them out by shuffles was
 // measured slower (0.84 against 0.70 ms per launch on the headline sector: more registers, the
 // shuffles on the issue path).
-template <typename R, int NB, bool HAS_B>
+// PF: the hit records of a lane group's next two hits are loaded before the current two are
+// consumed (their stream comes from HBM; the x rows, from L2, then wait on one latency only).
+template <typename R, int NB, bool HAS_B, bool PF>
 __global__ void __launch_bounds__(kWarps * 32)
 k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
            const R* __restrict__ u, int64_t rows) {
@@ -301,26 +313,42 @@ k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, 
                 a[q].y += cx * xv[q].y + cy * xv[q].x;
             }
         };
-        // the hit at p: target and signed amplitude(s) of its kind
-        auto fetch = [&](int64_t p, uint32_t& j, C2& c, C2& cb) {
-            const uint2 h = ld_hit(hv.hit + p);
-            j = h.x;
+        // the hit with record h: target and signed amplitude(s) of its kind
+        auto use = [&](uint2 h) {
+            C2 c, cb;
             if constexpr (KIND == 0) c = signed_amp(B, h.y);
             else c = signed_amp(A, h.y);
             if constexpr (KIND == 2) cb = signed_amp(B, h.y);
-        };
-        auto one = [&](int64_t p) {
-            uint32_t j;
-            C2 c, cb;
-            fetch(p, j, c, cb);
-            fma(j, c, cb);
+            fma(h.x, c, cb);
         };
         int64_t p = beg + hslot;
-        for (; p + HPI < end; p += 2 * HPI) {
-            one(p);
-            one(p + HPI);
+        if constexpr (PF) {
+            if (p + HPI < end) {
+                uint2 h0 = ld_hit(hv.hit + p), h1 = ld_hit(hv.hit + p + HPI);
+                for (;;) {
+                    const int64_t pn = p + 2 * HPI;
+                    const bool more = pn + HPI < end;
+                    uint2 n0 = h0, n1 = h1;
+                    if (more) {
+                        n0 = ld_hit(hv.hit + pn);
+                        n1 = ld_hit(hv.hit + pn + HPI);
+                    }
+                    use(h0);
+                    use(h1);
+                    p = pn;
+                    if (!more) break;
+                    h0 = n0;
+                    h1 = n1;
+                }
+            }
+        } else {
+            for (; p + HPI < end; p += 2 * HPI) {
+                const uint2 h0 = ld_hit(hv.hit + p), h1 = ld_hit(hv.hit + p + HPI);
+                use(h0);
+                use(h1);
+            }
         }
-        if (p < end) one(p);
+        if (p < end) use(ld_hit(hv.hit + p));
     };
 
     for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
@@ -535,11 +563,14 @@ static void block_hc_dispatch(const momed_handle* h, const typename Cx<R>::T* x,
     const HitCacheView hv = h->hcache.view();
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
+    const bool pf = hc_prefetch();
     auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, ov, x, y, up, rows); };
 #define MOMED_BHC(NBV)                                                                        \
     case NBV:                                                                                 \
-        if (hb) go(k_block_hc<R, NBV, true>, u);                                              \
-        else go(k_block_hc<R, NBV, false>, nullptr);                                          \
+        if (hb && pf) go(k_block_hc<R, NBV, true, true>, u);                                  \
+        else if (hb) go(k_block_hc<R, NBV, true, false>, u);                                  \
+        else if (pf) go(k_block_hc<R, NBV, false, true>, nullptr);                            \
+        else go(k_block_hc<R, NBV, false, false>, nullptr);                                   \
         break;
     switch (nb) {
         MOMED_BHC(1)

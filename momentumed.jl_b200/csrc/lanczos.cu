@@ -432,6 +432,24 @@ int momed_eigsolve_impl(momed_handle* h, const momed_solve_opts* o, const double
     const int B = block_size_for(h, nev, o->precision);
     const bool blocked = B > 0 && eigsolve_block(h, o, nev, B, vec0 ? start64.p : nullptr, X.p, theta, res, nconv,
                                                  restarts, matvecs, matvecs64);
+    // mixed precision on the map without a start vector: the batched solver with one right-hand
+    // side at the handle's u (FP32 Lanczos, then its anchored FP64 refinement of the Ritz block,
+    // which a single-vector FP64 restart from one combined vector cannot match); it returns exact
+    // FP64 residuals and the vectors on the device
+    const char* mb_env = std::getenv("MOMED_MIXED_BATCHED");
+    if (!blocked && o->precision == MOMED_PREC_MIXED && !vec0 && !h->sparse.built && !(mb_env && mb_env[0] == '0')) {
+        momed_solve_opts o2 = *o;
+        o2.want_vectors = 1;
+        o2.vecs_on_device = 1;
+        const double u = h->u;
+        const int rc = momed_batch_solve_impl(h, &o2, &u, 1, vals, resid, reinterpret_cast<double*>(X.p), info);
+        if (vecs && o->want_vectors) {
+            cudaMemcpyKind kind = o->vecs_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+            MOMED_CUDA_TRY(cudaMemcpyAsync(vecs, X.p, (size_t)nev * N * sizeof(double2), kind, st));
+            MOMED_CUDA_TRY(cudaStreamSynchronize(st));
+        }
+        return rc;
+    }
     if (blocked) {
     } else if (o->precision == MOMED_PREC_MIXED) {
         // phase 1: FP32 Lanczos to the FP32 floor

@@ -98,24 +98,24 @@ def test_block_matches_single_vector_3x8(h):
 
 
 def test_block_is_default_for_large_sectors_without_hit_cache(h):
-    """nev >= 2 on >= 500k states takes the block solver when the map has no hit cache: its maps
-    are block-map launches.  Over a hit cache the single-vector solver runs."""
+    """nev >= 6 on >= 500k states takes the block solver when the map has no hit cache: its maps
+    are block-map launches.  Over a hit cache (below 2M states) the single-vector solver runs."""
     setup(h, 3, 10, 1, (10,), 3)
     assert h.n >= 500000
     with env(MOMED_HITCACHE=0):
         h.profile(True)
-        vals, _, resid, info = h.eigsolve(4, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
+        vals, _, resid, info = h.eigsolve(6, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
         nblk, _ = h.profile_read(_lib.KERNEL_BLOCK_MATVEC_C128)
         nsingle, _ = h.profile_read(_lib.KERNEL_MATVEC_C128)
         h.profile(False)
     assert h.hit_cache_info() is None
-    assert nblk > 0 and info["converged"] >= 4
-    assert nsingle <= 4 * 2            # only the final FP64 residual maps are single-vector
+    assert nblk > 0 and info["converged"] >= 6
+    assert nsingle <= 6 * 2            # only the final FP64 residual maps are single-vector
     with block(0):                     # and MOMED_BLOCK=0 keeps the single-vector solver
-        ref, _, _, _ = h.eigsolve(4, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
+        ref, _, _, _ = h.eigsolve(6, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
     assert np.max(np.abs(vals - ref) / np.abs(ref)) < 1e-10
     h.profile(True)                    # with the hit cache (built by the solver): single-vector maps
-    vals2, _, _, _ = h.eigsolve(4, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
+    vals2, _, _, _ = h.eigsolve(6, krylovdim=30, tol=1e-12, seed=1, want_vectors=False)
     nhc, _ = h.profile_read(_lib.KERNEL_HC_MATVEC_C128)
     nhb, _ = h.profile_read(_lib.KERNEL_HC_BLOCK_C128)
     h.profile(False)
