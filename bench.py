@@ -49,9 +49,10 @@ KRYLOV = 30
 # of `bench.py --profile-only` (dram__bytes_read.sum + dram__bytes_write.sum = 46.5 + 28.8 MB): the
 # x block and the term tables stay in L2, so the per-hit gathers of the algorithmic count hit L2.
 MV_DRAM_BYTES = 75.3e6
-# DRAM bytes per launch of the c64 block map over the hit cache (ncu dram__bytes_read + write on the
-# headline sector); None until captured
-MV_DRAM_BYTES_HC = None
+# DRAM bytes (read + write) of one launch of the c64 x32 block map over the hit cache on this
+# workload, from an ncu capture of `bench.py --profile-only` (381.3 + 32.5 MB): the hit stream,
+# x and y once and the row metadata; the x-row gathers (9.6 GB per launch) are served by L2.
+MV_DRAM_BYTES_HC = 413.8e6
 METRIC = "batched solves/s, p50/p99 latency vs plain GPU Lanczos at <=1e-10 eig error"
 
 
@@ -1002,6 +1003,10 @@ def main():
                          "peak_source": peak_src,
                          "kernel": ("block map c64 x32 over the hit cache (k_block_hc<float, 32>)" if use_hc
                                     else "block matvec c64 x32 (k_block_matvec_v<float, 32>)"),
+                         "dram_frac": ((MV_DRAM_BYTES_HC if use_hc else MV_DRAM_BYTES) / (avg_ms * 1e-3) / 1e9 / peak),
+                         "note": "algorithmic bytes count one 32-wide x-row gather per hit; x (44 MB) stays in "
+                                 "L2, so those gathers are L2 traffic and DRAM moves only the traffic bytes "
+                                 "(dram_frac: their rate against the copy peak)",
                          "launches": n_mv, "avg_launch_ms": avg_ms,
                          "algorithmic_bytes_per_launch": bytes_per_launch},
             "cpu_baseline": cpu,

@@ -275,7 +275,10 @@ void worker_loop(momed_server* S, int slot) {
             gres.assign((size_t)nu * nev, 0.0);
             const double u = r->u;
             if (nu == 1) {
+                // the handle's u, host copy and device copies alike: the solvers read the host copy
+                // (the mixed path's batched solve, the combined amplitudes of the cached map)
                 float uf = (float)u;
+                h->u = u;
                 MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev.p, &u, sizeof(u), cudaMemcpyHostToDevice, h->stream));
                 MOMED_CUDA_TRY(cudaMemcpyAsync(h->u_dev32.p, &uf, sizeof(uf), cudaMemcpyHostToDevice, h->stream));
                 MOMED_CUDA_TRY(cudaStreamSynchronize(h->stream));

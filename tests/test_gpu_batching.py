@@ -58,7 +58,8 @@ def test_graph_replay_matches_eager_launches(h3x8):
     # the norms of the Gram-Schmidt update are summed with atomics (order not fixed), so two runs
     # agree to rounding, graphs or not
     assert np.max(np.abs(v0 - v1) / np.abs(v0)) < 1e-12
-    assert abs(i0["matvecs"] - i1["matvecs"]) <= 0.1 * i0["matvecs"]
+    # a convergence test that sits at its threshold can take one restart cycle more or less
+    assert abs(i0["restarts"] - i1["restarts"]) <= 1
 
 
 def test_autotuner_records_a_choice(h3x8):
