@@ -274,15 +274,18 @@ MOMED_API int  momed_block_tuning(momed_handle* h, int32_t nb, int32_t precision
  * and term slot of every off-diagonal (row, term) hit (8 bytes each) and each row's diagonal
  * sums, so that a map skips the candidate stage (mask tests, signs, index lookups) and forms
  * only the values, from the term list, at each application.  The eigensolvers build it at their
- * start when it fits a quarter of the free device memory and no HBM budget is set
- * (MOMED_HITCACHE=0: never, =1: whatever its size); momed_build_hit_cache builds it on request
- * (MOMED_ENOMEM when it does not fit, MOMED_ESTATE while a sparse matrix is built).  It is
+ * start when it fits a quarter of the free device memory and no HBM budget is set; when it does
+ * not, its slot mode (the term slot of each hit only, 2 bytes, for at most 65536 terms; the
+ * single-vector map then forms each target itself) when that fits 30% (MOMED_HITCACHE=0: never,
+ * =1: full whatever its size, =2: slot mode); momed_build_hit_cache builds it on request (the
+ * slot mode under MOMED_HITCACHE=2; MOMED_ENOMEM when it does not fit, MOMED_ESTATE while a
+ * sparse matrix is built).  It is
  * dropped with the basis, the operator, a sparse-matrix build, or new amplitudes of a
  * parametrised operator.  No reference counterpart: the reference map evaluates every term at
  * every application (ka_linearmap_kernel!, MomentumED/src/method/gpu_interface.jl:128-163). */
 MOMED_API int  momed_build_hit_cache(momed_handle* h, int64_t* hits, int64_t* bytes);
 MOMED_API int  momed_hit_cache_info(momed_handle* h, int32_t* built, int64_t* hits, int64_t* bytes,
-                                    double* build_ms);
+                                    double* build_ms);          /* built: 0 none, 1 full, 2 slot mode */
 MOMED_API int  momed_release_hit_cache(momed_handle* h);
 
 /* Kernels this library has launched in the process so far (all handles). */

@@ -64,6 +64,7 @@ OpView Operator::view() const {
     v.generic = generic.p;
     v.ngeneric = ngeneric;
     v.t_in = t_in.p;
+    v.t_out = t_out.p;
     v.t_pm = t_pm.p;
     v.t_amp = amp.p;
     v.t_amp32 = amp32.p;
@@ -100,7 +101,7 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
     std::stable_sort(ord.begin(), ord.end(), [&](int64_t a, int64_t b) {
         return out[a] < out[b] || (out[a] == out[b] && in[a] < in[b]);
     });
-    std::vector<uint64_t> t_in(nscat), t_pm(nscat), g_out;
+    std::vector<uint64_t> t_in(nscat), t_out(nscat), t_pm(nscat), g_out;
     std::vector<double2> A(nscat), B(amp_b ? nscat : 0);
     std::vector<float2> A32(nscat), B32(amp_b ? nscat : 0);
     std::vector<int32_t> g_start;
@@ -112,6 +113,7 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
             g_start.push_back((int32_t)q);
         }
         t_in[q] = in[s];
+        t_out[q] = out[s];
         uint64_t pm = parity_mask_host(out[s]) ^ parity_mask_host(in[s]);
         MOMED_REQUIRE(!parity || parity[s] == pm, MOMED_EINVAL,
                       "parity mask does not match parity_mask(out) xor parity_mask(in)");
@@ -156,6 +158,7 @@ void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, 
     up(op.pair, pair);
     up(op.generic, generic);
     up(op.t_in, t_in);
+    up(op.t_out, t_out);
     up(op.t_pm, t_pm);
     up(op.amp, A);
     up(op.amp32, A32);
@@ -718,7 +721,8 @@ int momed_build_hit_cache(momed_handle* h, int64_t* hits, int64_t* bytes) {
         MOMED_REQUIRE(!h->sparse.built && !h->sparse_only, MOMED_ESTATE,
                       "a sparse matrix is built: maps read it (momed_release_sparse first)");
         ensure_ready(h);
-        build_hit_cache(h);
+        const char* e = std::getenv("MOMED_HITCACHE");
+        build_hit_cache(h, (e && e[0] == '2') ? 2 : 1);     // MOMED_HITCACHE=2: the slot mode
         if (hits) *hits = h->hcache.nnz;
         if (bytes) *bytes = h->hcache.bytes;
         return MOMED_OK;
@@ -728,7 +732,7 @@ int momed_build_hit_cache(momed_handle* h, int64_t* hits, int64_t* bytes) {
 int momed_hit_cache_info(momed_handle* h, int32_t* built, int64_t* hits, int64_t* bytes, double* build_ms) {
     if (!h) return MOMED_EINVAL;
     return guarded(h, [&]() {
-        if (built) *built = h->hcache.built ? 1 : 0;
+        if (built) *built = h->hcache.built ? h->hcache.mode : 0;   // 1 full, 2 slot mode
         if (hits) *hits = h->hcache.nnz;
         if (bytes) *bytes = h->hcache.bytes;
         if (build_ms) *build_ms = h->hcache.build_ms;

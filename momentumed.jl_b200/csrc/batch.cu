@@ -399,7 +399,7 @@ template <> struct BlockMv<float2> {
             prof_end(h, MOMED_KERNEL_BLOCK_SPMV_C64);
             return;
         }
-        if (h->hcache.built) {
+        if (h->hcache.full()) {
             launch_block_hc_c64(h, x, y, u, nb, h->n, h->stream);
             prof_end(h, MOMED_KERNEL_HC_BLOCK_C64);
             return;
@@ -411,7 +411,7 @@ template <> struct BlockMv<float2> {
 template <> struct BlockMv<double2> {
     static void run(momed_handle* h, const double2* x, double2* y, const double* u, int nb) {
         prof_begin(h);
-        if (h->hcache.built) {
+        if (h->hcache.full()) {
             launch_block_hc_c128(h, x, y, u, nb, h->n, h->stream);
             prof_end(h, MOMED_KERNEL_HC_BLOCK_C128);
             return;

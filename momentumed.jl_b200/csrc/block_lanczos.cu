@@ -415,7 +415,7 @@ struct BlockKrylov {
                 launch_block_spmv_c64(h->sparse, reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(y), u,
                                       B, N, st);
                 prof_end(h, MOMED_KERNEL_BLOCK_SPMV_C64);
-            } else if (h->hcache.built) {
+            } else if (h->hcache.full()) {
                 launch_block_hc_c64(h, reinterpret_cast<const float2*>(x), reinterpret_cast<float2*>(y), u, B, N, st);
                 prof_end(h, MOMED_KERNEL_HC_BLOCK_C64);
             } else {
@@ -425,7 +425,7 @@ struct BlockKrylov {
             }
         } else {
             const double* u = h->op.has_b ? reinterpret_cast<const double*>(ud.p) : nullptr;
-            if (h->hcache.built) {
+            if (h->hcache.full()) {
                 launch_block_hc_c128(h, reinterpret_cast<const double2*>(x), reinterpret_cast<double2*>(y), u, B, N,
                                      st);
                 prof_end(h, MOMED_KERNEL_HC_BLOCK_C128);
@@ -829,7 +829,7 @@ int block_size_for(momed_handle* h, int nev, int precision) {
     // Mixed precision goes to the batched solver with one right-hand side instead (its anchored
     // FP64 refinement): two-component 4x6, nev 8: 2.73 s against 7.56 s for the mixed block solver
     // (whose FP64 phase restarts from B of the refined vectors) and 4.2 s for the FP64 one.
-    if (nev < 6 || h->n < (h->hcache.built ? 2000000 : 500000)) return 0;
+    if (nev < 6 || h->n < (h->hcache.full() ? 2000000 : 500000)) return 0;
     if (precision == MOMED_PREC_MIXED) return h->sparse.built ? (nev <= 10 ? 8 : 16) : 0;
     return nev <= 10 ? 4 : 8;
 }

@@ -21,8 +21,11 @@
 // hit stream (coalesced), the amplitude of each hit's term slot (the term list stays in L1/L2)
 // and gathers x.  The cache is built when it fits a quarter of the free HBM (MOMED_HITCACHE=0
 // turns it off, =1 builds it whatever its size); sectors whose hits do not fit (the 35M-state
-// 4x9 sectors: ~170 GB) keep the candidate map.  It is dropped with the basis, the operator or
-// the amplitudes (a twisted-boundary update) it was built from.
+// 4x9 sectors: ~170 GB) get the slot mode instead: per hit only its term slot (uint16, 2 bytes;
+// 43 GB for a 4x9 Ne = 12 sector), from which the single-vector map forms the target exactly as
+// the candidate map does (mask arithmetic, sign, two table reads) without the candidate stage;
+// the block maps read full caches only.  It is dropped with the basis, the operator or the
+// amplitudes (a twisted-boundary update) it was built from.
 #include <chrono>
 #include <cstdlib>
 #include <string>
@@ -162,6 +165,73 @@ k_hc_fill(IndexView iv, OpView ov, const int64_t* __restrict__ row_ptr, const in
     if (lane == 0 && nbad) atomicAdd(bad, nbad);
 }
 
+// Slot mode: the term slot of every off-diagonal hit in candidate order (one run per row), and
+// the diagonal sums as k_hc_fill forms them.
+__global__ void __launch_bounds__(kWarps * 32)
+k_hc_fill_slots(IndexView iv, OpView ov, const int64_t* __restrict__ row_ptr, uint16_t* __restrict__ slot,
+                double2* __restrict__ dg64, float2* __restrict__ dg32, int64_t rows, unsigned long long* bad) {
+    __shared__ SharedTables sh;
+    __shared__ WarpScratch s_ws[kWarps];
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    WarpScratch& ws = s_ws[wid];
+    unsigned long long nbad = 0;
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        const int64_t base = row_ptr[row], end = row_ptr[row + 1];
+        int64_t p = base;                  // warp-uniform
+        double dar = 0.0, dai = 0.0, dbr = 0.0, dbi = 0.0;
+        for_each_group_batch(s, ov, [&](int g) {
+            int total = stage_batch(g, ov, ws);
+            int gi = 0;
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                int f = f0 + lane;
+                int64_t j = -1;
+                int t = 0;
+                bool neg = false;
+                if (f < total) j = eval_term(f, gi, s, row, ov, iv, ws, sh, t, neg);
+                if (j == row) {
+                    const double2 a = __ldg(ov.t_amp + t);
+                    dar += a.x;
+                    dai += a.y;
+                    if (ov.t_ampb) {
+                        const double2 b = __ldg(ov.t_ampb + t);
+                        dbr += b.x;
+                        dbi += b.y;
+                    }
+                }
+                const bool off = j >= 0 && j != row;
+                const unsigned m = __ballot_sync(kFull, off);
+                if (off) {
+                    const int64_t pos = p + __popc(m & lt);
+                    if (pos < end) slot[pos] = (uint16_t)t;
+                    else ++nbad;
+                }
+                p += __popc(m);
+            }
+            __syncwarp();
+        });
+        if (lane == 0 && p != end) ++nbad;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            dar += __shfl_xor_sync(kFull, dar, o);
+            dai += __shfl_xor_sync(kFull, dai, o);
+            dbr += __shfl_xor_sync(kFull, dbr, o);
+            dbi += __shfl_xor_sync(kFull, dbi, o);
+        }
+        if (lane == 0) {
+            dg64[2 * row] = make_double2(dar, dai);
+            dg64[2 * row + 1] = make_double2(dbr, dbi);
+            dg32[2 * row] = make_float2((float)dar, (float)dai);
+            dg32[2 * row + 1] = make_float2((float)dbr, (float)dbi);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nbad += __shfl_xor_sync(kFull, nbad, o);
+    if (lane == 0 && nbad) atomicAdd(bad, nbad);
+}
+
 template <typename R> __device__ __forceinline__ const typename Cx<R>::T* hc_diag(const HitCacheView& v);
 template <> __device__ __forceinline__ const double2* hc_diag<double>(const HitCacheView& v) { return v.dg64; }
 template <> __device__ __forceinline__ const float2* hc_diag<float>(const HitCacheView& v) { return v.dg32; }
@@ -247,6 +317,65 @@ k_matvec_hc(HitCacheView hv, const typename Cx<R>::T* __restrict__ amp, const ty
             ar += v.x * xv.x - v.y * xv.y;
             ai += v.x * xv.y + v.y * xv.x;
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ar += __shfl_xor_sync(kFull, ar, o);
+            ai += __shfl_xor_sync(kFull, ai, o);
+        }
+        if (lane == 0) {
+            const C2 da = __ldg(dg + 2 * row);
+            R cx = da.x, cy = da.y;
+            if (HAS_B) {
+                const C2 db = __ldg(dg + 2 * row + 1);
+                cx += u * db.x;
+                cy += u * db.y;
+            }
+            const C2 xd = __ldg(x + row);
+            C2 o;
+            o.x = ar + cx * xd.x - cy * xd.y;
+            o.y = ai + cx * xd.y + cy * xd.x;
+            y[row] = o;
+        }
+    }
+}
+
+// y = H x in slot mode, one right-hand side: a warp per row, lanes stride over its hit slots four
+// at a time; each slot's target is formed as the candidate map forms it (the term's out and in
+// masks on the row state, the sign from its parity mask, two index-table reads), its value from
+// the A (+ u B) table, so only the candidate stage (groups, mask tests of the misses) is saved.
+template <typename R, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_matvec_slots(IndexView iv, HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ amp,
+               const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+               const R* __restrict__ u_ptr, int64_t rows) {
+    using C2 = typename Cx<R>::T;
+    __shared__ SharedTables sh;
+    stage_tables(sh, iv);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const R u = HAS_B ? *u_ptr : R(0);
+    const C2* __restrict__ dg = hc_diag<R>(hv);
+    for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
+        const uint64_t s = __ldg(iv.basis + row);
+        const int64_t b = __ldg(hv.row_ptr + row), e = __ldg(hv.row_ptr + row + 1);
+        R ar = 0, ai = 0;
+        auto hit = [&](int t) {
+            const uint64_t mid = s & ~__ldg(ov.t_out + t);
+            const int64_t j = lookup_index(iv, mid | __ldg(ov.t_in + t), sh.base_hi, sh.base_lo, sh.binom);
+            C2 v = __ldg(amp + t);
+            if (__popcll(mid & __ldg(ov.t_pm + t)) & 1) { v.x = -v.x; v.y = -v.y; }
+            const C2 xv = __ldg(x + j);
+            ar += v.x * xv.x - v.y * xv.y;
+            ai += v.x * xv.y + v.y * xv.x;
+        };
+        int64_t p = b + lane;
+        for (; p + 96 < e; p += 128) {
+            int t[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) t[q] = __ldg(hv.slot + p + 32 * q);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) hit(t[q]);
+        }
+        for (; p < e; p += 32) hit(__ldg(hv.slot + p));
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             ar += __shfl_xor_sync(kFull, ar, o);
@@ -418,6 +547,7 @@ HitCacheView HitCache::view() const {
     v.hit = hit.p;
     v.dg64 = dg64.p;
     v.dg32 = dg32.p;
+    v.slot = slot.p;
     return v;
 }
 
@@ -425,20 +555,33 @@ int64_t hit_cache_bytes(int64_t n, int64_t hits) {
     return (n + 1) * 8 + n * (8 + 32 + 16) + hits * 8;
 }
 
-bool hit_cache_wanted(const momed_handle* h) {
-    const char* e = std::getenv("MOMED_HITCACHE");
-    if (e && e[0] == '0') return false;
-    if (!h->hit_cache_ok || h->hbm_budget > 0 || h->sparse.built || h->sparse_only || h->n <= 0 || !h->op_set)
-        return false;
-    if (e && e[0] == '1') return true;
-    size_t free_b = 0, total_b = 0;
-    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return false;
-    return (double)hit_cache_bytes(h->n, h->nnz) <= 0.25 * (double)free_b;
+int64_t slot_cache_bytes(int64_t n, int64_t hits) {
+    return (n + 1) * 8 + n * (32 + 16) + hits * 2;
 }
 
-void build_hit_cache(momed_handle* h) {
+// The full cache when it fits a quarter of the free memory, else the slot mode when that fits
+// 30% (term slots must fit 16 bits); MOMED_HITCACHE=0: none, =1: full whatever its size, =2:
+// slot mode whatever its size.
+int hit_cache_wanted(const momed_handle* h) {
+    const char* e = std::getenv("MOMED_HITCACHE");
+    if (e && e[0] == '0') return 0;
+    if (!h->hit_cache_ok || h->hbm_budget > 0 || h->sparse.built || h->sparse_only || h->n <= 0 || !h->op_set)
+        return 0;
+    const bool slots_ok = h->op.nterms <= 65536;
+    if (e && e[0] == '1') return 1;
+    if (e && e[0] == '2') return slots_ok ? 2 : 0;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return 0;
+    if ((double)hit_cache_bytes(h->n, h->nnz) <= 0.25 * (double)free_b) return 1;
+    if (slots_ok && (double)slot_cache_bytes(h->n, h->nnz) <= 0.30 * (double)free_b) return 2;
+    return 0;
+}
+
+void build_hit_cache(momed_handle* h, int mode) {
     HitCache& hc = h->hcache;
     hc.release();
+    MOMED_REQUIRE(mode == 1 || mode == 2, MOMED_EINVAL, "hit cache: unknown mode");
+    MOMED_REQUIRE(mode == 1 || h->op.nterms <= 65536, MOMED_EINVAL, "hit cache: slot mode needs <= 65536 terms");
     const auto t0 = std::chrono::steady_clock::now();
     const int64_t n = h->n;
     cudaStream_t st = h->stream;
@@ -465,23 +608,30 @@ void build_hit_cache(momed_handle* h) {
         rp[i + 1] = rp[i] + a + b + d;
     }
     const int64_t nnz = rp[n];
-    const int64_t need = hit_cache_bytes(n, nnz);
+    const int64_t need = mode == 1 ? hit_cache_bytes(n, nnz) : slot_cache_bytes(n, nnz);
     size_t free_b = 0, total_b = 0;
     MOMED_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
     if ((double)need > 0.9 * (double)free_b)
         throw Error{MOMED_ENOMEM, "hit cache: needs " + std::to_string(need) + " bytes, " + std::to_string(free_b) +
                                      " free"};
     hc.row_ptr.resize(n + 1);
-    hc.seg.resize(n);
-    hc.hit.resize(std::max<int64_t>(nnz, 1));
     hc.dg64.resize(2 * n);
     hc.dg32.resize(2 * n);
     MOMED_CUDA_TRY(cudaMemcpyAsync(hc.row_ptr.p, rp.data(), (n + 1) * 8, cudaMemcpyHostToDevice, st));
-    MOMED_CUDA_TRY(cudaMemcpyAsync(hc.seg.p, sg.data(), n * sizeof(int2), cudaMemcpyHostToDevice, st));
     h->counters.resize(16);
     MOMED_CUDA_TRY(cudaMemsetAsync(h->counters.p + 4, 0, sizeof(unsigned long long), st));
-    k_hc_fill<<<hc_grid(k_hc_fill, n), kWarps * 32, 0, st>>>(iv, ov, hc.row_ptr.p, hc.seg.p, hc.hit.p, hc.dg64.p,
-                                                              hc.dg32.p, n, h->counters.p + 4);
+    if (mode == 1) {
+        hc.seg.resize(n);
+        hc.hit.resize(std::max<int64_t>(nnz, 1));
+        MOMED_CUDA_TRY(cudaMemcpyAsync(hc.seg.p, sg.data(), n * sizeof(int2), cudaMemcpyHostToDevice, st));
+        k_hc_fill<<<hc_grid(k_hc_fill, n), kWarps * 32, 0, st>>>(iv, ov, hc.row_ptr.p, hc.seg.p, hc.hit.p,
+                                                                  hc.dg64.p, hc.dg32.p, n, h->counters.p + 4);
+    } else {
+        hc.slot.resize(std::max<int64_t>(nnz, 1));
+        k_hc_fill_slots<<<hc_grid(k_hc_fill_slots, n), kWarps * 32, 0, st>>>(iv, ov, hc.row_ptr.p, hc.slot.p,
+                                                                              hc.dg64.p, hc.dg32.p, n,
+                                                                              h->counters.p + 4);
+    }
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
     unsigned long long bad = 0;
@@ -493,12 +643,15 @@ void build_hit_cache(momed_handle* h) {
     }
     hc.nnz = nnz;
     hc.bytes = need;
+    hc.mode = mode;
     hc.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     hc.built = true;
 }
 
 void ensure_hit_cache(momed_handle* h) {
-    if (!h->hcache.built && hit_cache_wanted(h)) build_hit_cache(h);
+    if (h->hcache.built) return;
+    const int mode = hit_cache_wanted(h);
+    if (mode) build_hit_cache(h, mode);
 }
 
 template <typename R> struct CombSlot;
@@ -524,6 +677,7 @@ static void matvec_hc_dispatch(momed_handle* h, const typename Cx<R>::T* x, type
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
     const C2* amp = amp_a_host<R>(ov);
+    MOMED_REQUIRE(h->hcache.built, MOMED_ESTATE, "hit cache: not built");
     if (hb) {
         HitCache& hc = h->hcache;
         auto& cb = CombSlot<R>::buf(hc);
@@ -539,9 +693,16 @@ static void matvec_hc_dispatch(momed_handle* h, const typename Cx<R>::T* x, type
         }
         amp = cb.p;
     }
-    auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, amp, x, y, up, rows); };
-    if (hb) go(k_matvec_hc<R, true>, u);
-    else go(k_matvec_hc<R, false>, nullptr);
+    if (h->hcache.mode == 2) {
+        const IndexView iv = index_view(h);
+        auto gs = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(iv, hv, ov, amp, x, y, up, rows); };
+        if (hb) gs(k_matvec_slots<R, true>, u);
+        else gs(k_matvec_slots<R, false>, nullptr);
+    } else {
+        auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, amp, x, y, up, rows); };
+        if (hb) go(k_matvec_hc<R, true>, u);
+        else go(k_matvec_hc<R, false>, nullptr);
+    }
     MOMED_CUDA_TRY(cudaGetLastError());
     note_launches(1);
 }
@@ -560,6 +721,7 @@ template <typename R>
 static void block_hc_dispatch(const momed_handle* h, const typename Cx<R>::T* x, typename Cx<R>::T* y, const R* u,
                               int32_t nb, int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
+    MOMED_REQUIRE(h->hcache.full(), MOMED_ESTATE, "hit cache: the block map needs a full cache");
     const HitCacheView hv = h->hcache.view();
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);

@@ -132,6 +132,7 @@ struct OpView {
     const int32_t* generic;    // [ngeneric]  other groups
     int32_t ngeneric;
     const uint64_t* t_in;      // [nterms]
+    const uint64_t* t_out;     // [nterms] (the group's out mask, per term)
     const uint64_t* t_pm;      // [nterms]
     const double2* t_amp;      // [nterms] c128 (A part)
     const float2* t_amp32;     // [nterms] c64  (A part)
@@ -154,7 +155,7 @@ struct Operator {
     int64_t nterms = 0;
     int32_t ngroups = 0, ngeneric = 0, max_groups = 0;
     bool has_b = false;
-    DevBuf<uint64_t> g_out, t_in, t_pm;
+    DevBuf<uint64_t> g_out, t_in, t_out, t_pm;
     DevBuf<int32_t> g_start, single, pair, generic;
     DevBuf<double2> amp, ampb;
     DevBuf<float2> amp32, ampb32;
@@ -213,10 +214,12 @@ struct HitCacheView {
     const uint2* hit;          // [nnz] {target row, term slot | sign << 31}
     const double2* dg64;       // [2n] diagonal sums: A part, B part
     const float2* dg32;        // [2n] the same in c64
+    const uint16_t* slot;      // [nnz] slot mode: the term slot of each off-diagonal hit
 };
 
 struct HitCache {
     bool built = false;
+    int mode = 0;               // 1: full (target and term slot per hit), 2: term slots only
     int64_t nnz = 0, bytes = 0;
     double build_ms = 0.0;
     DevBuf<int64_t> row_ptr;
@@ -224,15 +227,19 @@ struct HitCache {
     DevBuf<uint2> hit;
     DevBuf<double2> dg64;
     DevBuf<float2> dg32;
+    DevBuf<uint16_t> slot;
     // A + u B per term slot at the u of the single-vector map (one amplitude load per hit)
     DevBuf<double2> comb64;
     DevBuf<float2> comb32;
     double comb_u64 = 0.0, comb_u32 = 0.0;
     bool comb_ok64 = false, comb_ok32 = false;
     HitCacheView view() const;
+    bool full() const { return built && mode == 1; }   // the block maps read full caches only
     void release() {
         built = false;
+        mode = 0;
         nnz = bytes = 0;
+        slot.release();
         comb64.release();
         comb32.release();
         comb_ok64 = comb_ok32 = false;
@@ -313,8 +320,9 @@ int64_t validate_operator(momed_handle* h);   // counts (row, term) targets miss
 
 // hitcache.cu
 int64_t hit_cache_bytes(int64_t n, int64_t hits);
-bool hit_cache_wanted(const momed_handle* h);
-void build_hit_cache(momed_handle* h);
+int64_t slot_cache_bytes(int64_t n, int64_t hits);
+int hit_cache_wanted(const momed_handle* h);             // 0 none, 1 full, 2 term slots only
+void build_hit_cache(momed_handle* h, int mode = 1);
 void ensure_hit_cache(momed_handle* h);
 void launch_matvec_hc_c128(momed_handle* h, const double2* x, double2* y, const double* u, int64_t rows,
                            cudaStream_t st);

@@ -449,12 +449,14 @@ class Handle:
         return self.hit_cache_info()
 
     def hit_cache_info(self):
-        """{"hits", "bytes", "build_ms"} of the built hit cache, or None."""
+        """{"hits", "bytes", "build_ms", "mode"} of the built hit cache (mode "full": target and
+        term slot per hit; "slots": the term slot only), or None."""
         built, hits, nbytes, ms = C.c_int32(), C.c_int64(), C.c_int64(), C.c_double()
         self._check(lib().momed_hit_cache_info(self._h, C.byref(built), C.byref(hits), C.byref(nbytes), C.byref(ms)))
         if not built.value:
             return None
-        return {"hits": hits.value, "bytes": nbytes.value, "build_ms": ms.value}
+        return {"hits": hits.value, "bytes": nbytes.value, "build_ms": ms.value,
+                "mode": "full" if built.value == 1 else "slots"}
 
     def release_hit_cache(self):
         self._check(lib().momed_release_hit_cache(self._h))

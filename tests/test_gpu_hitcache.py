@@ -168,3 +168,27 @@ def test_solvers_over_the_cache_vs_lapack(setup):
     with env(MOMED_BLOCK=0):
         vals1, _, _, _ = h.eigsolve(8, krylovdim=48, tol=1e-12)
     assert np.max(np.abs(vals1 - w) / np.abs(w)) < 1e-10
+
+
+def test_slot_mode_matches_full_cache(setup):
+    """Slot mode (term slot per hit, the target formed at each application): the same hits as
+    the full cache and the same products."""
+    h, basis, pair = setup
+    n = len(basis)
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    h.set_param(0.9)
+    full = h.build_hit_cache()
+    y_full, y32_full = h.matvec(x), h.matvec(x.astype(np.complex64))
+    with env(MOMED_HITCACHE=2):
+        slots = h.build_hit_cache()
+    assert slots["hits"] == full["hits"] and slots["bytes"] < full["bytes"]
+    assert full["mode"] == "full" and slots["mode"] == "slots"
+    y_sl, y32_sl = h.matvec(x), h.matvec(x.astype(np.complex64))
+    y_ref = dense(basis, pair, 0.9) @ x
+    assert rel(y_sl, y_ref) < 1e-13 and rel(y_sl, y_full) < 1e-13
+    assert rel(y32_sl.astype(np.complex128), y32_full.astype(np.complex128)) < 2e-6
+    w = np.linalg.eigvalsh(dense(basis, pair, 0.9))[:4]
+    vals, _, _, _ = h.eigsolve(4, tol=1e-12)            # the single-vector solver over the slots
+    assert np.max(np.abs(vals - w) / np.abs(w)) < 1e-10
+    h.release_hit_cache()

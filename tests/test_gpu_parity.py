@@ -7,6 +7,8 @@ Bars (stated per test):
   - eigenvalues within 1e-10 relative of LAPACK (numpy.linalg.eigh) on the
     dense matrix, eigenvector subspace overlap >= 1 - 1e-9, residual reported.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -227,6 +229,19 @@ def test_matvec_4x9_ne12_largest_sector(h):
     rows = rng.choice(len(basis), 2000, replace=False)
     assert rel(hx[rows], O.matvec_rows(basis, ofull, x, rows)) < 1e-13
     assert h.stats()["nnz"] > 500 * len(basis)
+    # the slot-mode hit cache (2 bytes per hit, ~43 GB here; a full cache would need ~170 GB)
+    old = os.environ.get("MOMED_HITCACHE")
+    os.environ["MOMED_HITCACHE"] = "2"
+    try:
+        info = h.build_hit_cache()
+    finally:
+        if old is None:
+            del os.environ["MOMED_HITCACHE"]
+        else:
+            os.environ["MOMED_HITCACHE"] = old
+    assert info["mode"] == "slots" and info["hits"] > 500 * len(basis)
+    assert rel(h.matvec(x), hx) < 1e-13
+    h.release_hit_cache()
 
 
 # ------------------------------------------------------------------------------ Lanczos
