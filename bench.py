@@ -433,8 +433,8 @@ def serve_bench(args, device: int):
                    "device_solves": n_solves, "group_sizes": {str(k): v for k, v in sorted(gsizes.items())},
                    "slowest_solves": [{"mesh": k[0], "nev": v, "device_s": round(k[3], 3), "matvecs": k[2]}
                                       for k, v in slow],
-                   "precision": "mixed requests: batched mixed solver for groups on one sector, FP64 "
-                                "single-vector solver for a request alone; maps over the hit cache when "
+                   "precision": "mixed requests: the batched mixed solver, for groups on one sector and "
+                                "(one right-hand side) for a request alone; maps over the hit cache when "
                                 "it fits the budget, else the sparse method when its matrix fits",
                    "all_converged": bool(all(s_conv)), "max_rel_eig_err_vs_plain_fp64": max(errs)},
         "plain_one_at_a_time": {"solves_per_s": n / plain_span, "latency_ms_p50": 1e3 * pct(plain_lat, 50),
@@ -457,7 +457,7 @@ def serve_bench(args, device: int):
                                  "max_rel_eig_err_vs_map": max(
                                      float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1.0)))
                                      for a, b in zip(bl_vals, plain_vals))},
-        "policy": args.serve_policy or "default (alone: fp64; hit cache, else sparse method, when it fits)",
+        "policy": args.serve_policy or "default (alone: the request's precision; hit cache, else sparse method, when it fits)",
         "speedup_served_vs_plain": (n / s_span) / (n / plain_span),
         "speedup_served_vs_plain_sparse": (n / s_span) / (n / sp_span),
     }
