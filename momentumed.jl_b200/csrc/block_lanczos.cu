@@ -752,8 +752,11 @@ int solve_blocked(momed_handle* h, const momed_solve_opts* o, int nev, const dou
         S1.resize((size_t)k1 * N);
         typename BlockKrylov<float2, B>::Out r1;
         {
+            // converge the nev wanted pairs to the FP32 floor and return k1 Ritz vectors: the
+            // extra ones need not reach the floor (asking it of them stalled the phase when
+            // k1 = B: 3x9, nev 4, B = 8 forced ran 14 s)
             BlockKrylov<float2, B> K(h, mb);
-            r1 = K.run(k1, 0.0, 2e-6, maxiter, start64, start64 ? 1 : 0, o->seed, k1, X1.p);
+            r1 = K.run(nev, 0.0, 2e-6, maxiter, start64, start64 ? 1 : 0, o->seed, k1, X1.p);
             matvecs += K.matvecs;
         }
         restarts += r1.restarts;
