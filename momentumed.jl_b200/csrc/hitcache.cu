@@ -246,14 +246,15 @@ __device__ __forceinline__ uint2 ld_hit(const uint2* p) {
 
 
 
-// MOMED_HC_PF=0: the block map loads each pair of hit records right before using them
-bool hc_prefetch() {
-    static int on = -1;
-    if (on < 0) {
-        const char* e = std::getenv("MOMED_HC_PF");
-        on = (e && e[0] == '0') ? 0 : 1;
+// MOMED_HC_MINB=5|6: the c64 32-wide block map fitted to 5 or 6 resident CTAs per SM (fewer
+// registers, more warps to hide the gathers' latency) instead of the compiler's choice (4)
+int hc_minb() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("MOMED_HC_MINB");
+        v = e ? std::atoi(e) : 0;
     }
-    return on == 1;
+    return v;
 }
 
 template <typename C2>
@@ -406,12 +407,14 @@ k_matvec_slots(IndexView iv, HitCacheView hv, OpView ov, const typename Cx<R>::T
 // 32 records per warp at once (the next 32 in flight) and handing them out by shuffles was
 // measured slower (0.84 against 0.70 ms per launch on the headline sector: more registers, the
 // shuffles on the issue path).
-// PF: the hit records of a lane group's next two hits are loaded before the current two are
-// consumed (their stream comes from HBM; the x rows, from L2, then wait on one latency only).
-template <typename R, int NB, bool HAS_B, bool PF>
-__global__ void __launch_bounds__(kWarps * 32)
-k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-           const R* __restrict__ u, int64_t rows) {
+// The hit records of a lane group's next two hits are loaded before the current two are
+// consumed (their stream comes from HBM; the x rows, from L2, then wait on one latency only;
+// 1% faster maps).  MINB: resident CTAs per SM the registers are fitted to.
+template <typename R, int NB, bool HAS_B>
+__device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpView& ov,
+                                              const typename Cx<R>::T* __restrict__ x,
+                                              typename Cx<R>::T* __restrict__ y, const R* __restrict__ u,
+                                              int64_t rows) {
     using C2 = typename Cx<R>::T;
     using IO = BlkIO<R, NB>;
     constexpr int RPL = IO::RPL, LPH = IO::LPH, HPI = IO::HPI;
@@ -451,30 +454,22 @@ k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, 
             fma(h.x, c, cb);
         };
         int64_t p = beg + hslot;
-        if constexpr (PF) {
-            if (p + HPI < end) {
-                uint2 h0 = ld_hit(hv.hit + p), h1 = ld_hit(hv.hit + p + HPI);
-                for (;;) {
-                    const int64_t pn = p + 2 * HPI;
-                    const bool more = pn + HPI < end;
-                    uint2 n0 = h0, n1 = h1;
-                    if (more) {
-                        n0 = ld_hit(hv.hit + pn);
-                        n1 = ld_hit(hv.hit + pn + HPI);
-                    }
-                    use(h0);
-                    use(h1);
-                    p = pn;
-                    if (!more) break;
-                    h0 = n0;
-                    h1 = n1;
+        if (p + HPI < end) {
+            uint2 h0 = ld_hit(hv.hit + p), h1 = ld_hit(hv.hit + p + HPI);
+            for (;;) {
+                const int64_t pn = p + 2 * HPI;
+                const bool more = pn + HPI < end;
+                uint2 n0 = h0, n1 = h1;
+                if (more) {
+                    n0 = ld_hit(hv.hit + pn);
+                    n1 = ld_hit(hv.hit + pn + HPI);
                 }
-            }
-        } else {
-            for (; p + HPI < end; p += 2 * HPI) {
-                const uint2 h0 = ld_hit(hv.hit + p), h1 = ld_hit(hv.hit + p + HPI);
                 use(h0);
                 use(h1);
+                p = pn;
+                if (!more) break;
+                h0 = n0;
+                h1 = n1;
             }
         }
         if (p < end) use(ld_hit(hv.hit + p));
@@ -526,6 +521,21 @@ k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, 
             store_lane<R, NB>(y + row * NB, kk, o);
         }
     }
+}
+
+template <typename R, int NB, bool HAS_B>
+__global__ void __launch_bounds__(kWarps * 32)
+k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+           const R* __restrict__ u, int64_t rows) {
+    block_hc_body<R, NB, HAS_B>(hv, ov, x, y, u, rows);
+}
+
+// the same map with its registers fitted to MINB resident CTAs per SM (MOMED_HC_MINB)
+template <typename R, int NB, bool HAS_B, int MINB>
+__global__ void __launch_bounds__(kWarps * 32, MINB)
+k_block_hc_mb(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
+              const R* __restrict__ u, int64_t rows) {
+    block_hc_body<R, NB, HAS_B>(hv, ov, x, y, u, rows);
 }
 
 template <typename K>
@@ -725,14 +735,20 @@ static void block_hc_dispatch(const momed_handle* h, const typename Cx<R>::T* x,
     const HitCacheView hv = h->hcache.view();
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
-    const bool pf = hc_prefetch();
     auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, ov, x, y, up, rows); };
+    if constexpr (std::is_same<R, float>::value) {
+        if (nb == 32 && hb && (hc_minb() == 5 || hc_minb() == 6)) {
+            if (hc_minb() == 5) go(k_block_hc_mb<R, 32, true, 5>, u);
+            else go(k_block_hc_mb<R, 32, true, 6>, u);
+            MOMED_CUDA_TRY(cudaGetLastError());
+            note_launches(1);
+            return;
+        }
+    }
 #define MOMED_BHC(NBV)                                                                        \
     case NBV:                                                                                 \
-        if (hb && pf) go(k_block_hc<R, NBV, true, true>, u);                                  \
-        else if (hb) go(k_block_hc<R, NBV, true, false>, u);                                  \
-        else if (pf) go(k_block_hc<R, NBV, false, true>, nullptr);                            \
-        else go(k_block_hc<R, NBV, false, false>, nullptr);                                   \
+        if (hb) go(k_block_hc<R, NBV, true>, u);                                              \
+        else go(k_block_hc<R, NBV, false>, nullptr);                                          \
         break;
     switch (nb) {
         MOMED_BHC(1)
