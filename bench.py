@@ -84,7 +84,8 @@ def parse():
     ap.add_argument("--serve-meshes", default="3x5,3x9,3x10", help="subset of 3x5,3x9,3x10,4x9")
     ap.add_argument("--serve-slots", type=int, default=4)
     ap.add_argument("--serve-hbm-gb", type=float, default=100.0)
-    ap.add_argument("--serve-policy", default="", help="served arm switches: alone=fp64|mixed,sparse=1|0,hitcache=1|0,large=<concurrent large solves>")
+    ap.add_argument("--serve-policy", default="", help="served arm switches: alone=fp64|mixed,sparse=1|0,hitcache=1|0,large=<concurrent large solves>,"
+                         "group=<smallest group>")
     ap.add_argument("--serve-only", action="store_true", help="only the serving stream (one JSON object)")
     return ap.parse_args()
 
@@ -387,7 +388,7 @@ def serve_bench(args, device: int):
     for kv in [x for x in args.serve_policy.split(",") if x]:
         k, v = kv.split("=")
         os.environ[{"alone": "MOMED_SERVE_ALONE", "sparse": "MOMED_SERVE_SPARSE", "hitcache": "MOMED_SERVE_HITCACHE",
-                    "large": "MOMED_SERVE_LARGE_MAX"}[k]] = v
+                    "large": "MOMED_SERVE_LARGE_MAX", "group": "MOMED_SERVE_MIN_GROUP"}[k]] = v
 
     def run_server():
         srv = momed.Server(device, slots=args.serve_slots, hbm_budget=int(args.serve_hbm_gb * (1 << 30)))

@@ -202,12 +202,15 @@ void worker_loop(momed_server* S, int slot) {
             // block Lanczos in FP64 on the matrix-free map) took longer than its requests solved
             // one by one with the sparse method (3x10, nev 15/8/11: 6.4 s against ~0.8 s each).
             const int64_t N = (int64_t)r->basis.size();
-            // A request whose sparse matrix will fit is solved alone on it: measured on the serving
-            // stream, a group of three 3x10 requests (nev 12) took 7.2 s on the batched solver and
-            // ~0.8 s each alone on the sparse method.  The matrix size comes from the hits per row
-            // that earlier solves on the operator measured.
+            // Without the hit cache (MOMED_SERVE_HITCACHE=0), a request whose sparse matrix will fit
+            // is solved alone on it: measured on the serving stream, a group of three 3x10 requests
+            // (nev 12) took 7.2 s on the batched solver over the candidate map and ~0.8 s each alone
+            // on the sparse method.  The matrix size comes from the hits per row that earlier
+            // solves on the operator measured.  Over the hit cache a group is one batched solve
+            // whose block map serves every member's right-hand side.
+            const bool use_hc = knob("MOMED_SERVE_HITCACHE", "1") != "0";
             bool sparse_fits = false;
-            if (N >= kSparseMinRows && opp && r->op < (int32_t)S->op_hits_per_row.size() &&
+            if (!use_hc && N >= kSparseMinRows && opp && r->op < (int32_t)S->op_hits_per_row.size() &&
                 knob("MOMED_SERVE_SPARSE", "1") != "0") {
                 const double hpr = S->op_hits_per_row[r->op];
                 const int64_t sp = (N + 1) * 8 + (int64_t)((hpr + 1.0) * (double)N) * sparse_bytes_per_entry(opp->has_b);
@@ -228,7 +231,8 @@ void worker_loop(momed_server* S, int slot) {
                     break;
                 }
             }
-            if ((int)grp.size() >= kMinGroup) {
+            const int min_group = std::max(2, std::atoi(knob("MOMED_SERVE_MIN_GROUP", std::to_string(kMinGroup).c_str()).c_str()));
+            if ((int)grp.size() >= min_group) {
                 gbytes = estimate_bytes(N, group_opts(grp), pow2_at_least((int64_t)grp.size()));
                 auto taken = [&](const std::shared_ptr<Request>& q) {
                     return std::find(grp.begin() + 1, grp.end(), q) != grp.end();
