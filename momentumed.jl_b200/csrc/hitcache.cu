@@ -401,8 +401,9 @@ k_matvec_slots(IndexView iv, HitCacheView hv, OpView ov, const typename Cx<R>::T
 // The hit records of a lane group's next two hits are loaded before the current two are
 // consumed (their stream comes from HBM; the x rows, from L2, then wait on one latency only;
 // 1% faster maps).  Fitting its registers to 5 or 6 resident CTAs per SM (48 or 40 registers)
-// spilled 156-232 bytes and ran 1.14-1.16 ms per launch against 0.70 ms at 63 registers.
-template <typename R, int NB, bool HAS_B, int U>
+// spilled 156-232 bytes and ran 1.14-1.16 ms per launch against 0.70 ms at 63 registers; four
+// hits in flight per lane group (72 registers, 3 CTAs per SM) ran 0.76 ms.
+template <typename R, int NB, bool HAS_B>
 __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpView& ov,
                                               const typename Cx<R>::T* __restrict__ x,
                                               typename Cx<R>::T* __restrict__ y, const R* __restrict__ u,
@@ -445,31 +446,27 @@ __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpVi
             if constexpr (KIND == 2) cb = signed_amp(B, h.y);
             fma(h.x, c, cb);
         };
-        // U hits of a lane group per step, the next U hit records loaded before these are used
+        // two hits of a lane group per step, the next two hit records loaded before these are used
         int64_t p = beg + hslot;
-        if (p + (U - 1) * HPI < end) {
-            uint2 hcur[U];
-#pragma unroll
-            for (int i = 0; i < U; ++i) hcur[i] = ld_hit(hv.hit + p + i * HPI);
+        if (p + HPI < end) {
+            uint2 h0 = ld_hit(hv.hit + p), h1 = ld_hit(hv.hit + p + HPI);
             for (;;) {
-                const int64_t pn = p + U * HPI;
-                const bool more = pn + (U - 1) * HPI < end;
-                uint2 hnext[U];
-#pragma unroll
-                for (int i = 0; i < U; ++i) hnext[i] = hcur[i];
+                const int64_t pn = p + 2 * HPI;
+                const bool more = pn + HPI < end;
+                uint2 n0 = h0, n1 = h1;
                 if (more) {
-#pragma unroll
-                    for (int i = 0; i < U; ++i) hnext[i] = ld_hit(hv.hit + pn + i * HPI);
+                    n0 = ld_hit(hv.hit + pn);
+                    n1 = ld_hit(hv.hit + pn + HPI);
                 }
-#pragma unroll
-                for (int i = 0; i < U; ++i) use(hcur[i]);
+                use(h0);
+                use(h1);
                 p = pn;
                 if (!more) break;
-#pragma unroll
-                for (int i = 0; i < U; ++i) hcur[i] = hnext[i];
+                h0 = n0;
+                h1 = n1;
             }
         }
-        for (; p < end; p += HPI) use(ld_hit(hv.hit + p));
+        if (p < end) use(ld_hit(hv.hit + p));
     };
 
     for (int64_t row = (int64_t)blockIdx.x * kWarps + wid; row < rows; row += (int64_t)gridDim.x * kWarps) {
@@ -524,15 +521,7 @@ template <typename R, int NB, bool HAS_B>
 __global__ void __launch_bounds__(kWarps * 32)
 k_block_hc(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
            const R* __restrict__ u, int64_t rows) {
-    block_hc_body<R, NB, HAS_B, 2>(hv, ov, x, y, u, rows);
-}
-
-// four hits of a lane group in flight instead of two (MOMED_HC_UNROLL=4)
-template <typename R, int NB, bool HAS_B>
-__global__ void __launch_bounds__(kWarps * 32)
-k_block_hc4(HitCacheView hv, OpView ov, const typename Cx<R>::T* __restrict__ x, typename Cx<R>::T* __restrict__ y,
-            const R* __restrict__ u, int64_t rows) {
-    block_hc_body<R, NB, HAS_B, 4>(hv, ov, x, y, u, rows);
+    block_hc_body<R, NB, HAS_B>(hv, ov, x, y, u, rows);
 }
 
 template <typename K>
@@ -733,15 +722,6 @@ static void block_hc_dispatch(const momed_handle* h, const typename Cx<R>::T* x,
     const OpView ov = h->op.view();
     const bool hb = (u != nullptr) && (std::is_same<R, double>::value ? ov.t_ampb != nullptr : ov.t_ampb32 != nullptr);
     auto go = [&](auto k, const R* up) { k<<<hc_grid(k, rows), kWarps * 32, 0, st>>>(hv, ov, x, y, up, rows); };
-    if constexpr (std::is_same<R, float>::value) {
-        const char* e = std::getenv("MOMED_HC_UNROLL");
-        if (nb == 32 && hb && e && e[0] == '4') {
-            go(k_block_hc4<R, 32, true>, u);
-            MOMED_CUDA_TRY(cudaGetLastError());
-            note_launches(1);
-            return;
-        }
-    }
 #define MOMED_BHC(NBV)                                                                        \
     case NBV:                                                                                 \
         if (hb) go(k_block_hc<R, NBV, true>, u);                                              \
