@@ -925,74 +925,6 @@ k_bgram(const VT* __restrict__ V, int64_t N, int ncols, GramRhs R, int nr, doubl
     }
 }
 
-// The same Gram partials with four columns per warp: a lane holds one right-hand-side value
-// (NB lanes per row, 32 / NB rows per pass) and multiplies each loaded right-hand-side value
-// into four columns, so the right-hand sides are read once per four columns instead of once per
-// column (k_bgram's warps re-read them through L1, which bounded it at ~0.2 of the copy peak).
-// Grid: x = row blocks, y = groups of 32 columns (8 warps x 4).
-constexpr int kGramCols = 4;
-template <typename VT, int NB>
-__global__ void __launch_bounds__(kT)
-k_bgram4(const VT* __restrict__ V, int64_t N, int ncols, GramRhs R, int nr, double2* __restrict__ partial) {
-    constexpr int RS = 32 / NB;                 // rows per warp pass
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    const int rr = lane % NB, rs = lane / NB;
-    const int c0 = (blockIdx.y * 8 + wid) * kGramCols;
-    if (c0 >= ncols) return;                    // warp-uniform
-    double ax[kGramCols][kGramRhs], ay[kGramCols][kGramRhs];
-#pragma unroll
-    for (int c = 0; c < kGramCols; ++c)
-#pragma unroll
-        for (int j = 0; j < kGramRhs; ++j) { ax[c][j] = 0.0; ay[c][j] = 0.0; }
-    const int64_t per = (N + gridDim.x - 1) / gridDim.x;
-    const int64_t r0 = (int64_t)blockIdx.x * per, r1 = min(N, r0 + per);
-    const VT* vc[kGramCols];
-#pragma unroll
-    for (int c = 0; c < kGramCols; ++c) vc[c] = V + (int64_t)min(c0 + c, ncols - 1) * N * NB + rr;
-#pragma unroll 1
-    for (int64_t t = r0 + rs; t < r1; t += RS) {
-        double2 w[kGramRhs];
-#pragma unroll
-        for (int j = 0; j < kGramRhs; ++j) w[j] = j < nr ? __ldg(R.p[j] + t * NB + rr) : make_double2(0.0, 0.0);
-#pragma unroll
-        for (int c = 0; c < kGramCols; ++c) {
-            const double2 v = to2(__ldg(vc[c] + t * NB));
-#pragma unroll
-            for (int j = 0; j < kGramRhs; ++j) {
-                ax[c][j] += v.x * w[j].x + v.y * w[j].y;
-                ay[c][j] += v.x * w[j].y - v.y * w[j].x;
-            }
-        }
-    }
-#pragma unroll
-    for (int c = 0; c < kGramCols; ++c)
-#pragma unroll
-        for (int j = 0; j < kGramRhs; ++j) {
-            double sx = ax[c][j], sy = ay[c][j];
-#pragma unroll
-            for (int o = NB; o < 32; o <<= 1) {
-                sx += __shfl_xor_sync(0xffffffffu, sx, o);
-                sy += __shfl_xor_sync(0xffffffffu, sy, o);
-            }
-            if (j < nr && rs == 0 && c0 + c < ncols)
-                partial[(((int64_t)blockIdx.x * kGramRhs + j) * ncols + c0 + c) * NB + rr] = make_double2(sx, sy);
-        }
-}
-
-inline dim3 bgram4_grid(int rowblocks, int ncols) {
-    return dim3(rowblocks, (unsigned)std::max(1, (ncols + 8 * kGramCols - 1) / (8 * kGramCols)));
-}
-
-// MOMED_GRAM=1: the column-per-warp Gram kernel (k_bgram) instead of k_bgram4
-bool gram_per_column() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = std::getenv("MOMED_GRAM");
-        v = (e && e[0] == '1') ? 1 : 0;
-    }
-    return v == 1;
-}
-
 // out[e] = sum over blocks b < grid of partial[b * bstride + e] for e < count, one warp per
 // element (fixed order)
 __global__ void k_bsum_blocks(const double2* __restrict__ partial, int grid, int64_t bstride, int64_t count,
@@ -1291,20 +1223,12 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                     for (int j = 0; j < nr; ++j)
                         R.p[j] = (g0 + j < k1 ? Wb.p + (size_t)(g0 + j) * stride : Xb.p + (size_t)(g0 + j - k1) * stride);
                     for (int j = nr; j < kGramRhs; ++j) R.p[j] = R.p[0];
-                    if (gram_per_column()) {
-                        if (fp32)
-                            k_bgram<float2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
-                                reinterpret_cast<const float2*>(cols), N, ncols, R, nr, gpart.p);
-                        else
-                            k_bgram<double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
-                                reinterpret_cast<const double2*>(cols), N, ncols, R, nr, gpart.p);
-                    } else if (fp32) {
-                        k_bgram4<float2, NB><<<bgram4_grid(rb, ncols), kT, 0, st>>>(
+                    if (fp32)
+                        k_bgram<float2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
                             reinterpret_cast<const float2*>(cols), N, ncols, R, nr, gpart.p);
-                    } else {
-                        k_bgram4<double2, NB><<<bgram4_grid(rb, ncols), kT, 0, st>>>(
+                    else
+                        k_bgram<double2, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(
                             reinterpret_cast<const double2*>(cols), N, ncols, R, nr, gpart.p);
-                    }
                     // the nr valid slabs lead each block's [kGramRhs][ncols][NB] partials
                     const int64_t bstride = (int64_t)kGramRhs * ncols * NB, count = (int64_t)nr * ncols * NB;
                     k_bsum_blocks<<<(unsigned)((count + 7) / 8), 256, 0, st>>>(gpart.p, rb, bstride, count, out);
