@@ -540,7 +540,6 @@ int momed_matvec(momed_handle* h, const void* x, void* y, int32_t precision, int
         MOMED_CUDA_TRY(cudaEventRecord(h->ev1, st));
         if (!on_device) MOMED_CUDA_TRY(cudaMemcpyAsync(y, dy, n * es, cudaMemcpyDeviceToHost, st));
         MOMED_CUDA_TRY(cudaStreamSynchronize(st));
-        if (h->sparse.built) check_spmv_status(h->sparse, st);
         float ms = 0.f;
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
         h->last_kernel_ms = ms;

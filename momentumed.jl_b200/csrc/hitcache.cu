@@ -441,8 +441,6 @@ __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpVi
         // the hit with record h: target and signed amplitude(s) of its kind
         auto use = [&](uint2 h) {
             C2 c, cb;
-            cb.x = R(0);
-            cb.y = R(0);
             if constexpr (KIND == 0) c = signed_amp(B, h.y);
             else c = signed_amp(A, h.y);
             if constexpr (KIND == 2) cb = signed_amp(B, h.y);

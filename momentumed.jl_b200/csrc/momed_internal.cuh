@@ -194,12 +194,9 @@ struct SparseMatrix {
     // the A and B parts of H(u) = A + u B per entry (c64), for the batched solver's block SpMV
     // (parametrised operators only; a single operator's block SpMV reads val32)
     DevBuf<float2> pa32, pb32;
-    // waits of the bulk-copy SpMV that ran out (k_spmv_bulk sets it; read after a solve)
-    DevBuf<unsigned long long> err;
     void release() {
         built = false;
         nnz = 0;
-        err.release();
         row_ptr.release();
         col.release();
         val.release();
@@ -372,7 +369,6 @@ void launch_block_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, c
                            int64_t rows, cudaStream_t st);
 void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int64_t rows, cudaStream_t st);
 void launch_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, int64_t rows, cudaStream_t st);
-void check_spmv_status(const SparseMatrix& sp, cudaStream_t st);   // throws when a bulk-copy wait ran out
 
 // operator.cpp-side (in abi.cu)
 void upload_operator(momed_handle* h, const double* amp_a, const double* amp_b, const uint64_t* in,

@@ -237,135 +237,6 @@ k_spmv(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col, con
     }
 }
 
-// CSR SpMV with bulk-copied column and value streams.  A warp owns a contiguous range of rows,
-// whose entries form one contiguous stream; lane 0 brings it into the warp's two shared-memory
-// stages with 1-D bulk copies (cp.async.bulk: the copy engine reads HBM, no L1 request slots)
-// one chunk of kSpChunk entries ahead of the lanes, an mbarrier per stage signalling completion.
-// The lanes take columns and values from shared memory and gather x through L1/L2.  Chunks
-// start on multiples of 4 entries (16-byte source alignment of the int32 columns); the arrays are
-// padded by 4 entries so that the last chunk's copy stays inside them.  Every wait is bounded: a
-// wait that runs out is counted in err, the warp waits (bounded) for its copies in flight and
-// stops; the host reads err after the solve.
-constexpr int kSpChunk = 256;
-constexpr int kSpWarps = 8;
-constexpr unsigned kSpWaitLimit = 1u << 22;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_test(uint64_t* bar, unsigned parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-    for (unsigned it = 0; it < kSpWaitLimit; ++it) {
-        if (mbar_test(bar, parity)) return true;
-        if (it > 64) __nanosleep(64);
-    }
-    return false;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(kSpWarps * 32)
-k_spmv_bulk(const int64_t* __restrict__ row_ptr, const int32_t* __restrict__ col,
-            const typename SpVal<R>::T* __restrict__ val, const typename SpVal<R>::T* __restrict__ x,
-            typename SpVal<R>::T* __restrict__ y, int64_t rows, unsigned long long* err) {
-    using C2 = typename SpVal<R>::T;
-    constexpr int kColB = kSpChunk * 4, kValB = kSpChunk * (int)sizeof(C2);
-    extern __shared__ __align__(128) unsigned char sp_smem[];
-    __shared__ __align__(8) uint64_t bars[kSpWarps][2];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    unsigned char* wb = sp_smem + (size_t)wid * 2 * (kColB + kValB);
-    int32_t* scol[2] = {reinterpret_cast<int32_t*>(wb), reinterpret_cast<int32_t*>(wb + kColB + kValB)};
-    C2* sval[2] = {reinterpret_cast<C2*>(wb + kColB), reinterpret_cast<C2*>(wb + 2 * kColB + kValB)};
-    const int64_t nwarps = (int64_t)gridDim.x * kSpWarps;
-    const int64_t per = (rows + nwarps - 1) / nwarps;
-    const int64_t wr0 = min(rows, ((int64_t)blockIdx.x * kSpWarps + wid) * per), wr1 = min(rows, wr0 + per);
-    if (wr0 >= wr1) return;                     // warp-uniform; this warp's barriers are never used
-    if (lane == 0) {
-        mbar_init(&bars[wid][0], 1);
-        mbar_init(&bars[wid][1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncwarp();
-    const int64_t e0 = __ldg(row_ptr + wr0), e1 = __ldg(row_ptr + wr1);
-    const int64_t base = e0 & ~(int64_t)3, e1r = (e1 + 3) & ~(int64_t)3;
-    const int64_t nchunk = (e1 - base + kSpChunk - 1) / kSpChunk;
-    auto issue = [&](int64_t k) {
-        if (lane == 0) {
-            const int st = (int)(k & 1);
-            const int64_t c0 = base + k * kSpChunk;
-            const int64_t c1 = min(c0 + (int64_t)kSpChunk, e1r);
-            const unsigned cnt = (unsigned)(c1 - c0);          // a positive multiple of 4
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_expect_tx(&bars[wid][st], cnt * (4u + (unsigned)sizeof(C2)));
-            bulk_g2s(scol[st], col + c0, cnt * 4u, &bars[wid][st]);
-            bulk_g2s(sval[st], val + c0, cnt * (unsigned)sizeof(C2), &bars[wid][st]);
-        }
-    };
-    issue(0);
-    int64_t r = wr0, rend = __ldg(row_ptr + wr0 + 1);
-    R ar = 0, ai = 0;
-    int64_t k = 0;
-    for (; k < nchunk; ++k) {
-        if (k + 1 < nchunk) issue(k + 1);
-        const int st = (int)(k & 1);
-        if (!__all_sync(kFull, mbar_wait(&bars[wid][st], (unsigned)((k >> 1) & 1)))) break;
-        const int64_t c0 = base + k * kSpChunk, c1 = min(c0 + (int64_t)kSpChunk, e1);
-        int64_t p = max(c0, e0);
-        while (p < c1) {                        // warp-uniform: the rows overlapping [p, c1)
-            const int64_t seg = min(rend, c1);
-            for (int64_t q = p + lane; q < seg; q += 32) {
-                const C2 v = sval[st][q - c0];
-                const C2 xv = __ldg(x + scol[st][q - c0]);
-                ar += v.x * xv.x - v.y * xv.y;
-                ai += v.x * xv.y + v.y * xv.x;
-            }
-            p = seg;
-            if (seg == rend) {                  // the row is complete
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    ar += __shfl_xor_sync(kFull, ar, o);
-                    ai += __shfl_xor_sync(kFull, ai, o);
-                }
-                if (lane == 0) {
-                    C2 out;
-                    out.x = ar;
-                    out.y = ai;
-                    y[r] = out;
-                }
-                ar = 0;
-                ai = 0;
-                if (++r >= wr1) break;
-                rend = __ldg(row_ptr + r + 1);
-            }
-        }
-        __syncwarp();                           // stage st is read; it may be refilled next
-    }
-    if (k < nchunk) {                           // a wait ran out: count it, let the copies land, stop
-        if (lane == 0) {
-            atomicAdd(err, 1ull);
-            mbar_wait(&bars[wid][k & 1], (unsigned)((k >> 1) & 1));
-            if (k + 1 < nchunk) mbar_wait(&bars[wid][(k + 1) & 1], (unsigned)(((k + 1) >> 1) & 1));
-        }
-        __syncwarp();
-    }
-}
-
 // Block SpMV for the batched solver: NB right-hand sides interleaved as x[row * NB + r], the
 // operator of right-hand side r is A + u[r] B (u null: val32 for all).  Each entry's NB values
 // are read by NB / RPL lanes, RPL = min(NB, 4) values per lane (16-byte loads, laid out as
@@ -500,11 +371,9 @@ void build_sparse(momed_handle* h, double u) {
                                      std::to_string(limit) + " available"};
 
     sp.row_ptr.resize(n + 1);
-    sp.col.resize(nnz + 4);                   // +4: the bulk-copy SpMV's last chunk is rounded up to 4
-    sp.val.resize(nnz + 4);
-    sp.val32.resize(nnz + 4);
-    sp.err.resize(1);
-    MOMED_CUDA_TRY(cudaMemsetAsync(sp.err.p, 0, sizeof(unsigned long long), st));
+    sp.col.resize(std::max<int64_t>(nnz, 1));
+    sp.val.resize(std::max<int64_t>(nnz, 1));
+    sp.val32.resize(std::max<int64_t>(nnz, 1));
     if (hb) {
         sp.pa32.resize(std::max<int64_t>(nnz, 1));
         sp.pb32.resize(std::max<int64_t>(nnz, 1));
@@ -553,11 +422,9 @@ void upload_sparse(momed_handle* h, int64_t n, const int64_t* row_ptr, const int
         throw Error{MOMED_ENOMEM, "sparse method: the matrix needs " + std::to_string(need) + " bytes, " +
                                      std::to_string(limit) + " available"};
     sp.row_ptr.resize(n + 1);
-    sp.col.resize(nnz + 4);                   // +4: the bulk-copy SpMV's last chunk is rounded up to 4
-    sp.val.resize(nnz + 4);
-    sp.val32.resize(nnz + 4);
-    sp.err.resize(1);
-    MOMED_CUDA_TRY(cudaMemsetAsync(sp.err.p, 0, sizeof(unsigned long long), st));
+    sp.col.resize(std::max<int64_t>(nnz, 1));
+    sp.val.resize(std::max<int64_t>(nnz, 1));
+    sp.val32.resize(std::max<int64_t>(nnz, 1));
     MOMED_CUDA_TRY(cudaMemcpyAsync(sp.row_ptr.p, row_ptr, (n + 1) * 8, cudaMemcpyHostToDevice, st));
     if (nnz > 0) {
         MOMED_CUDA_TRY(cudaMemcpyAsync(sp.col.p, col, nnz * 4, cudaMemcpyHostToDevice, st));
@@ -573,56 +440,8 @@ void upload_sparse(momed_handle* h, int64_t n, const int64_t* row_ptr, const int
     sp.built = true;
 }
 
-// MOMED_SPMV_BULK=1: the bulk-copy SpMV (k_spmv_bulk) for the single-vector maps
-bool spmv_bulk() {
-    static int on = -1;
-    if (on < 0) {
-        const char* e = std::getenv("MOMED_SPMV_BULK");
-        on = (e && e[0] == '1') ? 1 : 0;
-    }
-    return on == 1;
-}
-
-template <typename R>
-void launch_spmv_bulk(const SparseMatrix& sp, const typename SpVal<R>::T* val, const typename SpVal<R>::T* x,
-                      typename SpVal<R>::T* y, int64_t rows, cudaStream_t st) {
-    auto k = k_spmv_bulk<R>;
-    const int smem = kSpWarps * 2 * kSpChunk * (4 + (int)sizeof(typename SpVal<R>::T));
-    MOMED_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    int per_sm = 0;
-    MOMED_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kSpWarps * 32, smem));
-    const int64_t warps_needed = (rows + 15) / 16;              // at least 16 rows per warp
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * std::max(per_sm, 1),
-                                                                  (warps_needed + kSpWarps - 1) / kSpWarps));
-    k<<<grid, kSpWarps * 32, smem, st>>>(sp.row_ptr.p, sp.col.p, val, x, y, rows, sp.err.p);
-}
-
-void check_spmv_status(const SparseMatrix& sp, cudaStream_t st) {
-    if (!sp.built || !sp.err.p || !spmv_bulk()) return;
-    unsigned long long e = 0;
-    MOMED_CUDA_TRY(cudaMemcpyAsync(&e, sp.err.p, sizeof(e), cudaMemcpyDeviceToHost, st));
-    MOMED_CUDA_TRY(cudaStreamSynchronize(st));
-    if (e != 0) {
-        MOMED_CUDA_TRY(cudaMemsetAsync(sp.err.p, 0, sizeof(e), st));
-        throw Error{MOMED_ECUDA, "sparse SpMV: " + std::to_string(e) + " bulk-copy waits ran out"};
-    }
-}
-
 void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
-    if (spmv_bulk() && sp.err.p) {
-        launch_spmv_bulk<double>(sp, sp.val.p, x, y, rows, st);
-        MOMED_CUDA_TRY(cudaGetLastError());
-        note_launches(1);
-        return;
-    }
     if (spmv_stream()) k_spmv<double, true><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val.p, x, y, rows);
     else k_spmv<double, false><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val.p, x, y, rows);
     MOMED_CUDA_TRY(cudaGetLastError());
@@ -631,12 +450,6 @@ void launch_spmv_c128(const SparseMatrix& sp, const double2* x, double2* y, int6
 
 void launch_spmv_c64(const SparseMatrix& sp, const float2* x, float2* y, int64_t rows, cudaStream_t st) {
     if (rows <= 0) return;
-    if (spmv_bulk() && sp.err.p) {
-        launch_spmv_bulk<float>(sp, sp.val32.p, x, y, rows, st);
-        MOMED_CUDA_TRY(cudaGetLastError());
-        note_launches(1);
-        return;
-    }
     if (spmv_stream()) k_spmv<float, true><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val32.p, x, y, rows);
     else k_spmv<float, false><<<spmv_grid(rows), kWarps * 32, 0, st>>>(sp.row_ptr.p, sp.col.p, sp.val32.p, x, y, rows);
     MOMED_CUDA_TRY(cudaGetLastError());
