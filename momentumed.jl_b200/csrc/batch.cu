@@ -875,7 +875,7 @@ struct GramRhs {
     const double2* p[kGramRhs];
 };
 template <typename VT, int NB>
-__global__ void __launch_bounds__(kT)
+__global__ void __launch_bounds__(kT, 4)
 k_bgram(const VT* __restrict__ V, int64_t N, int ncols, GramRhs R, int nr, double2* __restrict__ partial) {
     using P = Pack<VT, NB>;
     constexpr int E = P::E;
@@ -923,6 +923,29 @@ k_bgram(const VT* __restrict__ V, int64_t N, int ncols, GramRhs R, int nr, doubl
                 partial[(((int64_t)blockIdx.x * kGramRhs + j) * ncols + i) * NB + rp * E + q] = make_double2(sx, sy);
         }
     }
+}
+
+// Row blocks of k_bgram: one wave of the CTAs that are resident at once over the ncols / 8
+// column groups (measured: a grid of 0.67 or 3 waves left the SMs a third idle or ran a partial
+// last wave), at least one row tile each, at most cap.
+constexpr int kGramBlocksPerSm = 8;
+template <int NB>
+int gram_rowblocks_t(int64_t N, int ncols, bool fp32, int cap) {
+    static int per_sm[2] = {0, 0};
+    int& ps = per_sm[fp32 ? 1 : 0];
+    if (ps == 0) {
+        if (fp32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_bgram<float2, NB>, kT, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_bgram<double2, NB>, kT, 0);
+        if (ps <= 0) ps = 1;
+    }
+    int sm = 0, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
+    if (sm <= 0) sm = 148;
+    const int groups = std::max(1, (ncols + 7) / 8);
+    int rb = std::max(1, ps * sm / groups);
+    rb = (int)std::min<int64_t>(rb, (N + rows_tile<NB>() - 1) / rows_tile<NB>());
+    return std::max(1, std::min(rb, cap));
 }
 
 // out[e] = sum over blocks b < grid of partial[b * bstride + e] for e < count, one warp per
@@ -1139,7 +1162,10 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
             W2.resize((size_t)k1 * stride);
             // Gram partials [row block][kGramRhs][columns][NB] and the summed blocks [2 k1][columns][NB]
             DevBuf<double2> gpart, gx, gq;
-            gpart.resize((size_t)LR.grid * kGramRhs * std::max(k1, m - k1) * NB);
+            // Gram row blocks: one wave of resident CTAs over all column groups (occupancy of
+            // k_bgram), up to kGramBlocksPerSm per SM; the partial buffer holds that many
+            const int gram_cap = kGramBlocksPerSm * sms();
+            gpart.resize((size_t)gram_cap * kGramRhs * std::max(k1, m - k1) * NB);
             const size_t gx_n = (size_t)2 * k1 * k1 * NB, gq_n = (size_t)2 * k1 * (m - k1) * NB;
             gx.resize(gx_n);
             gq.resize(gq_n);
@@ -1218,7 +1244,7 @@ int run_batch(momed_handle* h, const momed_solve_opts* o, const double* u, int32
                 // 2 k1 right-hand sides (W_i, then X_i) go kGramRhs at a time
                 const int nrhs = 2 * k1;
                 auto gram = [&](const void* cols, bool fp32, int ncols, int g0, int nr, double2* out) {
-                    const int rb = bproj_rowblocks(N, ncols, sms(), LR.grid, rows_tile<NB>());
+                    const int rb = gram_rowblocks_t<NB>(N, ncols, fp32, gram_cap);
                     GramRhs R{};
                     for (int j = 0; j < nr; ++j)
                         R.p[j] = (g0 + j < k1 ? Wb.p + (size_t)(g0 + j) * stride : Xb.p + (size_t)(g0 + j - k1) * stride);
