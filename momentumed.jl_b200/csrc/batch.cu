@@ -574,9 +574,18 @@ struct BlockLanczos {
         using ACC = typename std::conditional<f32, float, double>::type;
         constexpr int RPT = f32 ? 4 : 2;
         constexpr int TR = (kT / NB) * RPT;
-        auto k = k_bcombine<VT, VOUT, ACC, NB, RPT, 8>;
-        int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms() * 8));
-        k<<<g, kT, 0, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
+        if (f32 && nout > 8 && nout <= 16) {
+            // 9..16 outputs (the headline restart keeps 12): one pass over V with 16 outputs per
+            // thread and 2 rows, instead of two passes of 8 outputs and 4 rows
+            auto k = k_bcombine<VT, VOUT, ACC, NB, 2, 16>;
+            constexpr int TR2 = (kT / NB) * 2;
+            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR2 - 1) / TR2, (int64_t)sms() * 8));
+            k<<<g, kT, 0, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
+        } else {
+            auto k = k_bcombine<VT, VOUT, ACC, NB, RPT, 8>;
+            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms() * 8));
+            k<<<g, kT, 0, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
+        }
         MOMED_CUDA_TRY(cudaGetLastError());
         MOMED_CUDA_TRY(cudaStreamSynchronize(st));
         ++launches;
@@ -837,16 +846,45 @@ k_bcombine_xq(const double2* __restrict__ X, int kx, const double2* __restrict__
             for (int j = 0; j < RPT; ++j)
 #pragma unroll
                 for (int k = 0; k < OC; ++k) { ax[j][k] = 0.0; ay[j][k] = 0.0; }
-            for (int a = 0; a < d; ++a) {
+            {
+                // the FP32 extension Q in FP32 arithmetic (its values carry FP32 rounding already;
+                // the products add an error of the same order), summed into the FP64 sums after
+                float fx[RPT][OC], fy[RPT][OC];
+#pragma unroll
+                for (int j = 0; j < RPT; ++j)
+#pragma unroll
+                    for (int k = 0; k < OC; ++k) { fx[j][k] = 0.f; fy[j][k] = 0.f; }
+                for (int a = kx + kz; a < d; ++a) {
+                    float2 y[OC];
+#pragma unroll
+                    for (int k = 0; k < OC; ++k) {
+                        const double2 yd = (c0 + k < nout) ? __ldg(Y + ((int64_t)(c0 + k) * d + a) * NB + r)
+                                                           : make_double2(0.0, 0.0);
+                        y[k] = make_float2((float)yd.x, (float)yd.y);
+                    }
+#pragma unroll
+                    for (int j = 0; j < RPT; ++j) {
+                        const float2 v = Q[(int64_t)(a - kx - kz) * stride + off[j]];
+#pragma unroll
+                        for (int k = 0; k < OC; ++k) {
+                            fx[j][k] += y[k].x * v.x - y[k].y * v.y;
+                            fy[j][k] += y[k].x * v.y + y[k].y * v.x;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < RPT; ++j)
+#pragma unroll
+                    for (int k = 0; k < OC; ++k) { ax[j][k] = (double)fx[j][k]; ay[j][k] = (double)fy[j][k]; }
+            }
+            for (int a = 0; a < kx + kz; ++a) {            // the FP64 anchors X (and Z)
                 double2 y[OC];
 #pragma unroll
                 for (int k = 0; k < OC; ++k)
                     y[k] = (c0 + k < nout) ? __ldg(Y + ((int64_t)(c0 + k) * d + a) * NB + r) : make_double2(0.0, 0.0);
 #pragma unroll
                 for (int j = 0; j < RPT; ++j) {
-                    const double2 v = a < kx        ? X[(int64_t)a * stride + off[j]]
-                                      : a < kx + kz ? Z[(int64_t)(a - kx) * stride + off[j]]
-                                                    : to2(Q[(int64_t)(a - kx - kz) * stride + off[j]]);
+                    const double2 v = a < kx ? X[(int64_t)a * stride + off[j]] : Z[(int64_t)(a - kx) * stride + off[j]];
 #pragma unroll
                     for (int k = 0; k < OC; ++k) {
                         ax[j][k] += y[k].x * v.x - y[k].y * v.y;
