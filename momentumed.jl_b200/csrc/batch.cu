@@ -574,18 +574,11 @@ struct BlockLanczos {
         using ACC = typename std::conditional<f32, float, double>::type;
         constexpr int RPT = f32 ? 4 : 2;
         constexpr int TR = (kT / NB) * RPT;
-        if (f32 && nout > 8 && nout <= 16) {
-            // 9..16 outputs (the headline restart keeps 12): one pass over V with 16 outputs per
-            // thread and 2 rows, instead of two passes of 8 outputs and 4 rows
-            auto k = k_bcombine<VT, VOUT, ACC, NB, 2, 16>;
-            constexpr int TR2 = (kT / NB) * 2;
-            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR2 - 1) / TR2, (int64_t)sms() * 8));
-            k<<<g, kT, 0, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
-        } else {
-            auto k = k_bcombine<VT, VOUT, ACC, NB, RPT, 8>;
-            int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms() * 8));
-            k<<<g, kT, 0, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
-        }
+        // (one pass of 16 outputs and 2 rows per thread for 9..16 outputs was slower: 1.61 against
+        // 1.21 ms for the headline restart's 12)
+        auto k = k_bcombine<VT, VOUT, ACC, NB, RPT, 8>;
+        int g = (int)std::max<int64_t>(1, std::min<int64_t>((N + TR - 1) / TR, (int64_t)sms() * 8));
+        k<<<g, kT, 0, st>>>(V.p, N, mm, Ud.p, nout, out, copy_col);
         MOMED_CUDA_TRY(cudaGetLastError());
         MOMED_CUDA_TRY(cudaStreamSynchronize(st));
         ++launches;
