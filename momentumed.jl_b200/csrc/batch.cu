@@ -525,7 +525,17 @@ struct BlockLanczos {
     VT* col(int i) { return V.p + (size_t)i * N * NB; }
 
     void proj(int ncols, const VT* w, double2* out, const int* act) {
-        const int rb = bproj_rowblocks(N, ncols, sms(), grid, rows_tile<NB>());
+        // one full wave of resident CTAs over all column groups (measured: 1.5 waves left the
+        // second half-wave's SMs idle at the end of every projection)
+        static int per_sm = 0;
+        if (per_sm == 0) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bproj<VT, VT, NB>, kT, 0);
+            if (per_sm <= 0) per_sm = 1;
+        }
+        const int groups = std::max(1, (ncols + 7) / 8);
+        int rb = std::max(1, per_sm * sms() / groups);
+        rb = (int)std::min<int64_t>(rb, (N + rows_tile<NB>() - 1) / rows_tile<NB>());
+        rb = std::max(1, std::min(rb, grid));
         k_bproj<VT, VT, NB><<<bproj_grid(rb, ncols), kT, 0, st>>>(V.p, N, ncols, w, partial.p, act);
         k_breduce<NB><<<breduce_grid(ncols + 1, NB), 256, 0, st>>>(partial.p, rb, ncols + 1, out, act);
         launches += 2;
