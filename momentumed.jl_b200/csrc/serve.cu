@@ -292,6 +292,7 @@ void worker_loop(momed_server* S, int slot) {
             // candidate map.  A group's batched solver runs its FP32 maps over the cache (or as a
             // block SpMV over the matrix).  MOMED_SERVE_HITCACHE=0 / MOMED_SERVE_SPARSE=0 skip one.
             int64_t sp_bytes = 0, hc_bytes = 0;
+            int hc_mode = 1;
             if (N >= kSparseMinRows) {
                 ensure_ready(h);                      // index and validation: h->nnz counts every hit
                 std::lock_guard<std::mutex> lk(S->mu);
@@ -310,6 +311,17 @@ void worker_loop(momed_server* S, int slot) {
                         sp_bytes = need;
                     }
                 }
+                // neither fits (the 35M-state sectors): the cache's slot mode, 2 bytes per hit,
+                // for the single-vector map
+                if (hc_bytes == 0 && sp_bytes == 0 && h->op.nterms <= 65536 &&
+                    knob("MOMED_SERVE_HITCACHE", "1") != "0") {
+                    const int64_t need = slot_cache_bytes(N, h->nnz);
+                    if (S->used + need <= S->budget) {
+                        S->used += need;
+                        hc_bytes = need;
+                        hc_mode = 2;
+                    }
+                }
             }
             auto unreserve = [&]() {
                 h->sparse.release();
@@ -323,7 +335,7 @@ void worker_loop(momed_server* S, int slot) {
             try {
                 if (hc_bytes > 0) {
                     try {
-                        build_hit_cache(h);
+                        build_hit_cache(h, hc_mode);
                     } catch (const Error& e) {
                         if (e.code != MOMED_ENOMEM) throw;
                         unreserve();          // the device is shorter than the budget: candidate map
@@ -344,7 +356,10 @@ void worker_loop(momed_server* S, int slot) {
                     // 4.35 served solves/s against 3.98 with FP64 for every request alone,
                     // eigenvalues within 4e-13 of FP64).  MOMED_SERVE_ALONE=fp64 gives every
                     // request alone FP64 arithmetic.
-                    const bool alone_mixed = knob("MOMED_SERVE_ALONE", "mixed") == "mixed";
+                    // (over a slot-mode cache the batched solver's block maps would fall back to the
+                    // candidate map, so such a request runs FP64 on the single-vector map)
+                    const bool alone_mixed = knob("MOMED_SERVE_ALONE", "mixed") == "mixed" &&
+                                             !(h->hcache.built && h->hcache.mode == 2);
                     o.precision = (alone_mixed && r->opts.precision == MOMED_PREC_MIXED) ? MOMED_PREC_MIXED
                                                                                          : MOMED_PREC_FP64;
                     rc = momed_eigsolve_impl(h, &o, nullptr, gvals.data(), gres.data(), nullptr, &ginfo);

@@ -196,8 +196,9 @@ def test_queued_requests_on_one_sector_are_batched(workload):
 
 def test_sparse_method_and_map_fallback_by_budget(workload):
     """A 3x8 request (~30k states) is solved over the map's hit cache when it fits the budget, on
-    the sparse method when the cache is switched off and the matrix fits, and on the candidate map
-    when only the Krylov state fits: the same eigenvalues every way."""
+    the sparse method when the cache is switched off and the matrix fits, and over the cache's slot
+    mode when neither fits (96 MB: ~50 MB for the solve, ~50 MB for a full cache, ~265 MB for the
+    matrix, ~14 MB for the slots): the same eigenvalues every way."""
     p35, p38, b35, b38 = workload
     vals = {}
     for budget, knobs in ((8 << 30, {}), (8 << 30, {"MOMED_SERVE_HITCACHE": "0"}), (96 << 20, {})):
