@@ -170,6 +170,38 @@ def test_solvers_over_the_cache_vs_lapack(setup):
     assert np.max(np.abs(vals1 - w) / np.abs(w)) < 1e-10
 
 
+def test_block_map_at_32_right_hand_sides(setup):
+    """The 32-wide block map of the batched solver (FP32 Lanczos and FP64 checks) over the cache
+    against LAPACK and against the candidate block map; with a B part (32 parameter values) and
+    without one (the operator set as one term list, all right-hand sides the same matrix)."""
+    h, basis, pair = setup
+    us = np.linspace(0.5, 2.0, 32)
+    nev = 3
+    ref = {i: np.linalg.eigvalsh(dense(basis, pair, us[i]))[:nev] for i in (0, 13, 31)}
+    res = {}
+    for flag in ("1", "0"):
+        with env(MOMED_HITCACHE=flag):
+            h.set_basis(basis)
+            vals, _, _, _ = h.batch_solve(us, nev, krylovdim=24, tol=1e-12, precision=_lib.PREC_MIXED)
+        assert vals.shape == (32, nev)
+        for i, r in ref.items():
+            assert np.max(np.abs(vals[i] - r) / np.abs(r)) < 1e-10
+        res[flag] = vals
+    assert np.max(np.abs(res["1"] - res["0"]) / np.abs(res["0"])) < 1e-12
+
+    a2, b2, in_, out, pm = pair
+    u = 1.1
+    w = np.linalg.eigvalsh(dense(basis, pair, u))[:nev]
+    h.set_scatter(a2 + u * b2, in_, out, pm)
+    try:
+        with env(MOMED_HITCACHE=1):
+            vals, _, _, _ = h.batch_solve(us, nev, krylovdim=24, tol=1e-12, precision=_lib.PREC_MIXED)
+        assert np.max(np.abs(vals - w[None, :]) / np.abs(w[None, :])) < 1e-10
+    finally:
+        h.set_scatter_pair(*pair)
+        h.set_basis(basis)
+
+
 def test_slot_mode_matches_full_cache(setup):
     """Slot mode (term slot per hit, the target formed at each application): the same hits as
     the full cache and the same products."""
