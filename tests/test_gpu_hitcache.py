@@ -10,7 +10,9 @@ Bars:
   - complex128 map within 1e-13 relative of the candidate map and of the dense product
     (same values, another summation order), complex64 within 2e-6;
   - the cache holds exactly the off-diagonal entries of the sparse method's matrix;
-  - eigenvalues within 1e-10 relative of LAPACK and 1e-12 of the solves without the cache.
+  - eigenvalues within 1e-10 relative of LAPACK and 1e-11 of the solves without the cache (the
+    batched solves converge to tol 1e-12; a near-degenerate pair, as the sixth and fifth levels
+    here, 6.0492 / 6.0477, moves by a few 1e-12 with the summation order).
 """
 import os
 from contextlib import contextmanager
@@ -155,7 +157,7 @@ def test_solvers_over_the_cache_vs_lapack(setup):
             for r, v in zip(ref, vals):
                 assert np.max(np.abs(v - r) / np.abs(r)) < 1e-10
             res[flag] = vals
-    assert np.max(np.abs(res["1"] - res["0"]) / np.abs(res["0"])) < 1e-12
+    assert np.max(np.abs(res["1"] - res["0"]) / np.abs(res["0"])) < 1e-11
 
     # block Lanczos (c128 block maps over the cache) and the single-vector solver
     h.set_basis(basis)
@@ -187,7 +189,7 @@ def test_block_map_at_32_right_hand_sides(setup):
         for i, r in ref.items():
             assert np.max(np.abs(vals[i] - r) / np.abs(r)) < 1e-10
         res[flag] = vals
-    assert np.max(np.abs(res["1"] - res["0"]) / np.abs(res["0"])) < 1e-12
+    assert np.max(np.abs(res["1"] - res["0"]) / np.abs(res["0"])) < 1e-11
 
     a2, b2, in_, out, pm = pair
     u = 1.1
