@@ -644,10 +644,18 @@ void build_hit_cache(momed_handle* h, int mode) {
     hc.built = true;
 }
 
+// The automatic build is an optimisation: when its allocations are refused (memory taken by
+// another handle between the size check and the build) the solve goes on over the candidate map.
 void ensure_hit_cache(momed_handle* h) {
     if (h->hcache.built) return;
     const int mode = hit_cache_wanted(h);
-    if (mode) build_hit_cache(h, mode);
+    if (!mode) return;
+    try {
+        build_hit_cache(h, mode);
+    } catch (const Error& e) {
+        if (e.code != MOMED_ENOMEM) throw;
+        h->hcache.release();
+    }
 }
 
 template <typename R> struct CombSlot;
