@@ -137,14 +137,6 @@ k_bproj(const VT* __restrict__ V, int64_t N, int ncols, const WT* __restrict__ W
     }
 }
 
-// Row blocks of k_bproj for ncols columns: about 6 blocks per SM over all column groups, between
-// 1 and 4 per SM, never more than the row tiles; maxrb (the partial buffer's capacity) caps it.
-inline int bproj_rowblocks(int64_t N, int ncols, int sm, int maxrb, int tile_rows) {
-    const int groups = std::max(1, (ncols + 7) / 8);
-    int rb = std::max(sm, std::min(4 * sm, 6 * sm / groups));
-    rb = (int)std::min<int64_t>(rb, (N + tile_rows - 1) / tile_rows);
-    return std::max(1, std::min(rb, maxrb));
-}
 inline dim3 bproj_grid(int rowblocks, int ncols) { return dim3(rowblocks, (unsigned)std::max(1, (ncols + 7) / 8)); }
 
 __device__ __forceinline__ double wsum(double v) {
@@ -429,6 +421,7 @@ struct BlockLanczos {
     int m;
     cudaStream_t st;
     int grid, ugrid;
+    int last_ugrid = 1;   // CTAs of the latest update: the count of its norm partials
     DevBuf<VT> V, V2;
     DevBuf<double2> partial, coefA, coefB;
     DevBuf<double> npart, after, scal, alpha, beta, Ud;
@@ -542,9 +535,19 @@ struct BlockLanczos {
     }
     void update(int ncols, const double2* coef, VT* w, const int* active, const int* act) {
         size_t smem = (size_t)ncols * NB * sizeof(double2);
-        // the shared-memory attribute (process-wide, always the largest size) is set by the constructor
-        k_bupdate<VT, NB><<<ugrid, kT, smem, st>>>(V.p, N, ncols, coef, w, npart.p, active, act);
+        // one wave of resident CTAs (their count depends on the coefficients' shared memory); the
+        // shared-memory attribute (process-wide, always the largest size) is set by the constructor
+        static int per_sm[kMaxCols + 1] = {};
+        const int nc = std::min(std::max(ncols, 0), kMaxCols);
+        if (per_sm[nc] == 0) {
+            int b = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_bupdate<VT, NB>, kT, smem);
+            per_sm[nc] = std::max(b, 1);
+        }
+        const int g = std::max(1, std::min(ugrid, per_sm[nc] * sms()));
+        k_bupdate<VT, NB><<<g, kT, smem, st>>>(V.p, N, ncols, coef, w, npart.p, active, act);
         ++launches;
+        last_ugrid = g;
     }
     // column k0 made orthogonal to columns [0, k0) (two classical Gram-Schmidt passes), then normalised
     void orth_start(int k0) {
@@ -567,11 +570,11 @@ struct BlockLanczos {
         const int nc = j + 1;
         proj(nc, w, coefA.p, nullptr);
         update(nc, coefA.p, w, nullptr, nullptr);
-        k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, ugrid, flag.p, any.p, after.p, dgks);
+        k_bdecide<NB><<<1, NB * 32, 0, st>>>(coefA.p, nc, npart.p, last_ugrid, flag.p, any.p, after.p, dgks);
         ++launches;
         proj(nc, w, coefB.p, any.p);
         update(nc, coefB.p, w, flag.p, any.p);
-        k_bfinalize<NB><<<1, NB * 32, 0, st>>>(coefA.p, coefB.p, nc, npart.p, ugrid, flag.p, any.p, after.p, scal.p,
+        k_bfinalize<NB><<<1, NB * 32, 0, st>>>(coefA.p, coefB.p, nc, npart.p, last_ugrid, flag.p, any.p, after.p, scal.p,
                                           alpha.p, beta.p, j, m);
         k_bscale<VT, NB><<<ugrid, kT, 0, st>>>(w, N, scal.p);
         launches += 2;
