@@ -471,7 +471,7 @@ struct BlockKrylov {
             d = std::max(d, std::hypot(a[i].x - b[i].x, a[i].y - b[i].y));
         }
         // scale: the largest coefficient or the largest column norm of W (|q^H w| <= |w|), so that
-        // the tiny coefficients of a second Gram-Schmidt pass are judged against |w|
+        // the tiny coefficients of a second Gram-Schmidt pass are compared with |w|
         proj_cuda(W, B, W, ref.p);
         std::vector<double2> g((size_t)B * B);
         MOMED_CUDA_TRY(cudaMemcpyAsync(g.data(), ref.p, g.size() * sizeof(double2), cudaMemcpyDeviceToHost, st));
