@@ -82,7 +82,11 @@ def _split_top(s: str):
 
 
 def shim_ccalls():
-    src = open(SHIM).read()
+    return ccalls_in(open(SHIM).read())
+
+
+def ccalls_in(src: str):
+    """(name, Julia return type, [Julia argument types], [arguments]) of every ccall in src."""
     src = "\n".join(l.split("#", 1)[0] if not l.lstrip().startswith("#") else "" for l in src.splitlines())
     calls = []
     for m in re.finditer(r"ccall\(", src):
