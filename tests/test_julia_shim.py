@@ -134,3 +134,39 @@ def test_header_parser_sees_every_exported_symbol():
     sys.path.insert(0, os.path.join(ROOT, "momentumed.jl_b200"))
     from momed import _lib
     assert set(header_prototypes()) == set(_lib.SIGNATURES)
+
+
+def header_structs():
+    """{struct name: [(field, C type)]} of the header's typedef'd structs, in declaration order."""
+    src = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"typedef\s+struct\s*\{(.*?)\}\s*(\w+)\s*;", src, flags=re.S):
+        fields = []
+        for decl in m.group(1).split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            tm = re.match(r"((?:const\s+)?\w+\s*\**)\s*(.*)", decl)
+            ctype = _norm(tm.group(1))
+            for nm in tm.group(2).split(","):
+                nm = nm.strip()
+                star = "*" * nm.count("*")
+                fields.append((nm.strip("* "), _norm(ctype + star)))
+        out[m.group(2)] = fields
+    return out
+
+
+def test_shim_structs_match_the_header():
+    """The shim's MomedPara / MomedSolveOpts / MomedInfo: same fields, order and widths as C."""
+    c_to_jl = {"int32_t": "Int32", "int64_t": "Int64", "uint64_t": "UInt64", "double": "Float64",
+               "const int64_t*": "Ptr{Int64}"}
+    src = open(SHIM).read()
+    hs = header_structs()
+    for cname, jname in (("momed_para", "MomedPara"), ("momed_solve_opts", "MomedSolveOpts"),
+                         ("momed_info", "MomedInfo")):
+        m = re.search(r"(?:mutable\s+)?struct\s+" + jname + r"\s*\n(.*?)\nend", src, flags=re.S)
+        assert m, jname
+        jf = [tuple(x.strip() for x in l.split("::")) for l in m.group(1).splitlines() if "::" in l]
+        assert [f for f, _ in jf] == [f for f, _ in hs[cname]], jname
+        for (f, jt), (_, ct) in zip(jf, hs[cname]):
+            assert c_to_jl[ct] == jt, f"{jname}.{f}: {jt} vs C {ct}"
