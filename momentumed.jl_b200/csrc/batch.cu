@@ -14,6 +14,7 @@
 // sides whose estimated eigenvalue error stays above the target are finished by an
 // FP64 single-vector Lanczos warm-started from their refined vectors.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cmath>
 #include <complex>
@@ -372,13 +373,12 @@ __global__ void k_extract(const double2* src, int64_t N, int k, int r, double2* 
 }
 
 int sms() {
-    static int s = 0;
-    if (!s) {
-        int d = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, d);
-        if (s <= 0) s = 148;
-    }
+    static const int s = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();   // thread-safe first use (serving slots call concurrently)
     return s;
 }
 
@@ -520,10 +520,12 @@ struct BlockLanczos {
     void proj(int ncols, const VT* w, double2* out, const int* act) {
         // one full wave of resident CTAs over all column groups (measured: 1.5 waves left the
         // second half-wave's SMs idle at the end of every projection)
-        static int per_sm = 0;
+        static std::atomic<int> per_sm_cache{0};
+        int per_sm = per_sm_cache.load(std::memory_order_relaxed);
         if (per_sm == 0) {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_bproj<VT, VT, NB>, kT, 0);
             if (per_sm <= 0) per_sm = 1;
+            per_sm_cache.store(per_sm, std::memory_order_relaxed);
         }
         const int groups = std::max(1, (ncols + 7) / 8);
         int rb = std::max(1, per_sm * sms() / groups);
@@ -537,14 +539,16 @@ struct BlockLanczos {
         size_t smem = (size_t)ncols * NB * sizeof(double2);
         // one wave of resident CTAs (their count depends on the coefficients' shared memory); the
         // shared-memory attribute (process-wide, always the largest size) is set by the constructor
-        static int per_sm[kMaxCols + 1] = {};
+        static std::atomic<int> per_sm_cache[kMaxCols + 1];   // zero before first use (static storage)
         const int nc = std::min(std::max(ncols, 0), kMaxCols);
-        if (per_sm[nc] == 0) {
+        int per_sm = per_sm_cache[nc].load(std::memory_order_relaxed);
+        if (per_sm == 0) {
             int b = 0;
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_bupdate<VT, NB>, kT, smem);
-            per_sm[nc] = std::max(b, 1);
+            per_sm = std::max(b, 1);
+            per_sm_cache[nc].store(per_sm, std::memory_order_relaxed);
         }
-        const int g = std::max(1, std::min(ugrid, per_sm[nc] * sms()));
+        const int g = std::max(1, std::min(ugrid, per_sm * sms()));
         k_bupdate<VT, NB><<<g, kT, smem, st>>>(V.p, N, ncols, coef, w, npart.p, active, act);
         ++launches;
         last_ugrid = g;
@@ -975,12 +979,13 @@ k_bgram(const VT* __restrict__ V, int64_t N, int ncols, GramRhs R, int nr, doubl
 constexpr int kGramBlocksPerSm = 8;
 template <int NB>
 int gram_rowblocks_t(int64_t N, int ncols, bool fp32, int cap) {
-    static int per_sm[2] = {0, 0};
-    int& ps = per_sm[fp32 ? 1 : 0];
+    static std::atomic<int> per_sm[2];   // zero before first use (static storage)
+    int ps = per_sm[fp32 ? 1 : 0].load(std::memory_order_relaxed);
     if (ps == 0) {
         if (fp32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_bgram<float2, NB>, kT, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ps, k_bgram<double2, NB>, kT, 0);
         if (ps <= 0) ps = 1;
+        per_sm[fp32 ? 1 : 0].store(ps, std::memory_order_relaxed);
     }
     int sm = 0, dev = 0;
     cudaGetDevice(&dev);

@@ -343,13 +343,12 @@ __global__ void k_bl_add(const double2* __restrict__ a, const double2* __restric
 }
 
 int blk_sms() {
-    static int s = 0;
-    if (!s) {
-        int d = 0;
-        cudaGetDevice(&d);
-        cudaDeviceGetAttribute(&s, cudaDevAttrMultiProcessorCount, d);
-        if (s <= 0) s = 148;
-    }
+    static const int s = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();
     return s;
 }
 

@@ -153,13 +153,12 @@ __device__ __forceinline__ int64_t eval_term(int f, int& gi, uint64_t s, int64_t
 
 template <typename K>
 int persistent_grid(K kernel, int64_t rows) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, v = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, 0);
     if (per_sm <= 0) per_sm = 1;

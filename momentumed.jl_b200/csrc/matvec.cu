@@ -454,23 +454,21 @@ std::mutex g_tune_mu;
 std::map<TuneKey, TuneChoice> g_tune;
 
 bool autotune_enabled() {
-    static int on = -1;
-    if (on < 0) {
+    static const bool on = [] {
         const char* e = std::getenv("MOMED_AUTOTUNE");
-        on = (e && e[0] == '0') ? 0 : 1;
-    }
-    return on == 1;
+        return !(e && e[0] == '0');
+    }();
+    return on;
 }
 
 template <typename K>
 int tuned_grid(K kernel, int64_t rows, int rpw, int mult) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, v = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kWarps * 32, 0);
     if (per_sm <= 0) per_sm = 1;

@@ -310,22 +310,20 @@ __global__ void k_round_c64(const double2* __restrict__ v, float2* __restrict__ 
 
 // MOMED_SPMV_STREAM=0 reads the column and value arrays through L1 like the x gathers
 bool spmv_stream() {
-    static int on = -1;
-    if (on < 0) {
+    static const bool on = [] {
         const char* e = std::getenv("MOMED_SPMV_STREAM");
-        on = (e && e[0] == '0') ? 0 : 1;
-    }
-    return on == 1;
+        return !(e && e[0] == '0');
+    }();
+    return on;
 }
 
 int spmv_grid(int64_t rows) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, v = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();
     int64_t need = (rows + kWarps - 1) / kWarps;
     return (int)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * 8));   // 8 blocks of 8 warps per SM
 }

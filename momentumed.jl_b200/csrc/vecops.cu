@@ -283,13 +283,12 @@ __global__ void k_residual(const double2* W, const double2* X, int64_t N, int k,
 }
 
 int sm_count() {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
+    static const int sms = [] {
+        int dev = 0, v = 0;
         cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        return v > 0 ? v : 148;
+    }();
     return sms;
 }
 
