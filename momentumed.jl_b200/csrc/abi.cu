@@ -18,8 +18,13 @@ using namespace momed;
 namespace momed {
 
 static std::atomic<int64_t> g_launches{0};
-void note_launches(int64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+static thread_local int64_t t_launches = 0;   // this thread's share (graph captures count their own)
+void note_launches(int64_t n) {
+    g_launches.fetch_add(n, std::memory_order_relaxed);
+    t_launches += n;
+}
 int64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+int64_t launches_this_thread() { return t_launches; }
 
 // Fold the elapsed time of recorded event pairs into prof_ms and recycle them.
 static void prof_drain(momed_handle* h) {

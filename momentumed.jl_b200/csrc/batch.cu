@@ -458,7 +458,7 @@ struct BlockLanczos {
                     ++graph_replays;
                     return;
                 }
-            const int64_t l0 = launches_total();
+            const int64_t l0 = launches_this_thread();   // other threads (serving slots) launch meanwhile
             cudaGraph_t graph = nullptr;
             MOMED_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             bool ok = true;
@@ -471,7 +471,7 @@ struct BlockLanczos {
             cudaGraphExec_t exec = nullptr;
             if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
                 cudaGraphDestroy(graph);
-                graphs.push_back({k, V.p, exec, launches_total() - l0});
+                graphs.push_back({k, V.p, exec, launches_this_thread() - l0});
                 MOMED_CUDA_TRY(cudaGraphLaunch(exec, st));
                 ++graph_replays;
                 return;

@@ -400,6 +400,7 @@ void prof_end(momed_handle* h, int kind);
 // process-wide count of kernel launches issued by this library (diagnostics)
 void note_launches(int64_t n);
 int64_t launches_total();
+int64_t launches_this_thread();   // launches noted by the calling thread
 
 // small dense symmetric eigensolver (host, FP64): A n x n row-major (destroyed),
 // eigenvalues ascending in w, eigenvectors as columns of V (row-major n x n)
