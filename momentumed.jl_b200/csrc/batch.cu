@@ -458,7 +458,10 @@ struct BlockLanczos {
                     ++graph_replays;
                     return;
                 }
-            const int64_t l0 = launches_this_thread();   // other threads (serving slots) launch meanwhile
+            // the graph's kernels: those its launchers note at once (the maps) plus those this
+            // solver counts in `launches` (noted when the solve ends); other threads' launches
+            // (serving slots) do not enter
+            const int64_t l0 = launches_this_thread(), own0 = launches;
             cudaGraph_t graph = nullptr;
             MOMED_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             bool ok = true;
@@ -471,7 +474,7 @@ struct BlockLanczos {
             cudaGraphExec_t exec = nullptr;
             if (ok && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
                 cudaGraphDestroy(graph);
-                graphs.push_back({k, V.p, exec, launches_this_thread() - l0});
+                graphs.push_back({k, V.p, exec, (launches_this_thread() - l0) + (launches - own0)});
                 MOMED_CUDA_TRY(cudaGraphLaunch(exec, st));
                 ++graph_replays;
                 return;
