@@ -413,9 +413,7 @@ __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpVi
     constexpr int RPL = IO::RPL, LPH = IO::LPH, HPI = IO::HPI;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int hslot = lane / LPH, kk = lane % LPH;
-    R ur[RPL];
-#pragma unroll
-    for (int q = 0; q < RPL; ++q) ur[q] = HAS_B ? __ldg(u + IO::rhs(kk, q)) : R(0);
+    auto urq = [&](int q) { return HAS_B ? __ldg(u + IO::rhs(kk, q)) : R(0); };
     const C2* __restrict__ A = amp_a<R>(ov);
     const C2* __restrict__ B = amp_b<R>(ov);
     const C2* __restrict__ dg = hc_diag<R>(hv);
@@ -430,8 +428,8 @@ __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpVi
             for (int q = 0; q < RPL; ++q) {
                 R cx = c.x, cy = c.y;
                 if constexpr (KIND == 2) {
-                    cx += ur[q] * cb.x;
-                    cy += ur[q] * cb.y;
+                    cx += urq(q) * cb.x;
+                    cy += urq(q) * cb.y;
                 }
                 C2* a = KIND == 0 ? accb : acc;
                 a[q].x += cx * xv[q].x - cy * xv[q].y;
@@ -481,6 +479,15 @@ __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpVi
         }
         if (HAS_B) {
             run(std::integral_constant<int, 0>{}, b0, e0, acc, accb);
+            // fold u * (B-only sum) here, not after the other runs: the B accumulators and the
+            // u values are then dead in the A-only and A + uB runs and the kernel fits 48
+            // registers (5 CTAs per SM for c64) instead of 63 (4)
+#pragma unroll
+            for (int q = 0; q < RPL; ++q) {
+                const R uq = __ldg(u + IO::rhs(kk, q));
+                acc[q].x = uq * accb[q].x;
+                acc[q].y = uq * accb[q].y;
+            }
             run(std::integral_constant<int, 1>{}, e0, e1, acc, accb);
             run(std::integral_constant<int, 2>{}, e1, e2, acc, accb);
         } else {
@@ -489,10 +496,6 @@ __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpVi
         }
 #pragma unroll
         for (int q = 0; q < RPL; ++q) {
-            if (HAS_B) {
-                acc[q].x += ur[q] * accb[q].x;
-                acc[q].y += ur[q] * accb[q].y;
-            }
 #pragma unroll
             for (int o = LPH; o < 32; o <<= 1) {
                 acc[q].x += __shfl_xor_sync(kFull, acc[q].x, o);
@@ -508,7 +511,7 @@ __device__ __forceinline__ void block_hc_body(const HitCacheView& hv, const OpVi
             load_lane<R, NB>(x + row * NB, kk, xd);
 #pragma unroll
             for (int q = 0; q < RPL; ++q) {
-                const R cx = da.x + ur[q] * db.x, cy = da.y + ur[q] * db.y;
+                const R cx = da.x + urq(q) * db.x, cy = da.y + urq(q) * db.y;
                 o[q].x = acc[q].x + cx * xd[q].x - cy * xd[q].y;
                 o[q].y = acc[q].y + cx * xd[q].y + cy * xd[q].x;
             }
